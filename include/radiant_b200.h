@@ -1,0 +1,204 @@
+/*
+ * radiant_b200.h -- C ABI of the B200-native discrete-ordinates (SN) transport solve.
+ *
+ * This library replaces one Julia method of Radiant.jl:
+ *     compute_flux(cross_sections::Cross_Sections, geometry::Geometry, solver::SN,
+ *                  source::Source, electromagnetic_field::Electromagnetic_Field)
+ *   (src/particle_transport/sn_flux.jl:22-233)
+ * together with everything it calls: the in-group solve (sn_one_speed.jl:81-195), the
+ * source-iteration pass (sn_inner_pass.jl:17-137), the 1D/2D/3D sweeps
+ * (sn_sweep_1D.jl:51-123, sn_sweep_2D.jl:54-183, sn_sweep_3D.jl:57-239), the cell closures
+ * (sn_{1,2,3}D_{bte,bfp}.jl), the scattering and Fokker-Planck sources
+ * (scattering_source.jl:25-68, fokker_planck_source.jl:26-35) and the in-group solvers
+ * (src/tools/{livolant,anderson,gmres,bicgstab,krylov_state}.jl).
+ *
+ * Conventions (chosen so that a Julia `ccall` can pass its arrays unchanged):
+ *   - every array is column-major (first index fastest), exactly the shape the reference
+ *     holds it in; shapes are written [a,b,c] in that order;
+ *   - material ids are 1-based (Julia's `mat`), converted from Int64 to int32 by the caller;
+ *   - every entry point returns an int32 status, 0 = RB_OK; no exception crosses the ABI;
+ *   - host buffers belong to the caller; device memory belongs to the context.
+ *   - one host thread per context; calls on one context are serialised by the caller.
+ */
+#ifndef RADIANT_B200_H
+#define RADIANT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define RB_API __attribute__((visibility("default")))
+#else
+#define RB_API
+#endif
+
+/* ---- status codes -------------------------------------------------------------------- */
+#define RB_OK 0
+#define RB_ERR_INVALID 1     /* bad argument or inconsistent problem description          */
+#define RB_ERR_UNSUPPORTED 2 /* valid in the reference but not built here (AWD, EM field)  */
+#define RB_ERR_CUDA 3        /* a CUDA runtime call failed                                 */
+#define RB_ERR_BUDGET 4      /* admission refused: the solve does not fit the HBM budget   */
+#define RB_ERR_TIMEOUT 5     /* a bounded device wait gave up (never a hang)               */
+#define RB_ERR_NOT_READY 6   /* rb_poll: the request is still on the device                */
+#define RB_ERR_NOT_FOUND 7   /* unknown problem / request handle                           */
+
+/* ---- enumerations (values follow the reference) -------------------------------------- */
+/* solver_type, src/structures/SN.jl:478-500 */
+#define RB_SOLVER_BTE 1
+#define RB_SOLVER_BFP 2
+#define RB_SOLVER_BCSD 3
+#define RB_SOLVER_FP 4
+#define RB_SOLVER_CSD 5
+#define RB_SOLVER_BFP_EF 6
+/* boundary conditions, src/structures/Geometry.jl:604-631 */
+#define RB_BC_VOID 0
+#define RB_BC_REFLECTIVE 1
+#define RB_BC_PERIODIC 2
+/* in-group acceleration, src/structures/SN.jl:348-362 */
+#define RB_ACCEL_NONE 0
+#define RB_ACCEL_LIVOLANT 1
+#define RB_ACCEL_ANDERSON 2
+#define RB_ACCEL_GMRES 3
+#define RB_ACCEL_BICGSTAB 4
+/* arithmetic form */
+#define RB_PRECISION_FP64 0  /* plain form: FP64 throughout (the drop-in)                   */
+#define RB_PRECISION_MIXED 1 /* sweeps in FP32; Krylov / outer update / tests in FP64       */
+
+/*
+ * Everything compute_flux(::SN) holds when it enters its group loop (sn_flux.jl:27-147),
+ * i.e. the tables the reference's own host functions build: quadrature, angular bases,
+ * scheme weights, cross sections after the Fokker-Planck and elastic-free corrections
+ * (sn_flux.jl:69-113), and the fixed sources.
+ */
+typedef struct rb_sn_problem {
+    /* geometry (Geometry getters, sn_flux.jl:27-33) */
+    int32_t ndims;                /* 1, 2 or 3                                              */
+    int32_t nx, ny, nz;           /* voxels per axis (1 on unused axes)                     */
+    const double *dx, *dy, *dz;   /* voxel widths [nx], [ny], [nz] (NULL on unused axes)    */
+    const int32_t *mat;           /* [nx,ny,nz] 1-based material id per voxel               */
+    int32_t nmat;
+    int32_t bc[6];                /* X-,X+,Y-,Y+,Z-,Z+ : RB_BC_*                            */
+
+    /* angular discretisation (sn_flux.jl:44-48) */
+    int32_t nd;                   /* number of directions                                   */
+    const double *mu, *eta, *xi;  /* direction cosines [nd] (eta/xi may be NULL in 1D)      */
+    int32_t np;                   /* number of angular moments                              */
+    const double *mn;             /* moment-to-discrete  Mn [nd,np]                         */
+    const double *dn;             /* discrete-to-moment  Dn [np,nd]                         */
+    const int32_t *pl;            /* Legendre order of each moment [np]                     */
+    int32_t np_surf;              /* moments of the half-range surface bases                */
+    int32_t nd_plus[6];           /* incoming directions through each face                 */
+    const double *mn_surf[6];     /* per face [nd_plus[f], np_surf]                         */
+    const double *dn_surf[6];     /* per face [np_surf, nd_plus[f]]                         */
+    const int32_t *n_to_nplus[6]; /* per face [nd], 1-based half-range index, 0 = none      */
+
+    /* spatial / energy closures (sn_flux.jl:62-64, SN.jl:520-544, scheme_weights.jl) */
+    int32_t order[4];             /* scheme order 𝒪 along x, y, z, E                        */
+    int32_t nm[5];                /* Nm: face moments x,y,z, energy-face moments, cell moments */
+    int32_t is_fc;                /* full coupling of the high-order moments                */
+    const double *w_axis[4];      /* closure weights ω along x,y,z,E, length order[a]+1     */
+    const double *cc;             /* 𝒞 [ncc], 𝒞_i = sqrt(2i-1)                              */
+    int32_t ncc;
+    const double *ww;             /* 𝒲 [order[3],order[3],order[3]]                         */
+    int32_t is_adaptive;          /* AWD closures: rejected with RB_ERR_UNSUPPORTED         */
+    int32_t is_em;                /* external EM field: rejected with RB_ERR_UNSUPPORTED    */
+
+    /* cross sections of one particle (sn_flux.jl:53-113) */
+    int32_t solver_type;          /* RB_SOLVER_*                                            */
+    int32_t ng;                   /* energy groups                                          */
+    const double *sigma_t;        /* Σtot [ng,nmat] (with T·λ₀ / elastic-free corrections)  */
+    int32_t ls;                   /* highest Legendre order carried (maximum(pl))           */
+    const double *sigma_s;        /* Σs [nmat,ng,ng,ls+1]  (gi, gf)                         */
+    const double *s_minus;        /* S⁻ [ng,nmat]  (CSD only, else NULL)                   */
+    const double *s_plus;         /* S⁺ [ng,nmat]                                           */
+    const double *s_mom;          /* S  [ng,nmat,order[3]]                                  */
+    const double *t_mom;          /* T  [ng,nmat]  (solver 2 and 4, else NULL)              */
+    const double *fp;             /* ℳ  [np,np]    (solver 2 and 4, else NULL)              */
+    const double *e_width;        /* ΔE [ng]       (CSD only)                               */
+
+    /* fixed sources (Source getters, sn_flux.jl:138-140) */
+    const double *volume_sources; /* [ng,np,nm5,nx,ny,nz] or NULL                          */
+    int32_t np_source;            /* moments of the surface sources actually used           */
+    const double *surface_sources[6]; /* per face [ng,np_source,face cells] or NULL;
+                                         face cells: 1 (1D); ny or nx (2D); (ny,nz),(nx,nz),
+                                         (nx,ny) column-major (3D)                           */
+
+    /* in-group solver (SN getters, sn_flux.jl:130-147) */
+    int32_t accel;                /* RB_ACCEL_*                                             */
+    double tol;                   /* convergence criterion ϵ_max                            */
+    int32_t max_iter;             /* I_max                                                  */
+    int32_t gmres_restart;
+    int32_t anderson_depth;
+
+    int32_t precision;            /* RB_PRECISION_*                                         */
+} rb_sn_problem;
+
+/* What compute_flux returns in its Flux_Per_Particle (sn_flux.jl:226-232), plus the
+ * per-group record sn_one_speed prints (sn_one_speed.jl:422-426). NULL pointers are skipped. */
+typedef struct rb_sn_result {
+    double *flux;            /* 𝚽l [ng,np,nm5,nx,ny,nz]                                     */
+    double *flux_cutoff;     /* 𝚽cutoff [np,nm5,nx,ny,nz] (CSD solvers)                     */
+    double *rho;             /* spectral-radius estimate per group [ng] (NaN where none)    */
+    int32_t *group_iters;    /* solver iterations per group [ng]                            */
+    double *group_resid;     /* final relative residual per group [ng]                      */
+    int32_t *group_converged;/* 1 if the group met tol [ng]                                 */
+    int64_t passes;          /* total source-iteration passes (the reference's Ntot)        */
+} rb_sn_result;
+
+typedef struct rb_context rb_context;
+typedef int64_t rb_handle;
+
+/* ---- context ------------------------------------------------------------------------- */
+/* Replaces nothing in the reference (which owns no device); the context holds the device,
+ * its stream pool and the HBM budget that admission control checks against. */
+RB_API int32_t rb_create(int32_t device, uint64_t hbm_budget_bytes, rb_context **ctx);
+RB_API int32_t rb_destroy(rb_context *ctx);
+/* Copies the message of the last failed call on ctx (or of the last rb_create failure when
+ * ctx is NULL) into buf, truncated to len bytes including the terminating zero. */
+RB_API int32_t rb_last_error(const rb_context *ctx, char *buf, uint64_t len);
+
+/* ---- one problem at a time: the compute_flux(::SN) drop-in ---------------------------- */
+/* Validates the description and copies every table to the device (the arrays
+ * compute_flux builds in sn_flux.jl:27-147). */
+RB_API int32_t rb_upload(rb_context *ctx, const rb_sn_problem *prob, rb_handle *out);
+/* Runs the full group loop of sn_flux.jl:162-224 on the device, asynchronously on
+ * `stream` (a cudaStream_t; NULL = the context's own stream). */
+RB_API int32_t rb_solve(rb_context *ctx, rb_handle h, void *stream);
+/* Solves several uploaded problems in one persistent launch (one work queue). */
+RB_API int32_t rb_solve_batch(rb_context *ctx, const rb_handle *hs, int32_t n, void *stream);
+/* Waits for the problem's stream and copies the results into caller-owned host buffers. */
+RB_API int32_t rb_download(rb_context *ctx, rb_handle h, rb_sn_result *res);
+RB_API int32_t rb_release(rb_context *ctx, rb_handle h);
+/* Bytes of device memory rb_upload would reserve for `prob` (admission control). */
+RB_API int32_t rb_required_bytes(const rb_sn_problem *prob, uint64_t *bytes);
+
+/* upload + solve + download + release on a private context: the one-call drop-in. */
+RB_API int32_t rb_compute_flux(int32_t device, const rb_sn_problem *prob, rb_sn_result *res);
+
+/* ---- serving: continuous batching over a device work queue --------------------------- */
+/* Admits a request when its state fits the remaining HBM budget (RB_ERR_BUDGET otherwise);
+ * admitted requests run as soon as a slot of the persistent kernel frees up. */
+RB_API int32_t rb_submit(rb_context *ctx, const rb_sn_problem *prob, rb_handle *out);
+/* RB_OK when the request finished (results copied into res and the request released),
+ * RB_ERR_NOT_READY while it is still running. */
+RB_API int32_t rb_poll(rb_context *ctx, rb_handle h, rb_sn_result *res);
+
+/* ---- post-processing ------------------------------------------------------------------- */
+/* energy_deposition.jl:24-87 for one particle: D[c] = (Σ_g Σe[g,mat]·𝚽l[g,1,1,c]
+ * + Σe[ng+1,mat]·𝚽cutoff[1,1,c]) / (ρ[mat]·norm). flux_cutoff may be NULL (no CSD). */
+RB_API int32_t rb_energy_deposition(int32_t ng, int32_t np, int32_t nm5, int64_t ncell,
+                             int32_t nmat, const int32_t *mat, const double *flux,
+                             const double *flux_cutoff, const double *sigma_e,
+                             const double *density, double norm, double *dep);
+
+/* Library version string. */
+RB_API const char *rb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RADIANT_B200_H */

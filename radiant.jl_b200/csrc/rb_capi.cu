@@ -1,0 +1,715 @@
+// rb_capi.cu -- the C ABI of include/radiant_b200.h.
+//
+// Host side of the library: validates a problem description, derives the per-direction
+// closure tables once per solve, lays every table and work buffer out in one device
+// allocation per problem, launches the persistent solve kernel on a stream and copies the
+// results back in the reference's array layouts. No exception crosses the ABI: every entry
+// point returns a status and records a message for rb_last_error.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/radiant_b200.h"
+#include "rb_solve.cuh"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct ProblemRec {
+    DevProblem h;            // host copy of the device record
+    DevProblem *d = nullptr; // device copy
+    char *block = nullptr;   // the problem's single device allocation
+    size_t bytes = 0;
+    int ng = 0, np = 0, nm5 = 0, csd = 0;
+    long long ncell = 0, nphi = 0;
+    cudaStream_t stream = nullptr;  // stream of the last solve
+    bool solved = false;
+};
+
+}  // namespace
+
+struct rb_context {
+    int device = 0;
+    int nsm = 0;
+    uint64_t budget = 0;
+    uint64_t used = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    std::map<int64_t, std::unique_ptr<ProblemRec>> probs;
+    int64_t next_handle = 1;
+    // launch scratch: problem pointer array + queue counter, staging for the layout change
+    DevProblem **d_list = nullptr;
+    int list_cap = 0;
+    int *d_queue = nullptr;
+    double *d_stage = nullptr;
+    size_t stage_cap = 0;
+    // serving
+    std::vector<int64_t> pending;
+};
+
+namespace {
+
+int fail(rb_context *ctx, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf; else g_create_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(ctx, RB_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------------
+// moment bookkeeping of the closures (same flattening as sn_{1,2,3}D_{bte,bfp}.jl)
+// ---------------------------------------------------------------------------------------------
+struct Moments {
+    int nax = 0, ax[4] = {0}, ord[4] = {0}, nm = 0;
+    int tup[RB_MAXNM][4];
+    int face[4][RB_MAXNM];
+    int nface[4] = {1, 1, 1, 1};
+};
+
+int flat_index(int nax, const int *ord, const int *t, int fc) {
+    if (fc) {
+        int idx = 0, stride = 1;
+        for (int a = 0; a < nax; a++) { idx += (t[a] - 1) * stride; stride *= ord[a]; }
+        return idx;
+    }
+    int off = 1;
+    for (int a = 0; a < nax; a++) {
+        if (t[a] > 1) return off + (t[a] - 2);
+        off += ord[a] - 1;
+    }
+    return 0;
+}
+int count_of(int nax, const int *ord, int fc) {
+    int c = 1;
+    if (fc) { for (int a = 0; a < nax; a++) c *= ord[a]; return c; }
+    for (int a = 0; a < nax; a++) c += ord[a] - 1;
+    return c;
+}
+bool build_moments(Moments &M, int ndims, int csd, const int32_t *order, int fc) {
+    M.nax = 0;
+    if (csd) { M.ax[M.nax] = 3; M.ord[M.nax] = order[3]; M.nax++; }
+    for (int d = 0; d < ndims; d++) { M.ax[M.nax] = d; M.ord[M.nax] = order[d]; M.nax++; }
+    M.nm = count_of(M.nax, M.ord, fc);
+    if (M.nm > RB_MAXNM) return false;
+    int total = 1;
+    for (int a = 0; a < M.nax; a++) total *= M.ord[a];
+    for (int c = 0; c < total; c++) {
+        int t[4], r = c, nbig = 0;
+        for (int a = 0; a < M.nax; a++) { t[a] = r % M.ord[a] + 1; r /= M.ord[a]; if (t[a] > 1) nbig++; }
+        if (!fc && nbig >= 2) continue;
+        int j = flat_index(M.nax, M.ord, t, fc);
+        for (int k = 0; k < 4; k++) M.tup[j][k] = 1;
+        for (int a = 0; a < M.nax; a++) M.tup[j][M.ax[a]] = t[a];
+        for (int a = 0; a < M.nax; a++) {
+            int sub[4], so[4], ns = 0;
+            for (int b = 0; b < M.nax; b++) if (b != a) { sub[ns] = t[b]; so[ns] = M.ord[b]; ns++; }
+            M.face[M.ax[a]][j] = flat_index(ns, so, sub, fc);
+            M.nface[M.ax[a]] = count_of(ns, so, fc);
+        }
+    }
+    return true;
+}
+
+double ipow(double s, int k) { double r = 1.0; for (int i = 0; i < k; i++) r *= s; return r; }
+double m1pow(int k) { return (k % 2 == 0) ? 1.0 : -1.0; }
+double jsign(double x) { return x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0); }
+
+long long face_cells(int ndims, const int *ns, int axis) {
+    if (ndims == 1) return 1;
+    if (ndims == 2) return axis == 0 ? ns[1] : ns[0];
+    if (axis == 0) return (long long)ns[1] * ns[2];
+    if (axis == 1) return (long long)ns[0] * ns[2];
+    return (long long)ns[0] * ns[1];
+}
+
+// Layout of one problem's device block.
+struct Layout {
+    size_t off = 0;
+    template <class T>
+    size_t take(size_t count) {
+        size_t o = (off + 255) & ~size_t(255);
+        off = o + sizeof(T) * (count > 0 ? count : 1);
+        return o;
+    }
+};
+
+int nvec_for(const rb_sn_problem *P) {
+    switch (P->accel) {
+        case RB_ACCEL_NONE:
+        case RB_ACCEL_LIVOLANT: return 5;
+        case RB_ACCEL_ANDERSON: return 5 + 2 * (P->anderson_depth > 1 ? P->anderson_depth : 1);
+        case RB_ACCEL_GMRES: return 5 + (P->gmres_restart > 1 ? P->gmres_restart : 1);
+        case RB_ACCEL_BICGSTAB: return 8;
+    }
+    return 8;
+}
+
+// Everything derived from the description before it goes to the device.
+struct Derived {
+    Moments M;
+    int ns[3];
+    long long ncell, nphi, nstate, off_b[3], nb[3];
+    int csd;
+    std::vector<int> mat0;
+    std::vector<double> cosv, mnfp, frow_m, frow_d, G, Gsrc, Gout, Kcsd, Bcsd, EsA, EsB, Eout, vol;
+    std::vector<int> tang;
+    double w1[4];
+    int nfmax = 1;
+};
+
+int validate_and_derive(rb_context *ctx, const rb_sn_problem *P, Derived &D) {
+    if (!P) return fail(ctx, RB_ERR_INVALID, "null problem");
+    if (P->ndims < 1 || P->ndims > 3) return fail(ctx, RB_ERR_INVALID, "ndims must be 1, 2 or 3 (got %d)", P->ndims);
+    if (P->ndims != 1)
+        return fail(ctx, RB_ERR_UNSUPPORTED, "ndims=%d: only the 1D sweep is built in this library version", P->ndims);
+    if (P->is_adaptive) return fail(ctx, RB_ERR_UNSUPPORTED, "adaptive (AWD) closures are not built");
+    if (P->is_em) return fail(ctx, RB_ERR_UNSUPPORTED, "external electromagnetic fields are not built");
+    if (P->solver_type < 1 || P->solver_type > 6) return fail(ctx, RB_ERR_INVALID, "solver_type %d", P->solver_type);
+    if (P->accel < 0 || P->accel > 4) return fail(ctx, RB_ERR_INVALID, "accel %d", P->accel);
+    if (P->accel == RB_ACCEL_GMRES && P->gmres_restart > RB_MAXRESTART)
+        return fail(ctx, RB_ERR_INVALID, "gmres_restart %d exceeds %d", P->gmres_restart, RB_MAXRESTART);
+    if (P->accel == RB_ACCEL_ANDERSON && P->anderson_depth > RB_MAXDEPTH)
+        return fail(ctx, RB_ERR_INVALID, "anderson_depth %d exceeds %d", P->anderson_depth, RB_MAXDEPTH);
+    if (P->nmat < 1 || P->nmat > RB_MAXMAT) return fail(ctx, RB_ERR_INVALID, "nmat %d out of [1,%d]", P->nmat, RB_MAXMAT);
+    if (P->nd < 1 || P->np < 1 || P->ng < 1) return fail(ctx, RB_ERR_INVALID, "empty angular or energy grid");
+    if (!P->mat || !P->mn || !P->dn || !P->pl || !P->sigma_t || !P->sigma_s || !P->mu || !P->dx)
+        return fail(ctx, RB_ERR_INVALID, "a required table is NULL");
+    if (P->max_iter < 1) return fail(ctx, RB_ERR_INVALID, "max_iter must be >= 1");
+    if (!(P->tol > 0)) return fail(ctx, RB_ERR_INVALID, "tol must be > 0");
+    D.csd = P->solver_type >= 2;
+    if (D.csd && (!P->s_minus || !P->s_plus || !P->s_mom || !P->e_width || !P->ww))
+        return fail(ctx, RB_ERR_INVALID, "CSD solver without stopping powers / energy widths");
+    if ((P->solver_type == 2 || P->solver_type == 4) && (!P->t_mom || !P->fp))
+        return fail(ctx, RB_ERR_INVALID, "Fokker-Planck solver without momentum transfer / matrix");
+    if (P->order[3] > RB_MAXORD || P->order[0] > RB_MAXORD) return fail(ctx, RB_ERR_INVALID, "scheme order too high");
+    D.ns[0] = P->nx; D.ns[1] = P->ndims >= 2 ? P->ny : 1; D.ns[2] = P->ndims >= 3 ? P->nz : 1;
+    if (D.ns[0] < 1 || D.ns[1] < 1 || D.ns[2] < 1) return fail(ctx, RB_ERR_INVALID, "empty geometry");
+    if (!build_moments(D.M, P->ndims, D.csd, P->order, P->is_fc))
+        return fail(ctx, RB_ERR_UNSUPPORTED, "cell system larger than %d moments", RB_MAXNM);
+    if (D.M.nm != P->nm[4]) return fail(ctx, RB_ERR_INVALID, "nm[4]=%d but the closures give %d moments", P->nm[4], D.M.nm);
+    for (int d = 0; d < P->ndims; d++)
+        if (D.M.nface[d] != P->nm[d]) return fail(ctx, RB_ERR_INVALID, "nm[%d]=%d but the closures give %d", d, P->nm[d], D.M.nface[d]);
+    if (D.csd && D.M.nface[3] != P->nm[3]) return fail(ctx, RB_ERR_INVALID, "nm[3] inconsistent");
+    if (P->nm[0] > RB_MAXFACE || P->nm[3] > RB_MAXFACE) return fail(ctx, RB_ERR_INVALID, "too many face moments");
+    for (int k = 0; k < P->np; k++)
+        if (P->pl[k] < 0 || P->pl[k] > P->ls) return fail(ctx, RB_ERR_INVALID, "pl[%d]=%d outside [0,ls=%d]", k, P->pl[k], P->ls);
+    D.ncell = (long long)D.ns[0] * D.ns[1] * D.ns[2];
+    const int nm5 = D.M.nm, np = P->np, nd = P->nd, nps = P->np_surf;
+    D.nphi = (long long)np * nm5 * D.ncell;
+    long long off = D.nphi;
+    for (int d = 0; d < 3; d++) {
+        D.nb[d] = d < P->ndims ? (long long)nps * P->nm[d] * 2 * face_cells(P->ndims, D.ns, d) : 0;
+        D.off_b[d] = off;
+        off += D.nb[d];
+    }
+    D.nstate = off;
+    // materials
+    D.mat0.resize(D.ncell);
+    for (long long c = 0; c < D.ncell; c++) {
+        int m = P->mat[c];
+        if (m < 1 || m > P->nmat) return fail(ctx, RB_ERR_INVALID, "mat[%lld]=%d outside 1..%d", c, m, P->nmat);
+        D.mat0[c] = m - 1;
+    }
+    for (long long c = 0; c < D.ns[0]; c++)
+        if (!(P->dx[c] > 0)) return fail(ctx, RB_ERR_INVALID, "dx[%lld] must be > 0", c);
+    // directions
+    D.cosv.assign(3 * (size_t)nd, 0.0);
+    for (int n = 0; n < nd; n++) {
+        D.cosv[n] = P->mu[n];
+        D.cosv[nd + n] = P->eta ? P->eta[n] : 0.0;
+        D.cosv[2 * nd + n] = P->xi ? P->xi[n] : 0.0;
+    }
+    // Mn·ℳ
+    if (P->solver_type == 2 || P->solver_type == 4) {
+        D.mnfp.assign((size_t)nd * np, 0.0);
+        for (int n = 0; n < nd; n++)
+            for (int p = 0; p < np; p++) {
+                double s = 0.0;
+                for (int q = 0; q < np; q++) s += P->mn[n + (long long)nd * q] * P->fp[q + (long long)np * p];
+                D.mnfp[n + (size_t)nd * p] = s;
+            }
+    }
+    // half-range rows per direction and axis (sn_inner_pass.jl:47-58)
+    D.frow_m.assign((size_t)3 * nd * (nps > 0 ? nps : 1), 0.0);
+    D.frow_d.assign((size_t)3 * nd * (nps > 0 ? nps : 1), 0.0);
+    for (int a = 0; a < P->ndims; a++) {
+        int fm = 2 * a, fp = 2 * a + 1;
+        for (int n = 0; n < nd; n++) {
+            int k1 = P->n_to_nplus[fm] ? P->n_to_nplus[fm][n] : 0;
+            int k2 = P->n_to_nplus[fp] ? P->n_to_nplus[fp][n] : 0;
+            int f = -1, k = 0;
+            if (k1 != 0) { f = fm; k = k1; } else if (k2 != 0) { f = fp; k = k2; }
+            if (f < 0) continue;
+            if (k > P->nd_plus[f]) return fail(ctx, RB_ERR_INVALID, "n_to_nplus[%d][%d]=%d > nd_plus", f, n, k);
+            for (int p = 0; p < nps; p++) {
+                D.frow_m[((size_t)a * nd + n) * nps + p] = P->mn_surf[f][(k - 1) + (long long)P->nd_plus[f] * p];
+                D.frow_d[((size_t)a * nd + n) * nps + p] = P->dn_surf[f][p + (long long)nps * (k - 1)];
+            }
+        }
+    }
+    // closure coefficient tables (the terms of flux_xD_BTE / flux_xD_BFP, factored by h)
+    const Moments &M = D.M;
+    const double *C = P->cc;
+    for (int a = 0; a < 4; a++) D.w1[a] = P->w_axis[a] ? P->w_axis[a][0] : 0.0;
+    int nfmax = 1;
+    for (int a = 0; a < P->ndims; a++) nfmax = P->nm[a] > nfmax ? P->nm[a] : nfmax;
+    D.nfmax = nfmax;
+    D.G.assign((size_t)nd * 3 * nm5 * nm5, 0.0);
+    D.Gsrc.assign((size_t)nd * 3 * nm5 * nfmax, 0.0);
+    D.Gout.assign((size_t)nd * 3 * nm5 * nfmax, 0.0);
+    D.tang.assign(nd, 0);
+    for (int n = 0; n < nd; n++) {
+        for (int a = 0; a < P->ndims; a++) {
+            double cosa = D.cosv[(size_t)a * nd + n];
+            double s = jsign(cosa);
+            if (P->ndims == 1 && std::fabs(cosa) <= 1e-10) { s = 1.0; D.tang[n] = 1; }  // sn_1D_bte.jl:30-32
+            const double *w = P->w_axis[a];
+            const int nfa = P->nm[a];
+            const size_t blk = (size_t)n * 3 + a;
+            double *Gb = &D.G[blk * nm5 * nm5];
+            for (int i = 0; i < nm5; i++)
+                for (int j = 0; j < nm5; j++) {
+                    bool same = true;
+                    for (int k = 0; k < 4; k++) if (k != a && M.tup[i][k] != M.tup[j][k]) same = false;
+                    if (!same) continue;
+                    int ia = M.tup[i][a], ja = M.tup[j][a];
+                    double v = 0.0;
+                    if (ia >= ja + 1) v -= C[ia - 1] * s * C[ja - 1] * (1.0 - m1pow(ia - ja));
+                    v += C[ia - 1] * ipow(s, ia - 1) * C[ja - 1] * ipow(s, ja - 1) * w[ja];
+                    Gb[i + nm5 * j] = v;
+                }
+            for (int j = 0; j < nm5; j++) {
+                int ja = M.tup[j][a], f = M.face[a][j];
+                D.Gsrc[blk * nm5 * nfmax + j + (size_t)nm5 * f] = -C[ja - 1] * (ipow(s, ja - 1) * w[0] - ipow(-s, ja - 1));
+                D.Gout[blk * nm5 * nfmax + f + (size_t)nfa * j] = C[ja - 1] * ipow(s, ja - 1) * w[ja];
+            }
+        }
+    }
+    const int oE = P->order[3];
+    const int nE = D.csd ? P->nm[3] : 1;
+    D.Kcsd.assign((size_t)oE * nm5 * nm5, 0.0);
+    D.Bcsd.assign((size_t)nm5 * nm5, 0.0);
+    D.EsA.assign((size_t)nm5 * nE, 0.0); D.EsB.assign((size_t)nm5 * nE, 0.0); D.Eout.assign((size_t)nm5 * nE, 0.0);
+    if (D.csd) {
+        const double *wE = P->w_axis[3];
+        for (int i = 0; i < nm5; i++)
+            for (int j = 0; j < nm5; j++) {
+                bool same = true;
+                for (int d = 0; d < P->ndims; d++) if (M.tup[i][d] != M.tup[j][d]) same = false;
+                if (!same) continue;
+                int iE = M.tup[i][3], jE = M.tup[j][3];
+                for (int kE = 1; kE <= iE - 1; kE++)
+                    for (int wi = 1; wi <= oE; wi++)
+                        D.Kcsd[(size_t)(wi - 1) * nm5 * nm5 + i + nm5 * j] +=
+                            C[iE - 1] * C[jE - 1] * C[kE - 1] * C[wi - 1] * (1.0 - m1pow(iE - kE)) *
+                            P->ww[(jE - 1) + oE * ((kE - 1) + oE * (wi - 1))];
+                D.Bcsd[i + nm5 * j] = C[iE - 1] * m1pow(iE - 1) * C[jE - 1] * m1pow(jE - 1) * wE[jE];
+            }
+        for (int j = 0; j < nm5; j++) {
+            int jE = M.tup[j][3], e = M.face[3][j];
+            D.EsA[j + (size_t)nm5 * e] = C[jE - 1] * m1pow(jE - 1) * wE[0];
+            D.EsB[j + (size_t)nm5 * e] = C[jE - 1];
+            D.Eout[e + (size_t)nE * j] = C[jE - 1] * m1pow(jE - 1) * wE[jE];
+        }
+    }
+    // volume sources, group-major
+    if (P->volume_sources) {
+        D.vol.resize((size_t)P->ng * D.nphi);
+        for (int g = 0; g < P->ng; g++)
+            for (long long k = 0; k < D.nphi; k++)
+                D.vol[(size_t)g * D.nphi + k] = P->volume_sources[g + (long long)P->ng * k];
+    }
+    return RB_OK;
+}
+
+template <class T>
+int put(rb_context *ctx, char *block, size_t off, const T *src, size_t count, cudaStream_t s) {
+    if (count == 0 || !src) return RB_OK;
+    CK(cudaMemcpyAsync(block + off, src, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+    return RB_OK;
+}
+
+int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64]) {
+    const int nd = P->nd, np = P->np, nm5 = D.M.nm, ng = P->ng, nmat = P->nmat;
+    const long long nq = (long long)nd * nm5 * D.ncell;
+    const long long nE = (long long)nd * P->nm[3] * D.ncell;
+    int k = 0;
+    offs[k++] = L.take<DevProblem>(1);
+    offs[k++] = L.take<double>(D.ns[0]);                  // 1 dx
+    offs[k++] = L.take<int>(D.ncell);                     // 2 mat
+    offs[k++] = L.take<double>(3 * (size_t)nd);           // 3 cosv
+    offs[k++] = L.take<double>((size_t)nd * np);          // 4 mn
+    offs[k++] = L.take<double>((size_t)np * nd);          // 5 dn
+    offs[k++] = L.take<int>(np);                          // 6 pl
+    offs[k++] = L.take<double>(D.mnfp.size());            // 7 mnfp
+    offs[k++] = L.take<double>(D.frow_m.size());          // 8
+    offs[k++] = L.take<double>(D.frow_d.size());          // 9
+    offs[k++] = L.take<double>(D.G.size());               // 10
+    offs[k++] = L.take<double>(D.Gsrc.size());            // 11
+    offs[k++] = L.take<double>(D.Gout.size());            // 12
+    offs[k++] = L.take<int>(D.tang.size());               // 13
+    offs[k++] = L.take<double>(3 * D.EsA.size());         // 14 EsA, EsB, Eout
+    offs[k++] = L.take<double>(D.Kcsd.size());            // 15
+    offs[k++] = L.take<double>(D.Bcsd.size());            // 16
+    offs[k++] = L.take<double>(1);                        // 17 (unused)
+    offs[k++] = L.take<double>((size_t)ng * nmat);        // 18 sigma_t
+    offs[k++] = L.take<double>((size_t)nmat * ng * ng * (P->ls + 1)); // 19 sigma_s
+    offs[k++] = L.take<double>(D.csd ? (size_t)ng * nmat : 0);        // 20 s_minus
+    offs[k++] = L.take<double>(D.csd ? (size_t)ng * nmat : 0);        // 21 s_plus
+    offs[k++] = L.take<double>(D.csd ? (size_t)ng * nmat * P->order[3] : 0); // 22 s_mom
+    offs[k++] = L.take<double>(P->t_mom ? (size_t)ng * nmat : 0);     // 23 t_mom
+    offs[k++] = L.take<double>(D.csd ? (size_t)ng : 0);               // 24 e_width
+    offs[k++] = L.take<double>(D.vol.size());                         // 25 vol
+    for (int f = 0; f < 6; f++)                                       // 26..31 surface
+        offs[k++] = L.take<double>((f < 2 * P->ndims && P->surface_sources[f])
+                                       ? (size_t)ng * P->np_source * face_cells(P->ndims, D.ns, f / 2) : 0);
+    offs[k++] = L.take<double>((size_t)ng * D.nphi);      // 32 flux
+    offs[k++] = L.take<double>((size_t)nvec_for(P) * D.nstate); // 33 vecs
+    offs[k++] = L.take<double>(D.nphi);                   // 34 qlout
+    offs[k++] = L.take<double>(nq);                       // 35 qnout
+    offs[k++] = L.take<double>(nq);                       // 36 psi
+    offs[k++] = L.take<double>((size_t)nmat * nd * np);   // 37 kmat
+    offs[k++] = L.take<double>((size_t)nmat * nm5 * nm5); // 38 scsd
+    offs[k++] = L.take<double>((size_t)nd * RB_MAXFACE);  // 39 fexit
+    offs[k++] = L.take<double>(D.csd ? nE : 0);           // 40 phiE_a
+    offs[k++] = L.take<double>(D.csd ? nE : 0);           // 41 phiE_b
+    offs[k++] = L.take<double>(D.csd ? D.nphi : 0);       // 42 cutoff
+    offs[k++] = L.take<double>(2 * (size_t)ng);           // 43 rho, resid
+    offs[k++] = L.take<int>(2 * (size_t)ng);              // 44 iters, conv
+    offs[k++] = L.take<long long>(1);                     // 45 passes
+    offs[k++] = L.take<int>(1);                           // 46 status
+    return k;
+}
+
+int ensure_launch_scratch(rb_context *ctx, int n) {
+    if (n > ctx->list_cap) {
+        if (ctx->d_list) cudaFree(ctx->d_list);
+        int cap = n < 64 ? 64 : n;
+        CK(cudaMalloc(&ctx->d_list, sizeof(DevProblem *) * cap));
+        ctx->list_cap = cap;
+    }
+    if (!ctx->d_queue) CK(cudaMalloc(&ctx->d_queue, sizeof(int) * 64));
+    return RB_OK;
+}
+
+int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t s) {
+    int n = (int)recs.size();
+    if (n == 0) return RB_OK;
+    int st = ensure_launch_scratch(ctx, n);
+    if (st) return st;
+    std::vector<DevProblem *> ptrs(n);
+    for (int i = 0; i < n; i++) ptrs[i] = recs[i]->d;
+    CK(cudaMemcpyAsync(ctx->d_list, ptrs.data(), sizeof(DevProblem *) * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), s));
+    for (auto *r : recs) CK(cudaMemsetAsync(r->h.status, 0, sizeof(int), s));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb::solve_batch_kernel, RB_THREADS, 0));
+    if (per_sm < 1) per_sm = 1;
+    int grid = ctx->nsm * per_sm;
+    if (grid > n) grid = n;
+    rb::solve_batch_kernel<<<grid, RB_THREADS, 0, s>>>(ctx->d_list, n, ctx->d_queue);
+    CK(cudaGetLastError());
+    for (auto *r : recs) { r->stream = s; r->solved = true; }
+    return RB_OK;
+}
+
+ProblemRec *find(rb_context *ctx, rb_handle h) {
+    auto it = ctx->probs.find(h);
+    return it == ctx->probs.end() ? nullptr : it->second.get();
+}
+
+}  // namespace
+
+// =============================================================================================
+// ABI
+// =============================================================================================
+extern "C" {
+
+const char *rb_version(void) { return "radiant_b200 0.1 (sm_100a)"; }
+
+int32_t rb_create(int32_t device, uint64_t hbm_budget_bytes, rb_context **out) {
+    if (!out) return fail(nullptr, RB_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return fail(nullptr, RB_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return fail(nullptr, RB_ERR_INVALID, "device %d out of range", device);
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, RB_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    auto *c = new rb_context();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)(fr * 0.9);
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete c; return fail(nullptr, RB_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
+    *out = c;
+    return RB_OK;
+}
+
+int32_t rb_destroy(rb_context *ctx) {
+    if (!ctx) return RB_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    for (auto &kv : ctx->probs) cudaFree(kv.second->block);
+    ctx->probs.clear();
+    if (ctx->d_list) cudaFree(ctx->d_list);
+    if (ctx->d_queue) cudaFree(ctx->d_queue);
+    if (ctx->d_stage) cudaFree(ctx->d_stage);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return RB_OK;
+}
+
+int32_t rb_last_error(const rb_context *ctx, char *buf, uint64_t len) {
+    if (!buf || len == 0) return RB_ERR_INVALID;
+    const std::string &s = ctx ? ctx->err : g_create_error;
+    size_t n = s.size() < len - 1 ? s.size() : (size_t)(len - 1);
+    memcpy(buf, s.data(), n);
+    buf[n] = 0;
+    return RB_OK;
+}
+
+int32_t rb_required_bytes(const rb_sn_problem *prob, uint64_t *bytes) {
+    Derived D;
+    int st = validate_and_derive(nullptr, prob, D);
+    if (st) return st;
+    Layout L;
+    size_t offs[64];
+    required(prob, D, L, offs);
+    if (bytes) *bytes = L.off;
+    return RB_OK;
+}
+
+int32_t rb_upload(rb_context *ctx, const rb_sn_problem *P, rb_handle *out) {
+    if (!ctx || !out) return fail(ctx, RB_ERR_INVALID, "null context or handle");
+    CK(cudaSetDevice(ctx->device));
+    Derived D;
+    int st = validate_and_derive(ctx, P, D);
+    if (st) return st;
+    Layout L;
+    size_t o[64];
+    required(P, D, L, o);
+    if (ctx->used + L.off > ctx->budget)
+        return fail(ctx, RB_ERR_BUDGET, "problem needs %zu bytes, %llu of %llu budget bytes in use", L.off,
+                    (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
+    auto rec = std::make_unique<ProblemRec>();
+    CK(cudaMalloc(&rec->block, L.off));
+    rec->bytes = L.off;
+    char *b = rec->block;
+    cudaStream_t s = ctx->stream;
+    DevProblem &h = rec->h;
+    memset(&h, 0, sizeof(h));
+    const int nd = P->nd, np = P->np, nm5 = D.M.nm, ng = P->ng, nmat = P->nmat;
+    h.ndims = P->ndims; h.nx = D.ns[0]; h.ny = D.ns[1]; h.nz = D.ns[2]; h.ncell = D.ncell;
+    h.nd = nd; h.np = np; h.nm5 = nm5;
+    for (int d = 0; d < 3; d++) h.nmf[d] = d < P->ndims ? P->nm[d] : 1;
+    h.nm4 = D.csd ? P->nm[3] : 1;
+    h.npsurf = P->np_surf; h.ng = ng; h.nmat = nmat; h.ls = P->ls; h.oE = P->order[3]; h.csd = D.csd;
+    h.solver_type = P->solver_type; h.accel = P->accel; h.maxit = P->max_iter; h.restart = P->gmres_restart;
+    h.depth = P->anderson_depth; h.precision = P->precision; h.tol = P->tol; h.np_source = P->np_source;
+    h.nphi = D.nphi; h.nstate = D.nstate;
+    for (int d = 0; d < 3; d++) { h.off_b[d] = D.off_b[d]; h.nb[d] = D.nb[d]; }
+    h.nvec = nvec_for(P);
+    for (int a = 0; a < 4; a++) h.w1[a] = D.w1[a];
+    for (int f = 0; f < 6; f++) h.bc[f] = P->bc[f];
+#define DP(T, k) (reinterpret_cast<T *>(b + o[k]))
+    h.dx = DP(double, 1); h.mat = DP(int, 2); h.cosv = DP(double, 3); h.mn = DP(double, 4); h.dn = DP(double, 5);
+    h.pl = DP(int, 6); h.mnfp = D.mnfp.empty() ? nullptr : DP(double, 7); h.frow_m = DP(double, 8);
+    h.frow_d = DP(double, 9); h.G = DP(double, 10); h.Gsrc = DP(double, 11); h.Gout = DP(double, 12);
+    h.tang = DP(int, 13); h.Kcsd = DP(double, 15); h.Bcsd = DP(double, 16);
+    h.EsA = DP(double, 14); h.EsB = h.EsA + D.EsA.size(); h.Eout = h.EsA + 2 * D.EsA.size();
+    h.nfmax = D.nfmax;
+    h.sigma_t = DP(double, 18); h.sigma_s = DP(double, 19);
+    h.s_minus = D.csd ? DP(double, 20) : nullptr; h.s_plus = D.csd ? DP(double, 21) : nullptr;
+    h.s_mom = D.csd ? DP(double, 22) : nullptr; h.t_mom = P->t_mom ? DP(double, 23) : nullptr;
+    h.e_width = D.csd ? DP(double, 24) : nullptr; h.vol = D.vol.empty() ? nullptr : DP(double, 25);
+    for (int f = 0; f < 6; f++) h.surf[f] = (f < 2 * P->ndims && P->surface_sources[f]) ? DP(double, 26 + f) : nullptr;
+    h.flux = DP(double, 32); h.vecs = DP(double, 33); h.qlout = DP(double, 34); h.qnout = DP(double, 35);
+    h.psi = DP(double, 36); h.kmat = DP(double, 37); h.scsd = DP(double, 38); h.fexit = DP(double, 39);
+    h.phiE_a = D.csd ? DP(double, 40) : nullptr; h.phiE_b = D.csd ? DP(double, 41) : nullptr;
+    h.cutoff = D.csd ? DP(double, 42) : nullptr;
+    h.rho = DP(double, 43); h.resid = h.rho + ng; h.iters = DP(int, 44); h.conv = h.iters + ng;
+    h.passes = DP(long long, 45); h.status = DP(int, 46);
+    int r = RB_OK;
+#define PUT(T, k, src, n) if ((r = put<T>(ctx, b, o[k], src, n, s)) != RB_OK) { cudaFree(rec->block); return r; }
+    PUT(double, 1, P->dx, D.ns[0]);
+    PUT(int, 2, D.mat0.data(), D.mat0.size());
+    PUT(double, 3, D.cosv.data(), D.cosv.size());
+    PUT(double, 4, P->mn, (size_t)nd * np);
+    PUT(double, 5, P->dn, (size_t)np * nd);
+    PUT(int, 6, P->pl, np);
+    PUT(double, 7, D.mnfp.data(), D.mnfp.size());
+    PUT(double, 8, D.frow_m.data(), D.frow_m.size());
+    PUT(double, 9, D.frow_d.data(), D.frow_d.size());
+    PUT(double, 10, D.G.data(), D.G.size());
+    PUT(double, 11, D.Gsrc.data(), D.Gsrc.size());
+    PUT(double, 12, D.Gout.data(), D.Gout.size());
+    PUT(int, 13, D.tang.data(), D.tang.size());
+    std::vector<double> eabo;
+    eabo.insert(eabo.end(), D.EsA.begin(), D.EsA.end());
+    eabo.insert(eabo.end(), D.EsB.begin(), D.EsB.end());
+    eabo.insert(eabo.end(), D.Eout.begin(), D.Eout.end());
+    PUT(double, 14, eabo.data(), eabo.size());
+    PUT(double, 15, D.Kcsd.data(), D.Kcsd.size());
+    PUT(double, 16, D.Bcsd.data(), D.Bcsd.size());
+    PUT(double, 18, P->sigma_t, (size_t)ng * nmat);
+    PUT(double, 19, P->sigma_s, (size_t)nmat * ng * ng * (P->ls + 1));
+    if (D.csd) {
+        PUT(double, 20, P->s_minus, (size_t)ng * nmat);
+        PUT(double, 21, P->s_plus, (size_t)ng * nmat);
+        PUT(double, 22, P->s_mom, (size_t)ng * nmat * P->order[3]);
+        PUT(double, 24, P->e_width, ng);
+    }
+    if (P->t_mom) PUT(double, 23, P->t_mom, (size_t)ng * nmat);
+    PUT(double, 25, D.vol.data(), D.vol.size());
+    for (int f = 0; f < 2 * P->ndims; f++)
+        if (P->surface_sources[f])
+            PUT(double, 26 + f, P->surface_sources[f], (size_t)ng * P->np_source * face_cells(P->ndims, D.ns, f / 2));
+#undef PUT
+    rec->d = DP(DevProblem, 0);
+#undef DP
+    CK(cudaMemcpyAsync(rec->d, &h, sizeof(DevProblem), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    rec->ng = ng; rec->np = np; rec->nm5 = nm5; rec->csd = D.csd; rec->ncell = D.ncell; rec->nphi = D.nphi;
+    ctx->used += L.off;
+    rb_handle hd = ctx->next_handle++;
+    ctx->probs[hd] = std::move(rec);
+    *out = hd;
+    return RB_OK;
+}
+
+int32_t rb_solve(rb_context *ctx, rb_handle hd, void *stream) {
+    return rb_solve_batch(ctx, &hd, 1, stream);
+}
+
+int32_t rb_solve_batch(rb_context *ctx, const rb_handle *hs, int32_t n, void *stream) {
+    if (!ctx || (!hs && n > 0) || n < 0) return fail(ctx, RB_ERR_INVALID, "bad arguments");
+    CK(cudaSetDevice(ctx->device));
+    std::vector<ProblemRec *> recs;
+    for (int i = 0; i < n; i++) {
+        ProblemRec *r = find(ctx, hs[i]);
+        if (!r) return fail(ctx, RB_ERR_NOT_FOUND, "unknown problem handle %lld", (long long)hs[i]);
+        recs.push_back(r);
+    }
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    return launch(ctx, recs, s);
+}
+
+int32_t rb_download(rb_context *ctx, rb_handle hd, rb_sn_result *res) {
+    if (!ctx || !res) return fail(ctx, RB_ERR_INVALID, "null context or result");
+    CK(cudaSetDevice(ctx->device));
+    ProblemRec *r = find(ctx, hd);
+    if (!r) return fail(ctx, RB_ERR_NOT_FOUND, "unknown problem handle %lld", (long long)hd);
+    if (!r->solved) return fail(ctx, RB_ERR_INVALID, "problem %lld was not solved", (long long)hd);
+    cudaStream_t s = r->stream;
+    const DevProblem &h = r->h;
+    if (res->flux) {
+        size_t need = (size_t)r->ng * r->nphi;
+        if (need > ctx->stage_cap) {
+            if (ctx->d_stage) cudaFree(ctx->d_stage);
+            ctx->d_stage = nullptr;
+            CK(cudaMalloc(&ctx->d_stage, need * sizeof(double)));
+            ctx->stage_cap = need;
+        }
+        dim3 blk(32, 8), grd((unsigned)((r->nphi + 31) / 32), (unsigned)((r->ng + 31) / 32));
+        rb::to_reference_layout<<<grd, blk, 0, s>>>(h.flux, ctx->d_stage, r->ng, r->nphi);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(res->flux, ctx->d_stage, need * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    if (res->flux_cutoff && r->csd)
+        CK(cudaMemcpyAsync(res->flux_cutoff, h.cutoff, r->nphi * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (res->rho) CK(cudaMemcpyAsync(res->rho, h.rho, r->ng * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (res->group_resid) CK(cudaMemcpyAsync(res->group_resid, h.resid, r->ng * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (res->group_iters) CK(cudaMemcpyAsync(res->group_iters, h.iters, r->ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (res->group_converged) CK(cudaMemcpyAsync(res->group_converged, h.conv, r->ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+    long long passes = 0;
+    int status = 0;
+    CK(cudaMemcpyAsync(&passes, h.passes, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&status, h.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    res->passes = passes;
+    if (status & RB_DEV_TIMEOUT) return fail(ctx, RB_ERR_TIMEOUT, "a device wait gave up");
+    if (status & RB_DEV_BAD_TABLE) return fail(ctx, RB_ERR_INVALID, "singular cell system or bad table");
+    return RB_OK;
+}
+
+int32_t rb_release(rb_context *ctx, rb_handle hd) {
+    if (!ctx) return RB_ERR_INVALID;
+    auto it = ctx->probs.find(hd);
+    if (it == ctx->probs.end()) return fail(ctx, RB_ERR_NOT_FOUND, "unknown problem handle %lld", (long long)hd);
+    if (it->second->stream) cudaStreamSynchronize(it->second->stream);
+    cudaFree(it->second->block);
+    ctx->used -= it->second->bytes;
+    ctx->probs.erase(it);
+    return RB_OK;
+}
+
+int32_t rb_compute_flux(int32_t device, const rb_sn_problem *prob, rb_sn_result *res) {
+    rb_context *ctx = nullptr;
+    int st = rb_create(device, 0, &ctx);
+    if (st) return st;
+    rb_handle h = 0;
+    st = rb_upload(ctx, prob, &h);
+    if (!st) st = rb_solve(ctx, h, nullptr);
+    if (!st) st = rb_download(ctx, h, res);
+    if (st) g_create_error = ctx->err;
+    rb_destroy(ctx);
+    return st;
+}
+
+int32_t rb_submit(rb_context *ctx, const rb_sn_problem *prob, rb_handle *out) {
+    int st = rb_upload(ctx, prob, out);
+    if (st) return st;
+    return rb_solve(ctx, *out, nullptr);
+}
+
+int32_t rb_poll(rb_context *ctx, rb_handle hd, rb_sn_result *res) {
+    if (!ctx) return RB_ERR_INVALID;
+    ProblemRec *r = find(ctx, hd);
+    if (!r) return fail(ctx, RB_ERR_NOT_FOUND, "unknown request %lld", (long long)hd);
+    cudaError_t q = cudaStreamQuery(r->stream);
+    if (q == cudaErrorNotReady) return RB_ERR_NOT_READY;
+    int st = rb_download(ctx, hd, res);
+    rb_release(ctx, hd);
+    return st;
+}
+
+int32_t rb_energy_deposition(int32_t ng, int32_t np, int32_t nm5, int64_t ncell, int32_t nmat,
+                             const int32_t *mat, const double *flux, const double *flux_cutoff,
+                             const double *sigma_e, const double *density, double norm, double *dep) {
+    // energy_deposition.jl:58-76: a reduction over groups per voxel; small, done on the host
+    // from the downloaded flux (it is outside the transport solve).
+    if (!mat || !flux || !sigma_e || !density || !dep) return fail(nullptr, RB_ERR_INVALID, "null argument");
+    for (int64_t c = 0; c < ncell; c++) {
+        int m = mat[c] - 1;
+        if (m < 0 || m >= nmat) return fail(nullptr, RB_ERR_INVALID, "mat[%lld] out of range", (long long)c);
+        double d = 0.0;
+        for (int g = 0; g < ng; g++) d += sigma_e[g + (int64_t)(ng + 1) * m] * flux[g + (int64_t)ng * ((int64_t)np * nm5 * c)];
+        if (flux_cutoff) d += sigma_e[ng + (int64_t)(ng + 1) * m] * flux_cutoff[(int64_t)np * nm5 * c];
+        dep[c] = d / (density[m] * norm);
+    }
+    return RB_OK;
+}
+
+}  // extern "C"

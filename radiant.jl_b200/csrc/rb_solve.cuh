@@ -1,0 +1,499 @@
+// rb_solve.cuh -- in-group accelerators and the group loop, run by one team per problem.
+//
+// Restates on the device: livolant! (src/tools/livolant.jl:110-154), anderson!
+// (src/tools/anderson.jl:38-140), gmres! (src/tools/gmres.jl:35-133), bicgstab!
+// (src/tools/bicgstab.jl:30-101), sn_one_speed (sn_one_speed.jl:81-195) and the group loop of
+// compute_flux(::SN) (sn_flux.jl:146-224). Every scalar decision (convergence tests,
+// Hessenberg, Givens, Anderson normal equations) is taken from team reductions whose bits
+// are identical in every thread, so the team's threads always branch together.
+#pragma once
+#include <math_constants.h>
+
+#include "rb_kernels.cuh"
+
+namespace rb {
+
+struct SolveStat {
+    int iter;
+    double resid;
+    int conv;
+    double rho;
+};
+
+__device__ __forceinline__ double rho_estimate(double r0, double r, int it) {  // krylov_state.jl:139-144
+    if (it > 1 && r0 > 0.0 && r > 0.0) return pow(r / r0, 1.0 / (it - 1));
+    return CUDART_NAN;
+}
+
+// One problem in flight on one team.
+template <class Team>
+struct Solver {
+    const Team &t;
+    const DevProblem &P;
+    GroupShared &gs;
+    int ig;
+    const double *phiE_in;
+    double *phiE_out;
+    long long npass;
+
+    __device__ double *vec(int k) const { return P.vecs + (long long)k * P.nstate; }
+
+    // load_and_pass! (sn_one_speed.jl:138-143): out <- T(zin) or A·zin
+    __device__ void pass(const double *zin, double *out, int homog) {
+        pass1d(t, P, gs, zin, out, homog, ig, phiE_in, phiE_out);
+        npass++;
+    }
+    __device__ void fixedpoint(double *out, const double *zin) { pass(zin, out, 0); }
+    // matvec! : out <- zin - A·zin
+    __device__ void matvec(double *out, const double *zin) {
+        pass(zin, out, 1);
+        vlin(t, 1.0, zin, -1.0, out, P.nstate);
+    }
+    __device__ double norm(const double *a) { return sqrt(vdot(t, a, a, P.nstate)); }
+
+    // ---------------------------------------------------------------- livolant (and "none")
+    __device__ SolveStat livolant(double *z, int maxit, double tol, int period) {
+        const long long N = P.nstate;
+        double *g = vec(1), *f = vec(2), *z1 = vec(3), *z0 = vec(4);
+        vzero(t, z1, N); vzero(t, z0, N);
+        int nhist = 0, iter = 0, conv = 0;
+        double resid = 1.0, resid0 = CUDART_NAN;
+        for (int it = 1; it <= maxit; it++) {
+            fixedpoint(g, z); iter++;
+            // f = g - z (state_copy!(f,g); state_axpy!(-1,z,f))
+            for (long long i = t.rank(); i < N; i += t.size()) f[i] = g[i] + (-1.0) * z[i];
+            t.sync();
+            double fnorm = norm(f);
+            double scale = fmax(norm(g), 1e-16);
+            resid = fnorm / scale;
+            if (isnan(resid0)) resid0 = resid;
+            if (resid < tol) { vcopy(t, z, g, N); conv = 1; break; }
+            if (period > 0 && it % period == 0 && nhist >= 2) {
+                double se = 0.0, sd = 0.0;
+                for (long long i = t.rank(); i < N; i += t.size()) {
+                    double e0 = z1[i] - z0[i], e1 = g[i] - z1[i], de = e1 - e0;
+                    se += e0 * de; sd += de * de;
+                }
+                se = t.sum(se); sd = t.sum(sd);
+                double mu = 1.0;
+                if (sd != 0.0) { mu = -se / sd; if (mu <= 0) mu = 1.0; }
+                for (long long i = t.rank(); i < N; i += t.size()) z[i] = g[i] * mu + (1.0 - mu) * z1[i];
+                t.sync();
+            } else {
+                vcopy(t, z, g, N);
+            }
+            vcopy(t, z0, z1, N); vcopy(t, z1, g, N); nhist++;
+        }
+        SolveStat s = {iter, resid, conv, rho_estimate(resid0, resid, iter)};
+        return s;
+    }
+
+    // ---------------------------------------------------------------- anderson (β = 1)
+    __device__ SolveStat anderson(double *z, int depth, int maxit, double tol) {
+        const long long N = P.nstate;
+        const int m = depth > 1 ? depth : 1;
+        double *g = vec(1), *f = vec(2), *fo = vec(3), *go = vec(4);
+        // history ring: logical i -> slot (head + i) % m; dF slot s = vec(5+s), dG = vec(5+m+s)
+        int nh = 0, head = 0, iter = 0, conv = 0;
+        double resid = 1.0, resid0 = CUDART_NAN;
+        for (int it = 1; it <= maxit; it++) {
+            fixedpoint(g, z); iter++;
+            for (long long i = t.rank(); i < N; i += t.size()) f[i] = g[i] + (-1.0) * z[i];
+            t.sync();
+            double fnorm = norm(f);
+            double scale = fmax(fmax(norm(z), norm(g)), 1e-16);
+            resid = fnorm / scale;
+            if (isnan(resid0)) resid0 = resid;
+            if (resid < tol) { conv = 1; break; }
+            if (it == 1) {
+                vaxpy(t, 1.0, f, z, N);
+            } else {
+                if (nh == m) { head = (head + 1) % m; nh--; }  // popfirst!
+                int slot = (head + nh) % m;
+                double *dF = vec(5 + slot), *dG = vec(5 + m + slot);
+                for (long long i = t.rank(); i < N; i += t.size()) {
+                    dF[i] = f[i] + (-1.0) * fo[i];
+                    dG[i] = g[i] + (-1.0) * go[i];
+                }
+                t.sync();
+                nh++;
+                const int mk = nh;
+                for (int i = 0; i < mk; i++) {
+                    const double *dFi = vec(5 + (head + i) % m);
+                    double bi = vdot(t, dFi, f, N);
+                    if (t.rank() == 0) gs.b[i] = bi;
+                    for (int j = 0; j < mk; j++) {
+                        double aij = vdot(t, dFi, vec(5 + (head + j) % m), N);
+                        if (t.rank() == 0) gs.A[i + mk * j] = aij;
+                    }
+                }
+                t.sync();
+                if (t.rank() == 0) {
+                    double *A = gs.A, *x = gs.b;
+                    double tr = 0.0;
+                    for (int i = 0; i < mk; i++) tr += A[i + mk * i];
+                    double lam = 1e-12 * (tr / mk + 1e-300);
+                    for (int i = 0; i < mk; i++) A[i + mk * i] += lam;
+                    // anderson_solve (anderson.jl:112-140)
+                    const int n = mk;
+                    for (int k = 0; k < n; k++) {
+                        int p = k; double mx = fabs(A[k + n * k]);
+                        for (int i = k + 1; i < n; i++) if (fabs(A[i + n * k]) > mx) { mx = fabs(A[i + n * k]); p = i; }
+                        if (p != k) {
+                            for (int j = k; j < n; j++) { double tt = A[k + n * j]; A[k + n * j] = A[p + n * j]; A[p + n * j] = tt; }
+                            double tt = x[k]; x[k] = x[p]; x[p] = tt;
+                        }
+                        double piv = A[k + n * k];
+                        if (piv == 0.0) continue;
+                        for (int i = k + 1; i < n; i++) {
+                            double fac = A[i + n * k] / piv;
+                            for (int j = k; j < n; j++) A[i + n * j] -= fac * A[k + n * j];
+                            x[i] -= fac * x[k];
+                        }
+                    }
+                    for (int k = n - 1; k >= 0; k--) {
+                        double s = x[k];
+                        for (int j = k + 1; j < n; j++) s -= A[k + n * j] * x[j];
+                        x[k] = A[k + n * k] != 0.0 ? s / A[k + n * k] : 0.0;
+                    }
+                }
+                t.sync();
+                vaxpy(t, 1.0, f, z, N);
+                for (int i = 0; i < mk; i++) {
+                    const double gam = gs.b[i];
+                    vaxpy(t, -gam, vec(5 + m + (head + i) % m), z, N);
+                    // β - 1 = 0: the ΔF term adds -(0)·γ·ΔF, kept for operation parity
+                    vaxpy(t, -(1.0 - 1.0) * gam, vec(5 + (head + i) % m), z, N);
+                }
+            }
+            vcopy(t, fo, f, N); vcopy(t, go, g, N);
+        }
+        SolveStat s = {iter, resid, conv, rho_estimate(resid0, resid, iter)};
+        return s;
+    }
+
+    // ---------------------------------------------------------------- gmres(m)
+    __device__ SolveStat gmres(double *z, const double *rhs, int restart, int maxit, double tol) {
+        const long long N = P.nstate;
+        const int m = restart > 1 ? restart : 1;
+        SolveStat st = {0, 0.0, 1, CUDART_NAN};
+        double bnorm = norm(rhs);
+        if (bnorm == 0.0) { vzero(t, z, N); return st; }
+        double *r = vec(2), *w = vec(3);
+        double *H = gs.H;
+#define HH(i, j) H[(i) + (m + 1) * (j)]
+        int iter = 0, conv = 0;
+        double resid = 1.0, resid0 = CUDART_NAN;
+        while (iter < maxit && !conv) {
+            matvec(r, z); iter++;
+            vlin(t, 1.0, rhs, -1.0, r, N);  // r = c - M z
+            double beta = norm(r);
+            resid = beta / bnorm;
+            if (isnan(resid0)) resid0 = resid;
+            if (resid < tol) { conv = 1; break; }
+            {
+                double inv = 1.0 / beta;
+                double *V0 = vec(4);
+                for (long long i = t.rank(); i < N; i += t.size()) V0[i] = r[i] * inv;
+            }
+            if (t.rank() == 0) {
+                for (int i = 0; i <= m; i++) gs.g[i] = 0.0;
+                gs.g[0] = beta;
+            }
+            t.sync();
+            int k = 0;
+            for (int j = 0; j < m; j++) {
+                if (iter >= maxit) break;
+                matvec(w, vec(4 + j)); iter++;
+                for (int i = 0; i <= j; i++) {  // modified Gram-Schmidt
+                    double h = vdot(t, w, vec(4 + i), N);
+                    if (t.rank() == 0) HH(i, j) = h;
+                    vaxpy(t, -h, vec(4 + i), w, N);
+                }
+                double hjp1 = norm(w);
+                if (hjp1 > 0.0) {
+                    double inv = 1.0 / hjp1;
+                    double *Vn = vec(4 + j + 1);
+                    for (long long i = t.rank(); i < N; i += t.size()) Vn[i] = w[i] * inv;
+                }
+                if (t.rank() == 0) {
+                    HH(j + 1, j) = hjp1;
+                    for (int i = 0; i < j; i++) {
+                        double temp = gs.cs[i] * HH(i, j) + gs.sn[i] * HH(i + 1, j);
+                        HH(i + 1, j) = -gs.sn[i] * HH(i, j) + gs.cs[i] * HH(i + 1, j);
+                        HH(i, j) = temp;
+                    }
+                    double denom = hypot(HH(j, j), HH(j + 1, j));
+                    if (denom == 0.0) { gs.cs[j] = 1.0; gs.sn[j] = 0.0; }
+                    else { gs.cs[j] = HH(j, j) / denom; gs.sn[j] = HH(j + 1, j) / denom; }
+                    HH(j, j) = gs.cs[j] * HH(j, j) + gs.sn[j] * HH(j + 1, j);
+                    HH(j + 1, j) = 0.0;
+                    gs.g[j + 1] = -gs.sn[j] * gs.g[j];
+                    gs.g[j] = gs.cs[j] * gs.g[j];
+                }
+                t.sync();
+                k = j + 1;
+                resid = fabs(gs.g[j + 1]) / bnorm;
+                if (resid < tol) { conv = 1; break; }
+                if (hjp1 == 0.0) break;
+            }
+            if (t.rank() == 0) {
+                for (int i = k - 1; i >= 0; i--) {
+                    double s = gs.g[i];
+                    for (int l = i + 1; l < k; l++) s -= HH(i, l) * gs.y[l];
+                    gs.y[i] = HH(i, i) != 0.0 ? s / HH(i, i) : 0.0;
+                }
+            }
+            t.sync();
+            for (int i = 0; i < k; i++) vaxpy(t, gs.y[i], vec(4 + i), z, N);
+            if (conv) break;
+        }
+#undef HH
+        st.iter = iter; st.resid = resid; st.conv = conv; st.rho = rho_estimate(resid0, resid, iter);
+        return st;
+    }
+
+    // ---------------------------------------------------------------- bicgstab
+    __device__ SolveStat bicgstab(double *z, const double *rhs, int maxit, double tol) {
+        const long long N = P.nstate;
+        SolveStat st = {0, 0.0, 1, CUDART_NAN};
+        double bnorm = norm(rhs);
+        if (bnorm == 0.0) { vzero(t, z, N); return st; }
+        double *r = vec(2), *rh = vec(3), *p = vec(4), *v = vec(5), *s = vec(6), *tt = vec(7);
+        matvec(r, z);
+        vlin(t, 1.0, rhs, -1.0, r, N);
+        int iter = 1, conv = 0;
+        double resid = norm(r) / bnorm, resid0 = resid;
+        if (resid < tol) { st.iter = iter; st.resid = resid; st.conv = 1; st.rho = CUDART_NAN; return st; }
+        vcopy(t, rh, r, N);
+        vzero(t, p, N); vzero(t, v, N);
+        double rho_old = 1.0, alpha = 1.0, omega = 1.0;
+        const double tiny = 1e-300;
+        while (iter < maxit) {
+            double rho_new = vdot(t, rh, r, N);
+            if (fabs(rho_new) < tiny) break;
+            double beta = (rho_new / rho_old) * (alpha / omega);
+            // p ← r + β (p − ω v)
+            for (long long i = t.rank(); i < N; i += t.size()) p[i] = r[i] + 1.0 * (beta * (p[i] + (-omega) * v[i]));
+            t.sync();
+            matvec(v, p); iter++;
+            double denom = vdot(t, rh, v, N);
+            if (fabs(denom) < tiny) break;
+            alpha = rho_new / denom;
+            for (long long i = t.rank(); i < N; i += t.size()) s[i] = r[i] + (-alpha) * v[i];
+            t.sync();
+            double sn_ = norm(s);
+            if (sn_ / bnorm < tol) {
+                vaxpy(t, alpha, p, z, N);
+                resid = sn_ / bnorm;
+                conv = 1;
+                break;
+            }
+            matvec(tt, s); iter++;
+            double ttd = vdot(t, tt, tt, N);
+            if (ttd < tiny) break;
+            omega = vdot(t, tt, s, N) / ttd;
+            for (long long i = t.rank(); i < N; i += t.size()) {
+                z[i] = (z[i] + alpha * p[i]) + omega * s[i];
+                r[i] = s[i] + (-omega) * tt[i];
+            }
+            t.sync();
+            resid = norm(r) / bnorm;
+            if (resid < tol) { conv = 1; break; }
+            if (fabs(omega) < tiny) break;
+            rho_old = rho_new;
+        }
+        st.iter = iter; st.resid = resid; st.conv = conv; st.rho = rho_estimate(resid0, resid, iter);
+        return st;
+    }
+
+    // ---------------------------------------------------------------- sn_one_speed
+    __device__ SolveStat one_speed(double *flux_g) {
+        const long long N = P.nstate, nphi = P.nphi;
+        const long long nE = (long long)P.nd * P.nm4 * P.ncell;
+        // zero-source short-circuit (sn_one_speed.jl:115-120)
+        int any = 0;
+        for (int f = 0; f < 2 * P.ndims; f++) {
+            const double *src = P.surf[f];
+            if (!src) continue;
+            long long fc = P.ndims == 1 ? 1 : 0;  // 1D faces hold one cell
+            for (long long k = t.rank(); k < (long long)P.np_source * fc; k += t.size())
+                if (src[ig + (long long)P.ng * k] != 0.0) any = 1;
+        }
+        for (long long i = t.rank(); i < nphi; i += t.size()) if (P.qlout[i] != 0.0) any = 1;
+        if (P.csd) for (long long i = t.rank(); i < nE; i += t.size()) if (phiE_in[i] != 0.0) any = 1;
+        any = t.any(any);
+        if (!any) {
+            vzero(t, flux_g, nphi);
+            if (P.csd) vzero(t, phiE_out, nE);
+            SolveStat s = {1, 0.0, 1, CUDART_NAN};
+            return s;
+        }
+        double *z = vec(0);
+        vzero(t, z, N);  // initial state (𝚽l of the group = 0, boundary in-moments = 0)
+        SolveStat st;
+        if (P.accel == 0 || P.accel == 1) {
+            st = livolant(z, P.maxit, P.tol, P.accel == 0 ? 0 : 3);
+        } else if (P.accel == 2) {
+            st = anderson(z, P.depth, P.maxit, P.tol);
+        } else {
+            double *rhs = vec(1);
+            pass(z, rhs, 0);  // c = T(0)
+            if (P.accel == 3) st = gmres(z, rhs, P.restart, P.maxit, P.tol);
+            else st = bicgstab(z, rhs, P.maxit, P.tol);
+        }
+        // reconstruction pass (sn_one_speed.jl:184-187)
+        double *out = vec(1);
+        pass(z, out, 0);
+        vcopy(t, flux_g, out, nphi);
+        return st;
+    }
+};
+
+// ------------------------------------------------------------------------------------------
+// the group loop of compute_flux(::SN) for one problem (sn_flux.jl:146-224)
+// ------------------------------------------------------------------------------------------
+template <class Team>
+__device__ void solve_problem(const Team &t, const DevProblem &P, GroupShared &gs) {
+    const int ng = P.ng, nmat = P.nmat, np = P.np, nd = P.nd, nm = P.nm5;
+    const long long nphi = P.nphi, ncell = P.ncell;
+    const long long nE = (long long)nd * P.nm4 * ncell;
+    const int st_ = P.solver_type;
+    double *phiE_in = P.phiE_a, *phiE_out = P.phiE_b;
+    if (P.csd) { vzero(t, phiE_in, nE); vzero(t, phiE_out, nE); }
+    long long npass = 0;
+    for (int ig = 0; ig < ng; ig++) {
+        // per-group constants
+        for (int m = t.rank(); m < nmat; m += t.size()) {
+            gs.sigt[m] = P.sigma_t[ig + (long long)ng * m];
+            if (P.csd) {
+                const double dE = P.e_width[ig];
+                gs.sm[m] = P.s_minus[ig + (long long)ng * m] / dE;
+                gs.sp[m] = P.s_plus[ig + (long long)ng * m] / dE;
+            } else {
+                gs.sm[m] = gs.sp[m] = 0.0;
+            }
+            gs.tg[m] = (st_ == 2 || st_ == 4) ? P.t_mom[ig + (long long)ng * m] : 0.0;
+        }
+        t.sync();
+        if (P.csd) {  // CSD block of the cell matrix: Σ_w (S_w/ΔE)·K_w + (S⁺/ΔE)·B
+            const int nn = nm * nm;
+            for (long long o = t.rank(); o < (long long)nmat * nn; o += t.size()) {
+                const int m = (int)(o / nn), e = (int)(o % nn);
+                const double dE = P.e_width[ig];
+                double v = gs.sp[m] * P.Bcsd[e];
+                for (int w = 0; w < P.oE; w++)
+                    v += (P.s_mom[ig + (long long)ng * (m + (long long)nmat * w)] / dE) * P.Kcsd[(long long)w * nn + e];
+                P.scsd[o] = v;
+            }
+        }
+        // K[m][n][p] = Mn[n,p]·Σs_in[m,pl[p]] + T[m]·(Mn·ℳ)[n,p]
+        const bool scat = (st_ != 4 && st_ != 5 && st_ != 6);
+        for (long long o = t.rank(); o < (long long)nmat * nd * np; o += t.size()) {
+            const int p = (int)(o % np);
+            const int n = (int)((o / np) % nd);
+            const int m = (int)(o / ((long long)np * nd));
+            double v = 0.0;
+            if (scat) {
+                const double sv = P.sigma_s[m + (long long)nmat * (ig + (long long)ng * (ig + (long long)ng * P.pl[p]))];
+                v = P.mn[n + (long long)nd * p] * sv;
+            }
+            if (P.mnfp) v += gs.tg[m] * P.mnfp[n + (long long)nd * p];
+            P.kmat[o] = v;
+        }
+        // Qlout = Σ_{gi≠ig} Σs[mat,gi,ig,l]·𝚽[gi] + volume source (scattering_source.jl:59-68;
+        // groups above ig are still zero in the single outer iteration, sn_flux.jl:150,157)
+        for (long long o = t.rank(); o < nphi; o += t.size()) {
+            const int p = (int)(o % np);
+            const long long c = o / ((long long)np * nm);
+            const int m = P.mat[c];
+            double q = 0.0;
+            if (st_ != 4 && st_ != 5) {
+                for (int gi = 0; gi < ig; gi++)
+                    q += P.sigma_s[m + (long long)nmat * (gi + (long long)ng * (ig + (long long)ng * P.pl[p]))] *
+                         P.flux[(long long)gi * nphi + o];
+            }
+            if (P.vol) q += P.vol[(long long)ig * nphi + o];
+            P.qlout[o] = q;
+        }
+        if (P.csd && ig != 0) {  // 𝚽E12 .* ΔE[ig] / ΔE[ig-1]
+            const double r1 = P.e_width[ig], r0 = P.e_width[ig - 1];
+            for (long long i = t.rank(); i < nE; i += t.size()) phiE_in[i] = phiE_in[i] * r1 / r0;
+        }
+        t.sync();
+        // Mn·Qlout
+        const long long nq = (long long)nd * nm * ncell;
+        for (long long o = t.rank(); o < nq; o += t.size()) {
+            const int n = (int)(o % nd);
+            const long long r = o / nd;
+            double s = 0.0;
+            for (int p = 0; p < np; p++) s += P.mn[n + (long long)nd * p] * P.qlout[p + (long long)np * r];
+            P.qnout[o] = s;
+        }
+        t.sync();
+        Solver<Team> S{t, P, gs, ig, phiE_in, phiE_out, 0};
+        SolveStat s = S.one_speed(P.flux + (long long)ig * nphi);
+        npass += S.npass;
+        if (t.rank() == 0) {
+            P.rho[ig] = s.rho; P.resid[ig] = s.resid; P.iters[ig] = s.iter; P.conv[ig] = s.conv;
+            if (!s.conv) atomicOr(P.status, RB_DEV_NOT_CONVERGED);
+        }
+        double *tmp = phiE_in; phiE_in = phiE_out; phiE_out = tmp;
+        t.sync();
+    }
+    // 𝚽cutoff[p,is,c] = Σ_n Dn[p,n]·𝚽E12[n,is,c] for is < Nm4 (sn_flux.jl:215-218)
+    if (P.csd) {
+        for (long long o = t.rank(); o < nphi; o += t.size()) {
+            const int p = (int)(o % np);
+            const int is = (int)((o / np) % nm);
+            const long long c = o / ((long long)np * nm);
+            double s = 0.0;
+            if (is < P.nm4)
+                for (int n = 0; n < nd; n++)
+                    s += P.dn[p + (long long)np * n] * phiE_in[n + (long long)nd * (is + (long long)P.nm4 * c)];
+            P.cutoff[o] = s;
+        }
+    }
+    if (t.rank() == 0) *P.passes = npass;
+    t.sync();
+}
+
+// ------------------------------------------------------------------------------------------
+// persistent batch kernel: CTAs pull problems from a device work queue
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(RB_THREADS) solve_batch_kernel(DevProblem *const *probs, int nprob,
+                                                                 int *queue) {
+    __shared__ GroupShared gs;
+    __shared__ int next;
+    CtaTeam t{gs.red};
+    while (true) {
+        if (threadIdx.x == 0) next = atomicAdd(queue, 1);
+        __syncthreads();
+        const int idx = next;
+        __syncthreads();
+        if (idx >= nprob) break;
+        const DevProblem *pp = probs[idx];
+        solve_problem(t, *pp, gs);
+    }
+}
+
+// [ng][nphi] (group-major) -> [ng, nphi] (group fastest, the reference's layout)
+__global__ void to_reference_layout(const double *__restrict__ src, double *__restrict__ dst, int ng,
+                                    long long nphi) {
+    __shared__ double tile[32][33];
+    const long long k0 = (long long)blockIdx.x * 32;
+    const int g0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int g = g0 + j;
+        const long long k = k0 + threadIdx.x;
+        if (g < ng && k < nphi) tile[j][threadIdx.x] = src[(long long)g * nphi + k];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const long long k = k0 + j;
+        const int g = g0 + threadIdx.x;
+        if (g < ng && k < nphi) dst[(long long)ng * k + g] = tile[threadIdx.x][j];
+    }
+}
+
+}  // namespace rb

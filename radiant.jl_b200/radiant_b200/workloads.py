@@ -1,0 +1,172 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+
+Radiant.jl generates multigroup cross sections from physics models and bundled data
+(src/cross_sections/*). That generator stays outside this library, and it cannot run
+where this library is built, so the workloads below use synthetic tables with the same
+shapes (groups, materials, Legendre orders) and physically shaped values:
+Σt ~ U(0.05, 5)/cm smooth in the group, downscatter-only Σs₀ whose row sums are c·Σt with
+c ~ U(0.3, 0.95), Henyey-Greenstein moments Σs_l = Σs₀·g^l with g ~ U(0.3, 0.9)
+(Radiant's Mn already carries the (2l+1)/2 factor, so the moments carry none), and positive stopping powers
+and momentum transfer smooth in the group. Every table is labelled synthetic.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import tables as T
+from .sn_flux import MultigroupXS, SNSettings, prepare_sn_tables
+
+
+def log_groups(ng: int, e_top: float, e_cut: float):
+    """Log-spaced group boundaries, highest energy first (the reference's group order)."""
+    eb = np.exp(np.linspace(math.log(e_top), math.log(e_cut), ng + 1))
+    e = np.sqrt(eb[:-1] * eb[1:])
+    return eb, e, eb[:-1] - eb[1:]
+
+
+def synthetic_xs(ng: int, nmat: int, L: int, seed: int, csd: bool = False,
+                 e_top: float = 2.0, e_cut: float = 0.01, scale: float = 1.0) -> MultigroupXS:
+    """Synthetic multigroup tables of one particle (labelled synthetic)."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(ng)
+    sigma_t = np.zeros((ng, nmat))
+    sigma_s = np.zeros((nmat, ng, ng, L + 1))
+    t_mom = np.zeros((ng, nmat))
+    sb = np.zeros((ng + 1, nmat))
+    sigma_e = np.zeros((ng + 1, nmat))
+    density = np.zeros(nmat)
+    for m in range(nmat):
+        lo, hi = sorted(rng.uniform(0.05, 5.0, size=2))
+        ramp = np.linspace(0.0, 1.0, ng) ** rng.uniform(0.5, 2.0)
+        sigma_t[:, m] = scale * (lo + (hi - lo) * ramp)
+        c = rng.uniform(0.3, 0.95)
+        aniso = rng.uniform(0.3, 0.9)
+        for gi in range(ng):
+            # downscatter-only row gi -> gf >= gi, geometric fall-off, row sum c·Σt
+            k = np.arange(ng - gi)
+            prof = np.exp(-k * rng.uniform(0.5, 2.0))
+            prof /= prof.sum()
+            row = c * sigma_t[gi, m] * prof
+            for l in range(L + 1):
+                sigma_s[m, gi, gi:, l] = row * aniso ** l
+        density[m] = rng.uniform(0.3, 2.0)
+        if csd:
+            s0 = rng.uniform(1.5, 2.5)
+            sb[:, m] = s0 * (1.0 + 0.5 * np.linspace(0.0, 1.0, ng + 1))
+            t_mom[:, m] = rng.uniform(0.05, 0.5) * (1.0 + np.linspace(0.0, 2.0, ng))
+        sigma_e[:ng, m] = rng.uniform(0.01, 0.1) * (1.0 + g / ng)
+        sigma_e[ng, m] = rng.uniform(0.5, 1.5)
+    eb, e, de = log_groups(ng, e_top, e_cut)
+    return MultigroupXS(sigma_t=sigma_t, sigma_s=sigma_s, sigma_a=sigma_t * 0.2, sb=sb if csd else None,
+                        t_mom=t_mom if csd else None, sigma_e=sigma_e, e_width=de, energies=e, e_bounds=eb,
+                        density=density)
+
+
+def surface_source_1d(tabs_np_surf_L: int, L_solver: int, btype: str, Om, w, ng: int, group: int,
+                      mu_s: float, intensity: float = 1.0, surface: str = "X-"):
+    """Moments of a monodirectional 1D surface beam (surface_source.jl:64-96, Qdims == 1).
+    Returns (Q [ng, Np_src, 2 faces], normalisation)."""
+    L = min(tabs_np_surf_L, L_solver)
+    Np, _, _, _, _, pl, _ = T.surface_angular_polynomial_basis_face(Om, w, L, btype, 1, surface)
+    Lmax = int(np.max(pl))
+    Pls = T.half_range_legendre_polynomials_up_to_L(Lmax, abs(mu_s))
+    Q = np.zeros((ng, Np, 2))
+    for p in range(Np):
+        l = pl[p]
+        if surface == "X-" and mu_s > 0:
+            Q[group, p, 0] = intensity * Pls[l]
+        elif surface == "X+" and mu_s < 0:
+            Q[group, p, 1] = intensity * Pls[l]
+    return Q, intensity
+
+
+def slab_tables(nx: int, widths, mats, ng: int, nmat: int, seed: int, sn: SNSettings, L_xs: int,
+                beam_group: int = 0, bc=(0, 0), volume_group=None, csd=False, precision="fp64",
+                xs: MultigroupXS | None = None, beam_mu: float = 1.0):
+    """A 1D slab: `mats` gives the material id (1-based) of each voxel, `widths` its width."""
+    xs = xs or synthetic_xs(ng, nmat, L_xs, seed, csd=csd)
+    Qdims = sn.qdims(1)
+    Om, w = T.quadrature(sn.quadrature_order, sn.quadrature_type, 1, Qdims)
+    surf = None
+    if beam_group is not None:
+        Q, _ = surface_source_1d(64, sn.legendre_order, sn.angular_boltzmann, [Om, 0 * Om, 0 * Om], w, ng,
+                                 beam_group, beam_mu)
+        surf = [Q[:, :, 0:1], Q[:, :, 1:2]]
+    vol = None
+    if volume_group is not None:
+        vol = np.zeros((ng, 1, 1, nx, 1, 1))
+        vol[volume_group, 0, 0, :, 0, 0] = 1.0
+    tabs = prepare_sn_tables(xs, 1, [nx], [np.asarray(widths, dtype=float)], np.asarray(mats).reshape(nx, 1, 1),
+                             list(bc) + [0] * 4, sn, volume_sources=vol, surface_sources=surf, precision=precision)
+    tabs["xs"] = xs
+    return tabs
+
+
+def c1_tables(seed: int = 1, precision: str = "fp64", accel: str = "gmres"):
+    """1D slab BTE, photons: 10 cm, 200 voxels, void/void, 40 groups, S16 Gauss-Legendre,
+    P7, diamond difference, GMRES to 1e-8, normal beam at x=0 in the top group."""
+    sn = SNSettings(solver_type="BTE", quadrature_type="gauss-legendre", quadrature_order=16,
+                    legendre_order=7, scheme_type={"x": "DD"}, scheme_order={"x": 1},
+                    acceleration=accel, convergence_criterion=1e-8)
+    nx = 200
+    return slab_tables(nx, np.full(nx, 10.0 / nx), np.ones(nx, dtype=np.int32), 40, 1, seed, sn, 7,
+                       precision=precision)
+
+
+def c2_tables(seed: int = 1, precision: str = "fp64", accel: str = "gmres", particle: str = "electron"):
+    """1D slab BFP: water 0-3 cm / bone 3-5 cm / water 5-15 cm, 300 voxels of 0.05 cm,
+    80 groups, S32 Gauss-Legendre, P15, linear DG in x and in E, Galerkin (moment-preserving)
+    angular Fokker-Planck, normal beam in the group holding 6 MeV."""
+    nx = 300
+    mats = np.ones(nx, dtype=np.int32)
+    mats[60:100] = 2
+    ng = 80
+    eb, e, de = log_groups(ng, 20.0, 0.001)
+    g6 = int(np.nonzero((eb[:-1] >= 6.0) & (eb[1:] < 6.0))[0][0])
+    if particle == "photon":
+        sn = SNSettings(solver_type="BTE", quadrature_type="gauss-legendre", quadrature_order=32,
+                        legendre_order=15, scheme_type={"x": "DG"}, scheme_order={"x": 2},
+                        acceleration=accel, convergence_criterion=1e-8)
+        csd = False
+    else:
+        sn = SNSettings(solver_type="BFP", quadrature_type="gauss-legendre", quadrature_order=32,
+                        legendre_order=15, scheme_type={"x": "DG", "E": "DG"}, scheme_order={"x": 2, "E": 2},
+                        angular_fokker_planck="galerkin", acceleration=accel, convergence_criterion=1e-8)
+        csd = True
+    xs = synthetic_xs(ng, 2, 15, seed, csd=csd, e_top=20.0, e_cut=0.001)
+    return slab_tables(nx, np.full(nx, 0.05), mats, ng, 2, seed, sn, 15, beam_group=g6, csd=csd,
+                       precision=precision, xs=xs)
+
+
+def random_slab_tables(seed: int, precision: str = "fp64", max_cells: int = 2000, max_groups: int = 120):
+    """One 1D request of the serving stream: cells U(50, max_cells), groups U(10, max_groups),
+    SN order in {8,16,32,64}, P order U(1,9), 1-5 layers of 4 materials, photon (BTE) or
+    electron (BFP) with probability 1/2."""
+    rng = np.random.default_rng(seed)
+    nx = int(rng.integers(50, max_cells + 1))
+    ng = int(rng.integers(10, max_groups + 1))
+    N = int(rng.choice([8, 16, 32, 64]))
+    L = int(rng.integers(1, 10))
+    nlay = int(rng.integers(1, 6))
+    cuts = np.sort(rng.choice(np.arange(1, nx), size=nlay - 1, replace=False)) if nlay > 1 else []
+    mats = np.ones(nx, dtype=np.int32)
+    start = 0
+    for k, cpos in enumerate(list(cuts) + [nx]):
+        mats[start:cpos] = int(rng.integers(1, 5))
+        start = cpos
+    bfp = bool(rng.integers(0, 2))
+    if bfp:
+        sn = SNSettings(solver_type="BFP", quadrature_type="gauss-legendre", quadrature_order=N,
+                        legendre_order=L, scheme_type={"x": "DD", "E": "DD"}, scheme_order={"x": 1, "E": 1},
+                        angular_fokker_planck="galerkin", acceleration="gmres", convergence_criterion=1e-7,
+                        angular_boltzmann="standard")
+    else:
+        sn = SNSettings(solver_type="BTE", quadrature_type="gauss-legendre", quadrature_order=N,
+                        legendre_order=L, scheme_type={"x": "DD"}, scheme_order={"x": 1},
+                        acceleration="gmres", convergence_criterion=1e-7, angular_boltzmann="standard")
+    width = rng.uniform(2.0, 20.0)
+    xs = synthetic_xs(ng, 4, L, seed + 7919, csd=bfp)
+    return slab_tables(nx, np.full(nx, width / nx), mats, ng, 4, seed, sn, L, beam_group=0, csd=bfp,
+                       precision=precision, xs=xs)
