@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark of the SN transport solve: cell-direction-group updates per second.
+
+Workload (one step): a batch of independent 1D slab coupled-BFP particle solves with the
+shapes of the 1D coupled Boltzmann Fokker-Planck configuration -- water 0-3 cm / cortical
+bone 3-5 cm / water 5-15 cm, 300 voxels, 80 log groups 1 keV-20 MeV, S32 Gauss-Legendre,
+P15, linear DG in x (and in E for the charged particles), Galerkin angular Fokker-Planck,
+normal beam in the 6 MeV group -- one photon (BTE), one electron (BFP) and one positron
+(BFP) solve per seed, `--seeds` seeds. Cross sections are seeded synthetic tables with the
+configuration's shapes (the reference's physics generator is not available here).
+
+  value  updates/s over the batch, inputs resident in HBM, one persistent launch per step
+  e2e    the same through the C ABI with host buffers: upload (H2D) + solve + download (D2H)
+  unit   of work: one (cell, direction) visit inside one transport pass of one group;
+         updates = Σ passes × cells × directions, passes as counted by the reference.
+
+`--impl reference` times the oracle port of the reference's CPU solve (the reference is
+Julia, unavailable here) on all host cores over a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "radiant.jl_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "cell-dir-group updates/s"
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload_tables(seeds, precision):
+    from radiant_b200 import workloads as W
+
+    tabs = []
+    for s in seeds:
+        for part in ("photon", "electron", "positron"):
+            t = W.c2_tables(seed=s * 3 + {"photon": 0, "electron": 1, "positron": 2}[part], precision=precision,
+                            particle="photon" if part == "photon" else "electron")
+            t["particle"] = part
+            tabs.append(t)
+    return tabs
+
+
+def algorithmic_bytes(t, passes, w=8):
+    """Minimal HBM traffic of a fused pass (per pass: read Qlout and 𝚽, write 𝚽, the material
+    id; energy-face fluxes in and out for CSD) × passes."""
+    ncell = int(np.prod(t["ns"]))
+    nm5, np_, nd = t["nm"][4], t["np"], t["nd"]
+    b = ncell * (3 * np_ * nm5 * w + 4)
+    if t["solver_type"] >= 2:
+        b += ncell * nd * 2 * t["nm"][3] * w
+    return b * passes
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                parts = [p.strip() for p in out.stdout.strip().split(",")]
+                if len(parts) >= 7:
+                    self.samples.append(parts)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=6)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------
+def run_ours(args, rank, world):
+    import torch
+
+    from radiant_b200._abi import Context, PackedProblem, ResultBuffers
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    seeds = [1 + rank * 1000 + k for k in range(args.seeds)]
+    tabs = workload_tables(seeds, args.precision)
+    ctx = Context(dev, 0)
+    packs = [PackedProblem(t) for t in tabs]
+    handles = [ctx.upload(p) for p in packs]
+    # a dedicated stream: the library launches on it and the CUDA events are recorded on it
+    stream = torch.cuda.Stream(dev)
+    sptr = stream.cuda_stream
+    rbs = [ResultBuffers(p) for p in packs]
+
+    def step():
+        ctx.solve_batch(handles, sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # passes per problem (identical every step: the solve is deterministic)
+    for h, rb in zip(handles, rbs):
+        ctx.download(h, rb)
+    updates = sum(rb.passes * int(np.prod(t["ns"])) * t["nd"] for rb, t in zip(rbs, tabs))
+    abytes = sum(algorithmic_bytes(t, rb.passes, 8 if args.precision == "fp64" else 4) for rb, t in zip(rbs, tabs))
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = updates * world / (ms / 1e3)
+
+    # e2e through the C ABI with host buffers: upload + solve + download per step
+    h2d = sum(p_bytes(t) for t in tabs)
+    d2h = sum(rb.flux.nbytes + (rb.flux_cutoff.nbytes if rb.flux_cutoff is not None else 0)
+              + rb.rho.nbytes + rb.group_iters.nbytes + rb.group_resid.nbytes + rb.group_converged.nbytes
+              for rb in rbs)
+    for h in handles:
+        ctx.release(h)
+    e2e_steps = max(1, min(args.steps, 2))
+
+    def e2e_step():
+        hs = [ctx.upload(p) for p in packs]
+        ctx.solve_batch(hs, sptr)
+        for h, rb in zip(hs, rbs):
+            ctx.download(h, rb)
+        for h in hs:
+            ctx.release(h)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    ctx.close()
+
+    peak, pk = peaks()
+    achieved = abytes / (ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded cross-section tables with the configuration's shapes)",
+        "config": {"workload": "1D slab coupled BFP: 300 voxels (water/bone/water), 80 groups, S32, P15, "
+                               "linear DG in x and E, Galerkin angular FP, 6 MeV beam; photon+electron+positron "
+                               f"solves x {args.seeds} seeds per GPU", "problems_per_gpu": len(tabs),
+                   "precision": args.precision, "accel": "gmres(30)", "tol": 1e-8,
+                   "l2": "per-step working set (flux + Krylov vectors of every problem) exceeds the 126 MB L2",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": pk,
+                     "kernel": "solve_batch_kernel"},
+        "e2e": {"value": updates * world / (e2e_ms / 1e3), "unit": "updates/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    return line
+
+
+def p_bytes(t):
+    """Bytes of the host tables rb_upload copies for one problem."""
+    tot = 0
+    for k, v in t.items():
+        if isinstance(v, np.ndarray) and k not in ("w", "pm", "omega"):
+            tot += v.nbytes
+        elif isinstance(v, list):
+            tot += sum(a.nbytes for a in v if isinstance(a, np.ndarray))
+    return tot
+
+
+# ------------------------------------------------------------------------------------------
+# CPU legs (the oracle port of the reference's CPU solve)
+# ------------------------------------------------------------------------------------------
+def _cpu_one(args_):
+    seed, particle = args_
+    sys.path.insert(0, os.path.join(ROOT, "radiant.jl_b200"))
+    sys.path.insert(0, ROOT)
+    from oracle import run as orun
+    from radiant_b200 import workloads as W
+
+    t = W.c2_tables(seed=seed, particle="photon" if particle == "photon" else "electron")
+    t0 = time.perf_counter()
+    rb = orun.solve(t)
+    dt = time.perf_counter() - t0
+    return rb.passes * int(np.prod(t["ns"])) * t["nd"], dt
+
+
+def cpu_baseline_single():
+    """~10-15 s of single-thread CPU work: one photon and one electron solve."""
+    u1, t1 = _cpu_one((1, "photon"))
+    u2, t2 = _cpu_one((2, "electron"))
+    return {"value": (u1 + u2) / (t1 + t2), "unit": "updates/s", "cores": 1, "kind": "port",
+            "sample": "one photon (BTE) and one electron (BFP) solve of the workload, single thread, "
+                      f"{t1 + t2:.1f} s of CPU work"}
+
+
+def run_reference(args):
+    ncores = os.cpu_count() or 1
+    jobs = [(k + 1, "photon" if k % 3 == 0 else "electron") for k in range(ncores)]
+    ctxmp = mp.get_context("spawn")
+    with ctxmp.Pool(ncores) as pool:
+        for _ in range(args.warmup):
+            pool.map(_cpu_one, jobs[:ncores])
+        vals = []
+        t_all = 0.0
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_one, jobs)
+            dt = time.perf_counter() - t0
+            t_all += dt
+            vals.append(sum(u for u, _ in res) / dt)
+    value = statistics.mean(vals)
+    line = {
+        "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_all * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+        "data": "synthetic (seeded cross-section tables with the configuration's shapes)",
+        "config": {"workload": "1D slab coupled BFP (same shapes as our arm); one photon or electron solve "
+                               "per host core per step", "precision": "fp64"},
+        "cpu_baseline": {"value": value, "unit": "updates/s", "cores": ncores, "kind": "port",
+                         "sample": f"{len(jobs)} solves per step on {ncores} processes (C restatement of the "
+                                   "reference's Julia solve; Julia is not installed)"},
+        "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--seeds", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args)))
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    line = run_ours(args, rank, world)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_single()
+        print(json.dumps(line))
+    if world > 1:
+        import torch
+
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -436,6 +436,84 @@ ProblemRec *find(rb_context *ctx, rb_handle h) {
     return it == ctx->probs.end() ? nullptr : it->second.get();
 }
 
+// Lays one problem out in the device block `b` (offsets `o` from required()): fills the
+// device record `h`, queues the table copies on `s` and writes the record to *dptr.
+int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, const size_t *o, char *b,
+                  cudaStream_t s, DevProblem &h, DevProblem **dptr) {
+    memset(&h, 0, sizeof(h));
+    const int nd = P->nd, np = P->np, nm5 = D.M.nm, ng = P->ng, nmat = P->nmat;
+    h.ndims = P->ndims; h.nx = D.ns[0]; h.ny = D.ns[1]; h.nz = D.ns[2]; h.ncell = D.ncell;
+    h.nd = nd; h.np = np; h.nm5 = nm5;
+    for (int d = 0; d < 3; d++) h.nmf[d] = d < P->ndims ? P->nm[d] : 1;
+    h.nm4 = D.csd ? P->nm[3] : 1;
+    h.npsurf = P->np_surf; h.ng = ng; h.nmat = nmat; h.ls = P->ls; h.oE = P->order[3]; h.csd = D.csd;
+    h.solver_type = P->solver_type; h.accel = P->accel; h.maxit = P->max_iter; h.restart = P->gmres_restart;
+    h.depth = P->anderson_depth; h.precision = P->precision; h.tol = P->tol; h.np_source = P->np_source;
+    h.nphi = D.nphi; h.nstate = D.nstate;
+    for (int d = 0; d < 3; d++) { h.off_b[d] = D.off_b[d]; h.nb[d] = D.nb[d]; }
+    h.nvec = nvec_for(P);
+    for (int a = 0; a < 4; a++) h.w1[a] = D.w1[a];
+    for (int f = 0; f < 6; f++) h.bc[f] = P->bc[f];
+#define DP(T, k) (reinterpret_cast<T *>(b + o[k]))
+    h.dx = DP(double, 1); h.mat = DP(int, 2); h.cosv = DP(double, 3); h.mn = DP(double, 4); h.dn = DP(double, 5);
+    h.pl = DP(int, 6); h.mnfp = D.mnfp.empty() ? nullptr : DP(double, 7); h.frow_m = DP(double, 8);
+    h.frow_d = DP(double, 9); h.G = DP(double, 10); h.Gsrc = DP(double, 11); h.Gout = DP(double, 12);
+    h.tang = DP(int, 13); h.Kcsd = DP(double, 15); h.Bcsd = DP(double, 16);
+    h.EsA = DP(double, 14); h.EsB = h.EsA + D.EsA.size(); h.Eout = h.EsA + 2 * D.EsA.size();
+    h.nfmax = D.nfmax;
+    h.sigma_t = DP(double, 18); h.sigma_s = DP(double, 19);
+    h.s_minus = D.csd ? DP(double, 20) : nullptr; h.s_plus = D.csd ? DP(double, 21) : nullptr;
+    h.s_mom = D.csd ? DP(double, 22) : nullptr; h.t_mom = P->t_mom ? DP(double, 23) : nullptr;
+    h.e_width = D.csd ? DP(double, 24) : nullptr; h.vol = D.vol.empty() ? nullptr : DP(double, 25);
+    for (int f = 0; f < 6; f++) h.surf[f] = (f < 2 * P->ndims && P->surface_sources[f]) ? DP(double, 26 + f) : nullptr;
+    h.flux = DP(double, 32); h.vecs = DP(double, 33); h.qlout = DP(double, 34); h.qnout = DP(double, 35);
+    h.psi = DP(double, 36); h.kmat = DP(double, 37); h.scsd = DP(double, 38); h.fexit = DP(double, 39);
+    h.phiE_a = D.csd ? DP(double, 40) : nullptr; h.phiE_b = D.csd ? DP(double, 41) : nullptr;
+    h.cutoff = D.csd ? DP(double, 42) : nullptr;
+    h.rho = DP(double, 43); h.resid = h.rho + ng; h.iters = DP(int, 44); h.conv = h.iters + ng;
+    h.passes = DP(long long, 45); h.status = DP(int, 46);
+    int r = RB_OK;
+#define PUT(T, k, src, n) if ((r = put<T>(ctx, b, o[k], src, n, s)) != RB_OK) return r;
+    PUT(double, 1, P->dx, D.ns[0]);
+    PUT(int, 2, D.mat0.data(), D.mat0.size());
+    PUT(double, 3, D.cosv.data(), D.cosv.size());
+    PUT(double, 4, P->mn, (size_t)nd * np);
+    PUT(double, 5, P->dn, (size_t)np * nd);
+    PUT(int, 6, P->pl, np);
+    PUT(double, 7, D.mnfp.data(), D.mnfp.size());
+    PUT(double, 8, D.frow_m.data(), D.frow_m.size());
+    PUT(double, 9, D.frow_d.data(), D.frow_d.size());
+    PUT(double, 10, D.G.data(), D.G.size());
+    PUT(double, 11, D.Gsrc.data(), D.Gsrc.size());
+    PUT(double, 12, D.Gout.data(), D.Gout.size());
+    PUT(int, 13, D.tang.data(), D.tang.size());
+    std::vector<double> eabo;
+    eabo.insert(eabo.end(), D.EsA.begin(), D.EsA.end());
+    eabo.insert(eabo.end(), D.EsB.begin(), D.EsB.end());
+    eabo.insert(eabo.end(), D.Eout.begin(), D.Eout.end());
+    PUT(double, 14, eabo.data(), eabo.size());
+    PUT(double, 15, D.Kcsd.data(), D.Kcsd.size());
+    PUT(double, 16, D.Bcsd.data(), D.Bcsd.size());
+    PUT(double, 18, P->sigma_t, (size_t)ng * nmat);
+    PUT(double, 19, P->sigma_s, (size_t)nmat * ng * ng * (P->ls + 1));
+    if (D.csd) {
+        PUT(double, 20, P->s_minus, (size_t)ng * nmat);
+        PUT(double, 21, P->s_plus, (size_t)ng * nmat);
+        PUT(double, 22, P->s_mom, (size_t)ng * nmat * P->order[3]);
+        PUT(double, 24, P->e_width, ng);
+    }
+    if (P->t_mom) PUT(double, 23, P->t_mom, (size_t)ng * nmat);
+    PUT(double, 25, D.vol.data(), D.vol.size());
+    for (int f = 0; f < 2 * P->ndims; f++)
+        if (P->surface_sources[f])
+            PUT(double, 26 + f, P->surface_sources[f], (size_t)ng * P->np_source * face_cells(P->ndims, D.ns, f / 2));
+#undef PUT
+    *dptr = DP(DevProblem, 0);
+#undef DP
+    CK(cudaMemcpyAsync(*dptr, &h, sizeof(DevProblem), cudaMemcpyHostToDevice, s));
+    return RB_OK;
+}
+
 }  // namespace
 
 // =============================================================================================
@@ -516,82 +594,12 @@ int32_t rb_upload(rb_context *ctx, const rb_sn_problem *P, rb_handle *out) {
     auto rec = std::make_unique<ProblemRec>();
     CK(cudaMalloc(&rec->block, L.off));
     rec->bytes = L.off;
-    char *b = rec->block;
     cudaStream_t s = ctx->stream;
     DevProblem &h = rec->h;
-    memset(&h, 0, sizeof(h));
-    const int nd = P->nd, np = P->np, nm5 = D.M.nm, ng = P->ng, nmat = P->nmat;
-    h.ndims = P->ndims; h.nx = D.ns[0]; h.ny = D.ns[1]; h.nz = D.ns[2]; h.ncell = D.ncell;
-    h.nd = nd; h.np = np; h.nm5 = nm5;
-    for (int d = 0; d < 3; d++) h.nmf[d] = d < P->ndims ? P->nm[d] : 1;
-    h.nm4 = D.csd ? P->nm[3] : 1;
-    h.npsurf = P->np_surf; h.ng = ng; h.nmat = nmat; h.ls = P->ls; h.oE = P->order[3]; h.csd = D.csd;
-    h.solver_type = P->solver_type; h.accel = P->accel; h.maxit = P->max_iter; h.restart = P->gmres_restart;
-    h.depth = P->anderson_depth; h.precision = P->precision; h.tol = P->tol; h.np_source = P->np_source;
-    h.nphi = D.nphi; h.nstate = D.nstate;
-    for (int d = 0; d < 3; d++) { h.off_b[d] = D.off_b[d]; h.nb[d] = D.nb[d]; }
-    h.nvec = nvec_for(P);
-    for (int a = 0; a < 4; a++) h.w1[a] = D.w1[a];
-    for (int f = 0; f < 6; f++) h.bc[f] = P->bc[f];
-#define DP(T, k) (reinterpret_cast<T *>(b + o[k]))
-    h.dx = DP(double, 1); h.mat = DP(int, 2); h.cosv = DP(double, 3); h.mn = DP(double, 4); h.dn = DP(double, 5);
-    h.pl = DP(int, 6); h.mnfp = D.mnfp.empty() ? nullptr : DP(double, 7); h.frow_m = DP(double, 8);
-    h.frow_d = DP(double, 9); h.G = DP(double, 10); h.Gsrc = DP(double, 11); h.Gout = DP(double, 12);
-    h.tang = DP(int, 13); h.Kcsd = DP(double, 15); h.Bcsd = DP(double, 16);
-    h.EsA = DP(double, 14); h.EsB = h.EsA + D.EsA.size(); h.Eout = h.EsA + 2 * D.EsA.size();
-    h.nfmax = D.nfmax;
-    h.sigma_t = DP(double, 18); h.sigma_s = DP(double, 19);
-    h.s_minus = D.csd ? DP(double, 20) : nullptr; h.s_plus = D.csd ? DP(double, 21) : nullptr;
-    h.s_mom = D.csd ? DP(double, 22) : nullptr; h.t_mom = P->t_mom ? DP(double, 23) : nullptr;
-    h.e_width = D.csd ? DP(double, 24) : nullptr; h.vol = D.vol.empty() ? nullptr : DP(double, 25);
-    for (int f = 0; f < 6; f++) h.surf[f] = (f < 2 * P->ndims && P->surface_sources[f]) ? DP(double, 26 + f) : nullptr;
-    h.flux = DP(double, 32); h.vecs = DP(double, 33); h.qlout = DP(double, 34); h.qnout = DP(double, 35);
-    h.psi = DP(double, 36); h.kmat = DP(double, 37); h.scsd = DP(double, 38); h.fexit = DP(double, 39);
-    h.phiE_a = D.csd ? DP(double, 40) : nullptr; h.phiE_b = D.csd ? DP(double, 41) : nullptr;
-    h.cutoff = D.csd ? DP(double, 42) : nullptr;
-    h.rho = DP(double, 43); h.resid = h.rho + ng; h.iters = DP(int, 44); h.conv = h.iters + ng;
-    h.passes = DP(long long, 45); h.status = DP(int, 46);
-    int r = RB_OK;
-#define PUT(T, k, src, n) if ((r = put<T>(ctx, b, o[k], src, n, s)) != RB_OK) { cudaFree(rec->block); return r; }
-    PUT(double, 1, P->dx, D.ns[0]);
-    PUT(int, 2, D.mat0.data(), D.mat0.size());
-    PUT(double, 3, D.cosv.data(), D.cosv.size());
-    PUT(double, 4, P->mn, (size_t)nd * np);
-    PUT(double, 5, P->dn, (size_t)np * nd);
-    PUT(int, 6, P->pl, np);
-    PUT(double, 7, D.mnfp.data(), D.mnfp.size());
-    PUT(double, 8, D.frow_m.data(), D.frow_m.size());
-    PUT(double, 9, D.frow_d.data(), D.frow_d.size());
-    PUT(double, 10, D.G.data(), D.G.size());
-    PUT(double, 11, D.Gsrc.data(), D.Gsrc.size());
-    PUT(double, 12, D.Gout.data(), D.Gout.size());
-    PUT(int, 13, D.tang.data(), D.tang.size());
-    std::vector<double> eabo;
-    eabo.insert(eabo.end(), D.EsA.begin(), D.EsA.end());
-    eabo.insert(eabo.end(), D.EsB.begin(), D.EsB.end());
-    eabo.insert(eabo.end(), D.Eout.begin(), D.Eout.end());
-    PUT(double, 14, eabo.data(), eabo.size());
-    PUT(double, 15, D.Kcsd.data(), D.Kcsd.size());
-    PUT(double, 16, D.Bcsd.data(), D.Bcsd.size());
-    PUT(double, 18, P->sigma_t, (size_t)ng * nmat);
-    PUT(double, 19, P->sigma_s, (size_t)nmat * ng * ng * (P->ls + 1));
-    if (D.csd) {
-        PUT(double, 20, P->s_minus, (size_t)ng * nmat);
-        PUT(double, 21, P->s_plus, (size_t)ng * nmat);
-        PUT(double, 22, P->s_mom, (size_t)ng * nmat * P->order[3]);
-        PUT(double, 24, P->e_width, ng);
-    }
-    if (P->t_mom) PUT(double, 23, P->t_mom, (size_t)ng * nmat);
-    PUT(double, 25, D.vol.data(), D.vol.size());
-    for (int f = 0; f < 2 * P->ndims; f++)
-        if (P->surface_sources[f])
-            PUT(double, 26 + f, P->surface_sources[f], (size_t)ng * P->np_source * face_cells(P->ndims, D.ns, f / 2));
-#undef PUT
-    rec->d = DP(DevProblem, 0);
-#undef DP
-    CK(cudaMemcpyAsync(rec->d, &h, sizeof(DevProblem), cudaMemcpyHostToDevice, s));
+    st = place_problem(ctx, P, D, o, rec->block, s, h, &rec->d);
+    if (st) { cudaFree(rec->block); return st; }
     CK(cudaStreamSynchronize(s));
-    rec->ng = ng; rec->np = np; rec->nm5 = nm5; rec->csd = D.csd; rec->ncell = D.ncell; rec->nphi = D.nphi;
+    rec->ng = P->ng; rec->np = P->np; rec->nm5 = D.M.nm; rec->csd = D.csd; rec->ncell = D.ncell; rec->nphi = D.nphi;
     ctx->used += L.off;
     rb_handle hd = ctx->next_handle++;
     ctx->probs[hd] = std::move(rec);
