@@ -179,6 +179,20 @@ RB_API int32_t rb_required_bytes(const rb_sn_problem *prob, uint64_t *bytes);
 /* upload + solve + download + release on a private context: the one-call drop-in. */
 RB_API int32_t rb_compute_flux(int32_t device, const rb_sn_problem *prob, rb_sn_result *res);
 
+/* rb_compute_flux without any device allocation. No counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc -- a process whose device memory belongs to another
+ * allocator (a Julia CUDA.jl pool, a PyTorch caching allocator) that must not see
+ * cudaMalloc/cudaFree, which synchronise the device and can fail or fragment that pool.
+ * All device memory it uses (tables, work buffers, result staging) is one file-scope static
+ * device array of 16 MiB that every GPU loading the library holds until the process exits;
+ * a problem needing more returns RB_ERR_BUDGET with the sizes in rb_last_error(NULL, ...).
+ * Runs on the current device and `stream` (NULL = the legacy default stream) and returns once
+ * the results are in the caller's host buffers. The first call on a device looks the array's
+ * device address up (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. Every call shares the one array and overwrites it: calls that
+ * overlap on the GPU (other host threads, other streams) race and must be serialised. */
+RB_API int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_result *res, void *stream);
+
 /* ---- serving: continuous batching over a device work queue --------------------------- */
 /* Admits a request when its state fits the remaining HBM budget (RB_ERR_BUDGET otherwise);
  * admitted requests run as soon as a slot of the persistent kernel frees up. */

@@ -721,3 +721,96 @@ int32_t rb_energy_deposition(int32_t ng, int32_t np, int32_t nm5, int64_t ncell,
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Entry point that allocates no device memory
+// =============================================================================================
+// Some callers cannot call cudaMalloc: a host process whose device memory is owned by another
+// allocator (a Julia CUDA.jl pool or a PyTorch caching allocator that has reserved the HBM)
+// must not see cudaMalloc/cudaFree, which synchronise the whole device and can fail or
+// fragment that pool mid-run. rb_compute_flux_static serves them: every byte of device memory
+// it touches -- the problem's tables, its work buffers and the result staging -- lives in the
+// file-scope array below, reserved once when the library is loaded and held by every GPU
+// that loads it until the process exits.
+#define RB_STATIC_SCRATCH_BYTES (16ull << 20)  // 16 MiB per device
+static __device__ __align__(256) unsigned char rb_static_scratch[RB_STATIC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+char *g_static_scratch[kMaxDevices] = {nullptr};  // device address of rb_static_scratch, per device
+std::mutex g_static_mu;
+
+// Host code cannot use `rb_static_scratch` as a device address: look it up once per device,
+// with that device current.
+int static_scratch_address(int dev, char **out) {
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (dev < 0 || dev >= kMaxDevices) return fail(nullptr, RB_ERR_INVALID, "device %d out of range", dev);
+    if (!g_static_scratch[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, rb_static_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(nullptr, RB_ERR_CUDA, "cudaGetSymbolAddress(rb_static_scratch): %s", cudaGetErrorString(e));
+        g_static_scratch[dev] = static_cast<char *>(p);
+    }
+    *out = g_static_scratch[dev];
+    return RB_OK;
+}
+}  // namespace
+
+extern "C" int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_result *res, void *stream) {
+    rb_context *ctx = nullptr;  // errors go to rb_last_error(NULL, ...)
+    if (!prob || !res) return fail(nullptr, RB_ERR_INVALID, "null problem or result");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    char *base = nullptr;
+    int st = static_scratch_address(dev, &base);
+    if (st) return st;
+    Derived D;
+    st = validate_and_derive(nullptr, prob, D);
+    if (st) return st;
+    Layout L;
+    size_t o[64];
+    required(prob, D, L, o);
+    const size_t off_list = L.take<DevProblem *>(1);
+    const size_t off_queue = L.take<int>(1);
+    const size_t off_stage = L.take<double>((size_t)prob->ng * D.nphi);
+    if (L.off > RB_STATIC_SCRATCH_BYTES)
+        return fail(nullptr, RB_ERR_BUDGET, "problem needs %zu bytes of device memory; the static scratch of "
+                    "rb_compute_flux_static holds %llu", L.off, (unsigned long long)RB_STATIC_SCRATCH_BYTES);
+    cudaStream_t s = (cudaStream_t)stream;
+    DevProblem h;
+    DevProblem *d = nullptr;
+    st = place_problem(nullptr, prob, D, o, base, s, h, &d);
+    if (st) return st;
+    DevProblem **d_list = reinterpret_cast<DevProblem **>(base + off_list);
+    int *d_queue = reinterpret_cast<int *>(base + off_queue);
+    double *d_stage = reinterpret_cast<double *>(base + off_stage);
+    // the array keeps the previous call's contents: zero the queue counter and status word
+    CK(cudaMemcpyAsync(d_list, &d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(d_queue, 0, sizeof(int), s));
+    CK(cudaMemsetAsync(h.status, 0, sizeof(int), s));
+    rb::solve_batch_kernel<<<1, RB_THREADS, 0, s>>>(d_list, 1, d_queue);
+    CK(cudaGetLastError());
+    const int ng = prob->ng;
+    if (res->flux) {
+        dim3 blk(32, 8), grd((unsigned)((D.nphi + 31) / 32), (unsigned)((ng + 31) / 32));
+        rb::to_reference_layout<<<grd, blk, 0, s>>>(h.flux, d_stage, ng, D.nphi);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(res->flux, d_stage, (size_t)ng * D.nphi * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    if (res->flux_cutoff && D.csd)
+        CK(cudaMemcpyAsync(res->flux_cutoff, h.cutoff, D.nphi * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (res->rho) CK(cudaMemcpyAsync(res->rho, h.rho, ng * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (res->group_resid) CK(cudaMemcpyAsync(res->group_resid, h.resid, ng * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (res->group_iters) CK(cudaMemcpyAsync(res->group_iters, h.iters, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (res->group_converged) CK(cudaMemcpyAsync(res->group_converged, h.conv, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+    long long passes = 0;
+    int status = 0;
+    CK(cudaMemcpyAsync(&passes, h.passes, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&status, h.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    res->passes = passes;
+    if (status & RB_DEV_TIMEOUT) return fail(nullptr, RB_ERR_TIMEOUT, "a device wait gave up");
+    if (status & RB_DEV_BAD_TABLE) return fail(nullptr, RB_ERR_INVALID, "singular cell system or bad table");
+    return RB_OK;
+}
