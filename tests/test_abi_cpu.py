@@ -1,0 +1,85 @@
+"""The C-ABI library loads, exports every entry point include/radiant_b200.h declares, and
+rejects bad descriptions on the host (no device call is made here)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from radiant_b200 import workloads as W
+from radiant_b200._abi import PackedProblem, load_library
+
+HDR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "radiant_b200.h")
+
+
+def declared_symbols():
+    with open(HDR) as f:
+        src = f.read()
+    return sorted(set(re.findall(r"RB_API\s+[\w\s\*]+?\b(rb_\w+)\s*\(", src)))
+
+
+def test_header_declares_the_abi():
+    syms = declared_symbols()
+    for s in ("rb_create", "rb_upload", "rb_solve", "rb_download", "rb_compute_flux", "rb_submit", "rb_poll",
+              "rb_last_error"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = load_library()
+    for s in declared_symbols():
+        assert hasattr(lib, s), s
+
+
+def _required(tabs):
+    lib = load_library()
+    pp = PackedProblem(tabs)
+    b = C.c_uint64()
+    st = lib.rb_required_bytes(C.byref(pp.P), C.byref(b))
+    buf = C.create_string_buffer(512)
+    lib.rb_last_error(None, buf, 512)
+    return st, b.value, buf.value.decode()
+
+
+def test_required_bytes_of_configs():
+    st, b, _ = _required(W.c1_tables(seed=1))
+    assert st == 0 and 1 << 20 < b < 8 << 20
+    st, b, _ = _required(W.c2_tables(seed=1))
+    assert st == 0 and b > 16 << 20
+
+
+def test_rejects_bad_material_id():
+    t = W.c1_tables(seed=1)
+    t["mat"] = t["mat"].copy()
+    t["mat"].flat[5] = 7
+    st, _, msg = _required(t)
+    assert st == 1 and "mat[5]=7" in msg
+
+
+def test_rejects_inconsistent_moments():
+    t = W.c1_tables(seed=1)
+    t["nm"] = list(t["nm"])
+    t["nm"][4] = 3
+    st, _, msg = _required(t)
+    assert st == 1 and "nm[4]" in msg
+
+
+def test_rejects_adaptive_and_em():
+    for key in ("is_adaptive", "is_em"):
+        t = W.c1_tables(seed=1)
+        t[key] = 1
+        st, _, _ = _required(t)
+        assert st == 2
+
+
+def test_rejects_oversized_restart():
+    t = W.c1_tables(seed=1)
+    t["gmres_restart"] = 1000
+    st, _, msg = _required(t)
+    assert st == 1 and "gmres_restart" in msg
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        load_library(str(tmp_path / "nope.so"))
