@@ -48,10 +48,12 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def workload_tables(seeds, precision):
+def workload_tables(seeds, precision, workload="c2"):
     from radiant_b200 import workloads as W
 
     tabs = []
+    if workload == "c1":  # small case (profiling): the 1D photon BTE slab, one solve per seed
+        return [W.c1_tables(seed=s, precision=precision) for s in seeds]
     for s in seeds:
         for part in ("photon", "electron", "positron"):
             t = W.c2_tables(seed=s * 3 + {"photon": 0, "electron": 1, "positron": 2}[part], precision=precision,
@@ -128,7 +130,7 @@ def run_ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     seeds = [1 + rank * 1000 + k for k in range(args.seeds)]
-    tabs = workload_tables(seeds, args.precision)
+    tabs = workload_tables(seeds, args.precision, args.workload)
     ctx = Context(dev, 0)
     packs = [PackedProblem(t) for t in tabs]
     handles = [ctx.upload(p) for p in packs]
@@ -297,6 +299,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--seeds", type=int, default=50)
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1"],
+                    help="c2: the benchmark workload; c1: the small photon slab (profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
