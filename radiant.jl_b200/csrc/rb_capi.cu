@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -40,6 +41,7 @@ struct ProblemRec {
 struct rb_context {
     int device = 0;
     int nsm = 0;
+    int cluster = 0;  // CTAs per problem team (0 = sized per batch); RB_CLUSTER_SIZE overrides
     uint64_t budget = 0;
     uint64_t used = 0;
     cudaStream_t stream = nullptr;
@@ -399,6 +401,35 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     return k;
 }
 
+// Launches the persistent solve kernel as clusters of `cluster` CTAs (one team per problem),
+// as many clusters as fit on the device at once, capped by the number of problems.
+int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm, int cluster, cudaStream_t s) {
+    if (cluster < 1) cluster = 1;
+    if (cluster > RB_MAXCLUSTER) cluster = RB_MAXCLUSTER;
+    const size_t smem = sizeof(rb::GroupShared);
+    CK(cudaFuncSetAttribute(rb::solve_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (cluster > 8) CK(cudaFuncSetAttribute(rb::solve_batch_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(RB_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int max_clusters = 0;
+    cfg.gridDim = dim3(cluster * (nsm / cluster > 0 ? nsm / cluster : 1), 1, 1);
+    CK(cudaOccupancyMaxActiveClusters(&max_clusters, rb::solve_batch_kernel, &cfg));
+    if (max_clusters < 1) return fail(ctx, RB_ERR_CUDA, "no cluster of %d CTAs fits on the device", cluster);
+    int nclusters = max_clusters < n ? max_clusters : n;
+    cfg.gridDim = dim3(cluster * nclusters, 1, 1);
+    CK(cudaLaunchKernelEx(&cfg, rb::solve_batch_kernel, (DevProblem *const *)list, n, queue));
+    return RB_OK;
+}
+
 int ensure_launch_scratch(rb_context *ctx, int n) {
     if (n > ctx->list_cap) {
         if (ctx->d_list) cudaFree(ctx->d_list);
@@ -420,13 +451,13 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
     CK(cudaMemcpyAsync(ctx->d_list, ptrs.data(), sizeof(DevProblem *) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), s));
     for (auto *r : recs) CK(cudaMemsetAsync(r->h.status, 0, sizeof(int), s));
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb::solve_batch_kernel, RB_THREADS, 0));
-    if (per_sm < 1) per_sm = 1;
-    int grid = ctx->nsm * per_sm;
-    if (grid > n) grid = n;
-    rb::solve_batch_kernel<<<grid, RB_THREADS, 0, s>>>(ctx->d_list, n, ctx->d_queue);
-    CK(cudaGetLastError());
+    int cluster = ctx->cluster;
+    if (cluster <= 0) {  // one cluster per problem, sized to the problem's directions
+        const DevProblem &h0 = recs[0]->h;
+        cluster = h0.nd >= 32 ? 8 : (h0.nd >= 16 ? 4 : (h0.nd >= 8 ? 2 : 1));
+    }
+    int st2 = launch_solve(ctx, ctx->d_list, n, ctx->d_queue, ctx->nsm, cluster, s);
+    if (st2) return st2;
     for (auto *r : recs) { r->stream = s; r->solved = true; }
     return RB_OK;
 }
@@ -539,6 +570,7 @@ int32_t rb_create(int32_t device, uint64_t hbm_budget_bytes, rb_context **out) {
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)(fr * 0.9);
+    if (const char *cs = getenv("RB_CLUSTER_SIZE")) c->cluster = atoi(cs);
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete c; return fail(nullptr, RB_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
     *out = c;
@@ -789,8 +821,8 @@ extern "C" int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_resul
     CK(cudaMemcpyAsync(d_list, &d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(d_queue, 0, sizeof(int), s));
     CK(cudaMemsetAsync(h.status, 0, sizeof(int), s));
-    rb::solve_batch_kernel<<<1, RB_THREADS, 0, s>>>(d_list, 1, d_queue);
-    CK(cudaGetLastError());
+    st = launch_solve(nullptr, d_list, 1, d_queue, 1, 1, s);
+    if (st) return st;
     const int ng = prob->ng;
     if (res->flux) {
         dim3 blk(32, 8), grd((unsigned)((D.nphi + 31) / 32), (unsigned)((ng + 31) / 32));

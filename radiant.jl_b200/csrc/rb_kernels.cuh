@@ -1,98 +1,76 @@
-// rb_kernels.cuh -- the device side of the SN solve.
+// rb_kernels.cuh -- one transport pass of a 1D problem, spread over a team (thread-block cluster).
 //
-// Design: one persistent launch solves a batch of problems. Each problem is owned by a
-// "team" (one CTA for 1D problems); the team runs the whole group loop of
-// sn_flux.jl:162-224 on the device: out-of-group source, the in-group accelerator
-// (livolant / anderson / gmres / bicgstab, sn_one_speed.jl:122-187) and every transport pass
-// (sn_inner_pass.jl:17-137), with no host round trip. Scalars the accelerators need (dots,
-// norms, Hessenberg/Givens) are reduced inside the team in a fixed order, so results are
-// deterministic and independent of which problems share the launch.
-//
-// A pass is three phases over the team's threads:
-//   M2D   Qn[n,is,c] = Mn·Qlout + Σ_p K[mat(c)][n,p]·𝚽[p,is,c],  K = Mn·(diag Σs_l + T·ℳ)
-//   sweep one thread per direction walks the cells upwind, solving the Nm5×Nm5 cell system of
-//         the diamond-difference / DG closures in registers (sn_1D_bte.jl, sn_1D_bfp.jl)
-//   D2M   𝚽[p,is,c] = Σ_n Dn[p,n]·ψ[n,is,c] and the outgoing boundary moments.
+// A pass (sn_inner_pass.jl:17-137) is three phases separated by team barriers:
+//   M2D   ψ[n,is,c] = Mn·Qlout + K[mat(c)]·𝚽[:,is,c],  K = Mn·(diag Σs_l + T·ℳ) built per group:
+//         the in-group scattering source (scattering_source.jl:25-30) and the Fokker-Planck
+//         source (fokker_planck_source.jl:29-33) folded into the moment-to-discrete product.
+//   sweep sn_sweep_1D.jl:51-123 with flux_1D_BTE / flux_1D_BFP. Along one direction the
+//         incoming face flux obeys an affine recurrence F_{k+1} = A_k·F_k + b_k (the closure
+//         solved for the outgoing face), so the cells are cut into chunks: every thread composes
+//         its chunk's map, one thread per direction chains the chunk maps from the boundary
+//         flux, and every thread re-sweeps its chunk from its now-known incoming flux. All
+//         threads work instead of one per direction.
+//   D2M   𝚽[p,is,c] = Σ_n Dn[p,n]·ψ[n,is,c] (direction order, as the reference accumulates)
+//         and the outgoing boundary moments; for the Krylov matvec the output is z − A·z.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 
 #include "rb_internal.h"
+#include "rb_team.cuh"
 
 #define RB_MAXRESTART 48
 #define RB_MAXDEPTH 16
 #define RB_THREADS 256
+#define RB_SCAN_NF 4      // scan path for face-moment counts up to this
+#define RB_MAXCLUSTER 16
 
 namespace rb {
-
-// ------------------------------------------------------------------------------------------
-// team of one CTA: barrier and deterministic reductions
-// ------------------------------------------------------------------------------------------
-struct CtaTeam {
-    double *red;  // shared scratch, >= nwarps doubles
-    __device__ __forceinline__ int rank() const { return threadIdx.x; }
-    __device__ __forceinline__ int size() const { return blockDim.x; }
-    __device__ __forceinline__ void sync() const { __syncthreads(); }
-    // Sum over the team; every thread receives the same bits (xor butterfly, then a fixed
-    // warp order).
-    __device__ double sum(double v) const {
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-        if ((threadIdx.x & 31) == 0) red[w] = v;
-        __syncthreads();
-        double s = 0.0;
-        for (int k = 0; k < nw; k++) s += red[k];
-        __syncthreads();
-        return s;
-    }
-    __device__ int any(int flag) const { return __syncthreads_or(flag); }
-};
 
 // ------------------------------------------------------------------------------------------
 // state algebra (krylov_state.jl:53-114) over [𝚽 | boundary in-moments]
 // ------------------------------------------------------------------------------------------
 template <class Team>
-__device__ double vdot(const Team &t, const double *a, const double *b, long long n) {
+__device__ double vdot(Team &t, const double *a, const double *b, long long n) {
     double s = 0.0;
     for (long long i = t.rank(); i < n; i += t.size()) s += a[i] * b[i];
     return t.sum(s);
 }
 template <class Team>
-__device__ void vaxpy(const Team &t, double al, const double *x, double *y, long long n) {
+__device__ void vaxpy(Team &t, double al, const double *x, double *y, long long n) {
     for (long long i = t.rank(); i < n; i += t.size()) y[i] += al * x[i];
     t.sync();
 }
 template <class Team>
-__device__ void vscale(const Team &t, double al, double *x, long long n) {
-    for (long long i = t.rank(); i < n; i += t.size()) x[i] *= al;
-    t.sync();
-}
-template <class Team>
-__device__ void vcopy(const Team &t, double *d, const double *s, long long n) {
+__device__ void vcopy(Team &t, double *d, const double *s, long long n) {
     for (long long i = t.rank(); i < n; i += t.size()) d[i] = s[i];
     t.sync();
 }
 template <class Team>
-__device__ void vzero(const Team &t, double *d, long long n) {
+__device__ void vzero(Team &t, double *d, long long n) {
     for (long long i = t.rank(); i < n; i += t.size()) d[i] = 0.0;
     t.sync();
 }
 // y = a·x + b·y
 template <class Team>
-__device__ void vlin(const Team &t, double a, const double *x, double b, double *y, long long n) {
+__device__ void vlin(Team &t, double a, const double *x, double b, double *y, long long n) {
     for (long long i = t.rank(); i < n; i += t.size()) y[i] = a * x[i] + b * y[i];
     t.sync();
 }
 
 // ------------------------------------------------------------------------------------------
 // cell solve: Gaussian elimination with partial pivoting (the arithmetic of Julia's `𝒮\Q`,
-// sn_1D_bte.jl:55 / sn_1D_bfp.jl:101). The compile-time version keeps the NM×NM system in
-// registers; the run-time one serves the rarer large systems from local memory.
+// sn_1D_bte.jl:55 / sn_1D_bfp.jl:101) on an NM×NM system in registers, NR right-hand sides
 // ------------------------------------------------------------------------------------------
-template <typename R, int NM>
-__device__ __forceinline__ void lu_solve(R (&S)[NM * NM], R (&q)[NM]) {
-    if (NM == 1) { q[0] = q[0] / S[0]; return; }
+template <typename R, int NM, int NR>
+__device__ __forceinline__ void lu_solve(R (&S)[NM * NM], R (&q)[NR][NM]) {
+    if (NM == 1) {
+        const R inv = R(1) / S[0];
+#pragma unroll
+        for (int r = 0; r < NR; r++) q[r][0] = q[r][0] * inv;
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < NM; k++) {
         int p = k;
@@ -105,7 +83,8 @@ __device__ __forceinline__ void lu_solve(R (&S)[NM * NM], R (&q)[NM]) {
             if (i == p) {
 #pragma unroll
                 for (int j = 0; j < NM; j++) { R tmp = S[k + NM * j]; S[k + NM * j] = S[i + NM * j]; S[i + NM * j] = tmp; }
-                R tq = q[k]; q[k] = q[i]; q[i] = tq;
+#pragma unroll
+                for (int r = 0; r < NR; r++) { R tq = q[r][k]; q[r][k] = q[r][i]; q[r][i] = tq; }
             }
         }
         const R inv = R(1) / S[k + NM * k];
@@ -114,15 +93,20 @@ __device__ __forceinline__ void lu_solve(R (&S)[NM * NM], R (&q)[NM]) {
             const R f = S[i + NM * k] * inv;
 #pragma unroll
             for (int j = k + 1; j < NM; j++) S[i + NM * j] -= f * S[k + NM * j];
-            q[i] -= f * q[k];
+#pragma unroll
+            for (int r = 0; r < NR; r++) q[r][i] -= f * q[r][k];
         }
     }
 #pragma unroll
     for (int i = NM - 1; i >= 0; i--) {
-        R s = q[i];
+        const R inv = R(1) / S[i + NM * i];
 #pragma unroll
-        for (int j = i + 1; j < NM; j++) s -= S[i + NM * j] * q[j];
-        q[i] = s / S[i + NM * i];
+        for (int r = 0; r < NR; r++) {
+            R s = q[r][i];
+#pragma unroll
+            for (int j = i + 1; j < NM; j++) s -= S[i + NM * j] * q[r][j];
+            q[r][i] = s * inv;
+        }
     }
 }
 
@@ -159,19 +143,22 @@ __device__ void lu_solve_rt(R *S, R *q, int n) {  // S is n×n, leading dimensio
 }
 
 // ------------------------------------------------------------------------------------------
-// per-group constants of a problem, cached in shared memory
+// per-CTA shared state
 // ------------------------------------------------------------------------------------------
 struct GroupShared {
     double sigt[RB_MAXMAT];
     double sp[RB_MAXMAT];   // S⁺/ΔE
     double sm[RB_MAXMAT];   // S⁻/ΔE
     double tg[RB_MAXMAT];
-    // Krylov scalars
+    // accelerator scalars (each CTA keeps an identical copy)
     double H[(RB_MAXRESTART + 1) * RB_MAXRESTART];
     double cs[RB_MAXRESTART], sn[RB_MAXRESTART], g[RB_MAXRESTART + 1], y[RB_MAXRESTART];
     double A[RB_MAXDEPTH * RB_MAXDEPTH], b[RB_MAXDEPTH];
-    double red[32];
-    int flag;
+    // sweep scan: per thread-chunk affine map (A: NF×NF, b: NF) and the chunk's incoming flux
+    double chA[RB_THREADS][RB_SCAN_NF * RB_SCAN_NF];
+    double chb[RB_THREADS][RB_SCAN_NF];
+    double chF[RB_THREADS][RB_SCAN_NF];
+    TeamShared team;
 };
 
 // Incoming x-face flux of a 1D direction: surface source into moment 1 plus the lagged
@@ -195,57 +182,46 @@ __device__ __forceinline__ void boundary_in_1d(const DevProblem &P, int n, const
     }
 }
 
-// ------------------------------------------------------------------------------------------
-// the 1D sweep of one direction (sn_sweep_1D.jl:51-123 with flux_1D_BTE / flux_1D_BFP),
-// compile-time shapes: NM cell moments, NF x-face moments, NE energy-face moments
-// ------------------------------------------------------------------------------------------
+// One cell of the closure in compile-time shapes. map() keeps the face dependence symbolic:
+// F_out = A·F_in + b. step() updates F in place and writes ψ (𝚽n) and the energy-face outputs.
 template <typename R, int NM, int NF, int NE, bool CSD>
-__device__ void sweep1d_dir(const DevProblem &P, const GroupShared &gs, int n, const double *zin_b,
-                            int np_source, const double *phiE_in, double *phiE_out, double *psi, int ig) {
-    const int nx = P.nx, nd = P.nd;
-    const double mu = P.cosv[n];
-    const bool fwd = mu >= 0.0;
-    const bool tang = P.tang[n] != 0;
-    R F[NF];
-    {
-        double f0[NF];
-        boundary_in_1d(P, n, zin_b, np_source, ig, f0);
-#pragma unroll
-        for (int f = 0; f < NF; f++) F[f] = (R)f0[f];
-    }
-    const long long tb = (long long)n * 3;  // axis-0 block of direction n
+struct Cell1D {
+    const DevProblem &P;
+    const GroupShared &gs;
+    int n, nd;
+    bool tang;
+    double amu;
     R Gr[NM * NM], Gs[NM * NF], Go[NF * NM];
+    R w1x, w1E;
+    const double *phiE_in;
+    double *phiE_out;
+
+    __device__ Cell1D(const DevProblem &P_, const GroupShared &gs_, int n_, const double *pEi, double *pEo)
+        : P(P_), gs(gs_), n(n_), nd(P_.nd), phiE_in(pEi), phiE_out(pEo) {
+        tang = P.tang[n] != 0;
+        amu = fabs(P.cosv[n]);
+        const long long tb = (long long)n * 3;  // axis-0 block of direction n
 #pragma unroll
-    for (int k = 0; k < NM * NM; k++) Gr[k] = (R)P.G[tb * NM * NM + k];
+        for (int k = 0; k < NM * NM; k++) Gr[k] = (R)P.G[tb * NM * NM + k];
 #pragma unroll
-    for (int k = 0; k < NM * NF; k++) { Gs[k] = (R)P.Gsrc[tb * NM * P.nfmax + k]; Go[k] = (R)P.Gout[tb * NM * P.nfmax + k]; }
-    R EA[NM * NE], EB[NM * NE], EO[NE * NM];
-    if (CSD) {
-#pragma unroll
-        for (int k = 0; k < NM * NE; k++) { EA[k] = (R)P.EsA[k]; EB[k] = (R)P.EsB[k]; EO[k] = (R)P.Eout[k]; }
+        for (int k = 0; k < NM * NF; k++) { Gs[k] = (R)P.Gsrc[tb * NM * P.nfmax + k]; Go[k] = (R)P.Gout[tb * NM * P.nfmax + k]; }
+        w1x = (R)P.w1[0];
+        w1E = (R)P.w1[3];
     }
-    const R w1x = (R)P.w1[0], w1E = (R)P.w1[3];
-    const double amu = fabs(mu);
-#pragma unroll 1
-    for (int k = 0; k < nx; k++) {
-        const int c = fwd ? k : nx - 1 - k;
+
+    // assemble S and the face-independent part q0 = Qn − E·F_E of cell c
+    __device__ __forceinline__ void assemble(int c, const double *psi, R (&S)[NM * NM], R (&q0)[NM], R &h,
+                                             R (&FE)[NE]) const {
         const int m = P.mat[c];
-        const R h = tang ? R(0) : (R)(amu / P.dx[c]);
-        R S[NM * NM], q[NM];
+        h = tang ? R(0) : (R)(amu / P.dx[c]);
         const R sig = (R)gs.sigt[m];
-        double *pc = psi + n + (long long)nd * NM * c;
 #pragma unroll
         for (int i = 0; i < NM; i++)
 #pragma unroll
             for (int j = 0; j < NM; j++) S[i + NM * j] = (i == j ? sig : R(0)) + h * Gr[i + NM * j];
+        const double *pc = psi + n + (long long)nd * NM * c;
 #pragma unroll
-        for (int j = 0; j < NM; j++) {
-            R a = R(0);
-#pragma unroll
-            for (int f = 0; f < NF; f++) a += Gs[j + NM * f] * F[f];
-            q[j] = (R)pc[(long long)nd * j] + h * a;
-        }
-        R FE[NE];
+        for (int j = 0; j < NM; j++) q0[j] = (R)pc[(long long)nd * j];
         if (CSD) {
             const double *Sc = P.scsd + (long long)m * NM * NM;
 #pragma unroll
@@ -257,18 +233,63 @@ __device__ void sweep1d_dir(const DevProblem &P, const GroupShared &gs, int n, c
             for (int j = 0; j < NM; j++) {
                 R a = R(0);
 #pragma unroll
-                for (int e = 0; e < NE; e++) a += (EA[j + NM * e] * spl - EB[j + NM * e] * smn) * FE[e];
-                q[j] -= a;
+                for (int e = 0; e < NE; e++) a += ((R)P.EsA[j + NM * e] * spl - (R)P.EsB[j + NM * e] * smn) * FE[e];
+                q0[j] -= a;
             }
         }
-        lu_solve<R, NM>(S, q);
+    }
+
+    __device__ __forceinline__ void map(int c, const double *psi, R (&A)[NF * NF], R (&b)[NF]) const {
+        R S[NM * NM], q[NF + 1][NM], h, FE[NE];
+        assemble(c, psi, S, q[0], h, FE);
+#pragma unroll
+        for (int f = 0; f < NF; f++)
+#pragma unroll
+            for (int j = 0; j < NM; j++) q[f + 1][j] = h * Gs[j + NM * f];
+        lu_solve<R, NM, NF + 1>(S, q);
+        if (tang) {  // the x face passes through unchanged (sn_1D_bte.jl:57)
+#pragma unroll
+            for (int f = 0; f < NF; f++) {
+                b[f] = R(0);
+#pragma unroll
+                for (int g = 0; g < NF; g++) A[f + NF * g] = (f == g) ? R(1) : R(0);
+            }
+            return;
+        }
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+            R bb = R(0);
+#pragma unroll
+            for (int j = 0; j < NM; j++) bb += Go[f + NF * j] * q[0][j];
+            b[f] = bb;
+#pragma unroll
+            for (int g = 0; g < NF; g++) {
+                R a = (f == g) ? w1x : R(0);
+#pragma unroll
+                for (int j = 0; j < NM; j++) a += Go[f + NF * j] * q[g + 1][j];
+                A[f + NF * g] = a;
+            }
+        }
+    }
+
+    __device__ __forceinline__ void step(int c, double *psi, R (&F)[NF]) const {
+        R S[NM * NM], q[1][NM], h, FE[NE];
+        assemble(c, psi, S, q[0], h, FE);
+#pragma unroll
+        for (int j = 0; j < NM; j++) {
+            R a = R(0);
+#pragma unroll
+            for (int f = 0; f < NF; f++) a += Gs[j + NM * f] * F[f];
+            q[0][j] += h * a;
+        }
+        lu_solve<R, NM, 1>(S, q);
         if (!tang) {
             R Fo[NF];
 #pragma unroll
             for (int f = 0; f < NF; f++) {
                 R a = w1x * F[f];
 #pragma unroll
-                for (int j = 0; j < NM; j++) a += Go[f + NF * j] * q[j];
+                for (int j = 0; j < NM; j++) a += Go[f + NF * j] * q[0][j];
                 Fo[f] = a;
             }
 #pragma unroll
@@ -279,18 +300,119 @@ __device__ void sweep1d_dir(const DevProblem &P, const GroupShared &gs, int n, c
             for (int e = 0; e < NE; e++) {
                 R a = w1E * FE[e];
 #pragma unroll
-                for (int j = 0; j < NM; j++) a += EO[e + NE * j] * q[j];
+                for (int j = 0; j < NM; j++) a += (R)P.Eout[e + NE * j] * q[0][j];
                 phiE_out[n + (long long)nd * (e + (long long)NE * c)] = (double)a;
             }
         }
+        double *pc = psi + n + (long long)nd * NM * c;
 #pragma unroll
-        for (int j = 0; j < NM; j++) pc[(long long)nd * j] = (double)q[j];
+        for (int j = 0; j < NM; j++) pc[(long long)nd * j] = (double)q[0][j];
     }
+};
+
+// The sweep phase with the chunked scan. Directions are dealt to the CTAs of the team round
+// robin; within a CTA the directions it owns share its threads, `chunks` threads each.
+template <typename R, int NM, int NF, int NE, bool CSD, class Team>
+__device__ void sweep1d_scan(Team &t, const DevProblem &P, GroupShared &gs, const double *zin_b, int np_source,
+                             const double *phiE_in, double *phiE_out, int ig) {
+    const int nd = P.nd, nx = P.nx;
+    const int ncta = (int)t.ncta, crank = (int)t.crank;
+    const int my_dirs = (nd - crank + ncta - 1) / ncta;  // directions n = crank + k·ncta
+    const int nthr = blockDim.x;
+    int per_round = my_dirs < nthr ? my_dirs : nthr;
+    if (per_round < 1) per_round = 1;
+    int chunks = nthr / per_round;
+    if (chunks > nx) chunks = nx;
+    for (int k0 = 0; k0 < my_dirs; k0 += per_round) {
+        const int dl = threadIdx.x / chunks, ch = threadIdx.x % chunks;
+        const int kdir = k0 + dl;
+        const bool active = (dl < per_round) && (kdir < my_dirs);
+        const int n = crank + kdir * ncta;
+        const int L = (nx + chunks - 1) / chunks;
+        const int kb = min(nx, ch * L), ke = min(nx, kb + L);
+        const bool fwd = active ? (P.cosv[n] >= 0.0) : true;
+        if (active) {
+            Cell1D<R, NM, NF, NE, CSD> cell(P, gs, n, phiE_in, phiE_out);
+            R Ac[NF * NF], bc[NF];
 #pragma unroll
-    for (int f = 0; f < NF; f++) P.fexit[(long long)n * RB_MAXFACE + f] = (double)F[f];
+            for (int f = 0; f < NF; f++) {
+                bc[f] = R(0);
+#pragma unroll
+                for (int g = 0; g < NF; g++) Ac[f + NF * g] = (f == g) ? R(1) : R(0);
+            }
+            for (int k = kb; k < ke; k++) {
+                R A[NF * NF], b[NF];
+                cell.map(fwd ? k : nx - 1 - k, P.psi, A, b);
+                R An[NF * NF], bn[NF];  // (A,b)∘(Ac,bc)
+#pragma unroll
+                for (int f = 0; f < NF; f++) {
+                    R s = b[f];
+#pragma unroll
+                    for (int g = 0; g < NF; g++) s += A[f + NF * g] * bc[g];
+                    bn[f] = s;
+#pragma unroll
+                    for (int g = 0; g < NF; g++) {
+                        R a = R(0);
+#pragma unroll
+                        for (int h2 = 0; h2 < NF; h2++) a += A[f + NF * h2] * Ac[h2 + NF * g];
+                        An[f + NF * g] = a;
+                    }
+                }
+#pragma unroll
+                for (int f = 0; f < NF; f++) {
+                    bc[f] = bn[f];
+#pragma unroll
+                    for (int g = 0; g < NF; g++) Ac[f + NF * g] = An[f + NF * g];
+                }
+            }
+#pragma unroll
+            for (int f = 0; f < NF; f++) {
+                gs.chb[threadIdx.x][f] = (double)bc[f];
+#pragma unroll
+                for (int g = 0; g < NF; g++) gs.chA[threadIdx.x][f + NF * g] = (double)Ac[f + NF * g];
+            }
+        }
+        __syncthreads();
+        // chain the chunk maps from the boundary flux (one thread per direction)
+        if (active && ch == 0) {
+            double F0[RB_MAXFACE];
+            boundary_in_1d(P, n, zin_b, np_source, ig, F0);
+            R F[NF];
+#pragma unroll
+            for (int f = 0; f < NF; f++) F[f] = (R)F0[f];
+            for (int c2 = 0; c2 < chunks; c2++) {
+                const int tid = dl * chunks + c2;
+#pragma unroll
+                for (int f = 0; f < NF; f++) gs.chF[tid][f] = (double)F[f];
+                R Fn[NF];
+#pragma unroll
+                for (int f = 0; f < NF; f++) {
+                    R s = (R)gs.chb[tid][f];
+#pragma unroll
+                    for (int g = 0; g < NF; g++) s += (R)gs.chA[tid][f + NF * g] * F[g];
+                    Fn[f] = s;
+                }
+#pragma unroll
+                for (int f = 0; f < NF; f++) F[f] = Fn[f];
+            }
+        }
+        __syncthreads();
+        // re-sweep every chunk from its incoming flux
+        if (active) {
+            Cell1D<R, NM, NF, NE, CSD> cell(P, gs, n, phiE_in, phiE_out);
+            R F[NF];
+#pragma unroll
+            for (int f = 0; f < NF; f++) F[f] = (R)gs.chF[threadIdx.x][f];
+            for (int k = kb; k < ke; k++) cell.step(fwd ? k : nx - 1 - k, P.psi, F);
+            if (ch == chunks - 1)
+#pragma unroll
+                for (int f = 0; f < NF; f++) P.fexit[(long long)n * RB_MAXFACE + f] = (double)F[f];
+        }
+        __syncthreads();
+    }
 }
 
-// Run-time shapes (nm up to RB_MAXNM): the same arithmetic from local memory.
+// Run-time shapes (nm up to RB_MAXNM): one thread per direction walks all cells.
 __device__ void sweep1d_dir_rt(const DevProblem &P, const GroupShared &gs, int n, const double *zin_b,
                                int np_source, const double *phiE_in, double *phiE_out, double *psi, int ig) {
     const int nx = P.nx, nd = P.nd, nm = P.nm5, nf = P.nmf[0], ne = P.nm4;
@@ -359,58 +481,97 @@ __device__ void sweep1d_dir_rt(const DevProblem &P, const GroupShared &gs, int n
     for (int f = 0; f < nf; f++) P.fexit[(long long)n * RB_MAXFACE + f] = F[f];
 }
 
-__device__ __forceinline__ void sweep1d_dispatch(const DevProblem &P, const GroupShared &gs, int n,
-                                                 const double *zin_b, int np_source, const double *pE,
-                                                 double *phiE_out, int ig) {
+template <class Team>
+__device__ void sweep1d(Team &t, const DevProblem &P, GroupShared &gs, const double *zin_b, int np_source,
+                        const double *pE, double *phiE_out, int ig) {
     const int nm = P.nm5, nf = P.nmf[0], ne = P.nm4;
     if (!P.csd) {
-        if (nm == 1 && nf == 1) return sweep1d_dir<double, 1, 1, 1, false>(P, gs, n, zin_b, np_source, pE, phiE_out, P.psi, ig);
-        if (nm == 2 && nf == 1) return sweep1d_dir<double, 2, 1, 1, false>(P, gs, n, zin_b, np_source, pE, phiE_out, P.psi, ig);
+        if (nm == 1 && nf == 1) return sweep1d_scan<double, 1, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
+        if (nm == 2 && nf == 1) return sweep1d_scan<double, 2, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
+        if (nm == 3 && nf == 1) return sweep1d_scan<double, 3, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
     } else {
-        if (nm == 1 && nf == 1 && ne == 1) return sweep1d_dir<double, 1, 1, 1, true>(P, gs, n, zin_b, np_source, pE, phiE_out, P.psi, ig);
-        if (nm == 4 && nf == 2 && ne == 2) return sweep1d_dir<double, 4, 2, 2, true>(P, gs, n, zin_b, np_source, pE, phiE_out, P.psi, ig);
+        if (nm == 1 && nf == 1 && ne == 1) return sweep1d_scan<double, 1, 1, 1, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
+        if (nm == 2 && nf == 1 && ne == 2) return sweep1d_scan<double, 2, 1, 2, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
+        if (nm == 2 && nf == 2 && ne == 1) return sweep1d_scan<double, 2, 2, 1, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
+        if (nm == 4 && nf == 2 && ne == 2) return sweep1d_scan<double, 4, 2, 2, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
     }
-    sweep1d_dir_rt(P, gs, n, zin_b, np_source, pE, phiE_out, P.psi, ig);
+    // other shapes: one thread per direction over the whole team
+    for (int n = t.rank(); n < P.nd; n += t.size()) sweep1d_dir_rt(P, gs, n, zin_b, np_source, pE, phiE_out, P.psi, ig);
 }
 
 // ------------------------------------------------------------------------------------------
-// the pass T(z) = A·z + c (homogeneous: A·z), sn_inner_pass.jl:17-137, for 1D problems
+// the pass T(z) = A·z + c (homogeneous: A·z), sn_inner_pass.jl:17-137, for 1D problems.
+// matvec != 0 writes zout = zin − A·zin instead (the Krylov operator of sn_one_speed.jl:147).
 // ------------------------------------------------------------------------------------------
 template <class Team>
-__device__ void pass1d(const Team &t, const DevProblem &P, const GroupShared &gs, const double *zin,
-                       double *zout, int homog, int ig, const double *phiE_in, double *phiE_out) {
+__device__ void pass1d(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, double *zout, int homog,
+                       int matvec, int ig, const double *phiE_in, double *phiE_out) {
     const int nd = P.nd, np = P.np, nm = P.nm5;
     const long long ncell = P.ncell;
-    const long long nq = (long long)nd * nm * ncell;
-    // M2D with the in-group scattering and Fokker-Planck sources folded into K
-    for (long long o = t.rank(); o < nq; o += t.size()) {
-        const int n = (int)(o % nd);
-        const long long r = o / nd;  // is + nm*c
-        const long long c = r / nm;
-        const int m = P.mat[c];
-        const double *K = P.kmat + ((long long)m * nd + n) * np;
-        const double *ph = zin + r * np;
-        double s = homog ? 0.0 : P.qnout[o];
-        for (int p = 0; p < np; p++) s += K[p] * ph[p];
-        P.psi[o] = s;
+    const long long ncol = (long long)nm * ncell;  // (is, c) columns
+    // M2D: 4 directions per thread share the loads of 𝚽[:,r]
+    {
+        const int nb4 = (nd + 3) >> 2;
+        const long long nwork = (long long)nb4 * ncol;
+        for (long long o = t.rank(); o < nwork; o += t.size()) {
+            const int n0 = (int)(o % nb4) * 4;
+            const long long r = o / nb4;
+            const long long c = r / nm;
+            const int m = P.mat[c];
+            const double *ph = zin + r * np;
+            const double *K = P.kmat + ((long long)m * nd) * np;
+            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+            const int n1 = min(n0 + 1, nd - 1), n2 = min(n0 + 2, nd - 1), n3 = min(n0 + 3, nd - 1);
+            const double *K0 = K + (long long)n0 * np, *K1 = K + (long long)n1 * np;
+            const double *K2 = K + (long long)n2 * np, *K3 = K + (long long)n3 * np;
+            for (int p = 0; p < np; p++) {
+                const double v = ph[p];
+                s0 += K0[p] * v; s1 += K1[p] * v; s2 += K2[p] * v; s3 += K3[p] * v;
+            }
+            double *out = P.psi + r * nd;
+            const double *qo = P.qnout + r * nd;
+            out[n0] = (homog ? 0.0 : qo[n0]) + s0;
+            if (n0 + 1 < nd) out[n0 + 1] = (homog ? 0.0 : qo[n0 + 1]) + s1;
+            if (n0 + 2 < nd) out[n0 + 2] = (homog ? 0.0 : qo[n0 + 2]) + s2;
+            if (n0 + 3 < nd) out[n0 + 3] = (homog ? 0.0 : qo[n0 + 3]) + s3;
+        }
     }
     t.sync();
-    // sweep: one thread per direction; homogeneous passes see no surface source and a zero
-    // incoming energy flux (sn_inner_pass.jl:37-38)
+    // sweep; homogeneous passes see no surface source and a zero incoming energy flux
+    // (sn_inner_pass.jl:37-38)
     const int np_source = homog ? 0 : P.np_source;
     const double *zin_b = zin + P.off_b[0];
     const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
-    for (int n = t.rank(); n < nd; n += t.size()) sweep1d_dispatch(P, gs, n, zin_b, np_source, pE, phiE_out, ig);
+    sweep1d(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
     t.sync();
-    // D2M, accumulated in direction order as the reference does
-    const long long nphi = P.nphi;
-    for (long long o = t.rank(); o < nphi; o += t.size()) {
-        const int p = (int)(o % np);
-        const long long r = o / np;
-        const double *ps = P.psi + r * nd;
-        double s = 0.0;
-        for (int n = 0; n < nd; n++) s += P.dn[p + (long long)np * n] * ps[n];
-        zout[o] = s;
+    // D2M: 4 moments per thread share the loads of ψ[:,r]; direction order kept per output
+    {
+        const int nb4 = (np + 3) >> 2;
+        const long long nwork = (long long)nb4 * ncol;
+        for (long long o = t.rank(); o < nwork; o += t.size()) {
+            const int p0 = (int)(o % nb4) * 4;
+            const long long r = o / nb4;
+            const double *ps = P.psi + r * nd;
+            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+            const int p1 = min(p0 + 1, np - 1), p2 = min(p0 + 2, np - 1), p3 = min(p0 + 3, np - 1);
+            for (int n = 0; n < nd; n++) {
+                const double v = ps[n];
+                const double *D = P.dn + (long long)np * n;
+                s0 += D[p0] * v; s1 += D[p1] * v; s2 += D[p2] * v; s3 += D[p3] * v;
+            }
+            const long long b = r * np;
+            if (matvec) {
+                zout[b + p0] = zin[b + p0] - s0;
+                if (p0 + 1 < np) zout[b + p0 + 1] = zin[b + p0 + 1] - s1;
+                if (p0 + 2 < np) zout[b + p0 + 2] = zin[b + p0 + 2] - s2;
+                if (p0 + 3 < np) zout[b + p0 + 3] = zin[b + p0 + 3] - s3;
+            } else {
+                zout[b + p0] = s0;
+                if (p0 + 1 < np) zout[b + p0 + 1] = s1;
+                if (p0 + 2 < np) zout[b + p0 + 2] = s2;
+                if (p0 + 3 < np) zout[b + p0 + 3] = s3;
+            }
+        }
     }
     // outgoing boundary moments: side 1 (X+) collects μ ≥ 0, side 0 (X-) μ < 0
     const int nf = P.nmf[0], nps = P.npsurf;
@@ -425,7 +586,8 @@ __device__ void pass1d(const Team &t, const DevProblem &P, const GroupShared &gs
             if ((side == 1) == fwd)
                 s += P.frow_d[(long long)nps * n + p] * P.fexit[(long long)n * RB_MAXFACE + is];
         }
-        zout[P.off_b[0] + o] = s;
+        const long long k = P.off_b[0] + o;
+        zout[k] = matvec ? zin[k] - s : s;
     }
     t.sync();
 }

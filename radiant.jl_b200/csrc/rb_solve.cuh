@@ -1,11 +1,12 @@
-// rb_solve.cuh -- in-group accelerators and the group loop, run by one team per problem.
+// rb_solve.cuh -- in-group accelerators and the group loop, run by one team (cluster) per problem.
 //
 // Restates on the device: livolant! (src/tools/livolant.jl:110-154), anderson!
 // (src/tools/anderson.jl:38-140), gmres! (src/tools/gmres.jl:35-133), bicgstab!
 // (src/tools/bicgstab.jl:30-101), sn_one_speed (sn_one_speed.jl:81-195) and the group loop of
 // compute_flux(::SN) (sn_flux.jl:146-224). Every scalar decision (convergence tests,
-// Hessenberg, Givens, Anderson normal equations) is taken from team reductions whose bits
-// are identical in every thread, so the team's threads always branch together.
+// Hessenberg, Givens, Anderson normal equations) is taken from team reductions whose bits are
+// identical in every thread, so all threads of the cluster branch together; each CTA keeps its
+// own copy of the small scalar arrays, updated by its leader thread.
 #pragma once
 #include <math_constants.h>
 
@@ -25,10 +26,9 @@ __device__ __forceinline__ double rho_estimate(double r0, double r, int it) {  /
     return CUDART_NAN;
 }
 
-// One problem in flight on one team.
 template <class Team>
 struct Solver {
-    const Team &t;
+    Team &t;
     const DevProblem &P;
     GroupShared &gs;
     int ig;
@@ -38,51 +38,59 @@ struct Solver {
 
     __device__ double *vec(int k) const { return P.vecs + (long long)k * P.nstate; }
 
-    // load_and_pass! (sn_one_speed.jl:138-143): out <- T(zin) or A·zin
-    __device__ void pass(const double *zin, double *out, int homog) {
-        pass1d(t, P, gs, zin, out, homog, ig, phiE_in, phiE_out);
+    // load_and_pass! (sn_one_speed.jl:138-143): out <- T(zin)
+    __device__ void fixedpoint(double *out, const double *zin) {
+        pass1d(t, P, gs, zin, out, 0, 0, ig, phiE_in, phiE_out);
         npass++;
     }
-    __device__ void fixedpoint(double *out, const double *zin) { pass(zin, out, 0); }
-    // matvec! : out <- zin - A·zin
+    // matvec! (sn_one_speed.jl:147): out <- zin − A·zin
     __device__ void matvec(double *out, const double *zin) {
-        pass(zin, out, 1);
-        vlin(t, 1.0, zin, -1.0, out, P.nstate);
+        pass1d(t, P, gs, zin, out, 1, 1, ig, phiE_in, phiE_out);
+        npass++;
     }
     __device__ double norm(const double *a) { return sqrt(vdot(t, a, a, P.nstate)); }
 
     // ---------------------------------------------------------------- livolant (and "none")
     __device__ SolveStat livolant(double *z, int maxit, double tol, int period) {
         const long long N = P.nstate;
-        double *g = vec(1), *f = vec(2), *z1 = vec(3), *z0 = vec(4);
-        vzero(t, z1, N); vzero(t, z0, N);
+        double *g = vec(1), *z1 = vec(3), *z0 = vec(4);
         int nhist = 0, iter = 0, conv = 0;
         double resid = 1.0, resid0 = CUDART_NAN;
         for (int it = 1; it <= maxit; it++) {
             fixedpoint(g, z); iter++;
-            // f = g - z (state_copy!(f,g); state_axpy!(-1,z,f))
-            for (long long i = t.rank(); i < N; i += t.size()) f[i] = g[i] + (-1.0) * z[i];
-            t.sync();
-            double fnorm = norm(f);
-            double scale = fmax(norm(g), 1e-16);
-            resid = fnorm / scale;
+            // ‖g − z‖ and ‖g‖ in one reduction
+            double v[2] = {0.0, 0.0};
+            for (long long i = t.rank(); i < N; i += t.size()) {
+                const double f = g[i] + (-1.0) * z[i];
+                v[0] += f * f; v[1] += g[i] * g[i];
+            }
+            t.template sumk<2>(v);
+            resid = sqrt(v[0]) / fmax(sqrt(v[1]), 1e-16);
             if (isnan(resid0)) resid0 = resid;
             if (resid < tol) { vcopy(t, z, g, N); conv = 1; break; }
             if (period > 0 && it % period == 0 && nhist >= 2) {
-                double se = 0.0, sd = 0.0;
+                double w[2] = {0.0, 0.0};
                 for (long long i = t.rank(); i < N; i += t.size()) {
-                    double e0 = z1[i] - z0[i], e1 = g[i] - z1[i], de = e1 - e0;
-                    se += e0 * de; sd += de * de;
+                    const double e0 = z1[i] - z0[i], e1 = g[i] - z1[i], de = e1 - e0;
+                    w[0] += e0 * de; w[1] += de * de;
                 }
-                se = t.sum(se); sd = t.sum(sd);
+                t.template sumk<2>(w);
                 double mu = 1.0;
-                if (sd != 0.0) { mu = -se / sd; if (mu <= 0) mu = 1.0; }
-                for (long long i = t.rank(); i < N; i += t.size()) z[i] = g[i] * mu + (1.0 - mu) * z1[i];
-                t.sync();
+                if (w[1] != 0.0) { mu = -w[0] / w[1]; if (mu <= 0) mu = 1.0; }
+                for (long long i = t.rank(); i < N; i += t.size()) {
+                    z[i] = g[i] * mu + (1.0 - mu) * z1[i];
+                    z0[i] = z1[i];
+                    z1[i] = g[i];
+                }
             } else {
-                vcopy(t, z, g, N);
+                for (long long i = t.rank(); i < N; i += t.size()) {
+                    z[i] = g[i];
+                    z0[i] = z1[i];
+                    z1[i] = g[i];
+                }
             }
-            vcopy(t, z0, z1, N); vcopy(t, z1, g, N); nhist++;
+            t.sync();
+            nhist++;
         }
         SolveStat s = {iter, resid, conv, rho_estimate(resid0, resid, iter)};
         return s;
@@ -93,23 +101,26 @@ struct Solver {
         const long long N = P.nstate;
         const int m = depth > 1 ? depth : 1;
         double *g = vec(1), *f = vec(2), *fo = vec(3), *go = vec(4);
-        // history ring: logical i -> slot (head + i) % m; dF slot s = vec(5+s), dG = vec(5+m+s)
+        // history ring: logical i -> slot (head + i) % m; ΔF slot s = vec(5+s), ΔG = vec(5+m+s)
         int nh = 0, head = 0, iter = 0, conv = 0;
         double resid = 1.0, resid0 = CUDART_NAN;
         for (int it = 1; it <= maxit; it++) {
             fixedpoint(g, z); iter++;
-            for (long long i = t.rank(); i < N; i += t.size()) f[i] = g[i] + (-1.0) * z[i];
-            t.sync();
-            double fnorm = norm(f);
-            double scale = fmax(fmax(norm(z), norm(g)), 1e-16);
-            resid = fnorm / scale;
+            double v[3] = {0.0, 0.0, 0.0};
+            for (long long i = t.rank(); i < N; i += t.size()) {
+                const double fi = g[i] + (-1.0) * z[i];
+                f[i] = fi;
+                v[0] += fi * fi; v[1] += z[i] * z[i]; v[2] += g[i] * g[i];
+            }
+            t.template sumk<3>(v);
+            resid = sqrt(v[0]) / fmax(fmax(sqrt(v[1]), sqrt(v[2])), 1e-16);
             if (isnan(resid0)) resid0 = resid;
             if (resid < tol) { conv = 1; break; }
             if (it == 1) {
                 vaxpy(t, 1.0, f, z, N);
             } else {
                 if (nh == m) { head = (head + 1) % m; nh--; }  // popfirst!
-                int slot = (head + nh) % m;
+                const int slot = (head + nh) % m;
                 double *dF = vec(5 + slot), *dG = vec(5 + m + slot);
                 for (long long i = t.rank(); i < N; i += t.size()) {
                     dF[i] = f[i] + (-1.0) * fo[i];
@@ -121,21 +132,20 @@ struct Solver {
                 for (int i = 0; i < mk; i++) {
                     const double *dFi = vec(5 + (head + i) % m);
                     double bi = vdot(t, dFi, f, N);
-                    if (t.rank() == 0) gs.b[i] = bi;
+                    if (t.leader()) gs.b[i] = bi;
                     for (int j = 0; j < mk; j++) {
                         double aij = vdot(t, dFi, vec(5 + (head + j) % m), N);
-                        if (t.rank() == 0) gs.A[i + mk * j] = aij;
+                        if (t.leader()) gs.A[i + mk * j] = aij;
                     }
                 }
-                t.sync();
-                if (t.rank() == 0) {
+                __syncthreads();
+                if (t.leader()) {
                     double *A = gs.A, *x = gs.b;
                     double tr = 0.0;
                     for (int i = 0; i < mk; i++) tr += A[i + mk * i];
-                    double lam = 1e-12 * (tr / mk + 1e-300);
+                    const double lam = 1e-12 * (tr / mk + 1e-300);
                     for (int i = 0; i < mk; i++) A[i + mk * i] += lam;
-                    // anderson_solve (anderson.jl:112-140)
-                    const int n = mk;
+                    const int n = mk;  // anderson_solve (anderson.jl:112-140)
                     for (int k = 0; k < n; k++) {
                         int p = k; double mx = fabs(A[k + n * k]);
                         for (int i = k + 1; i < n; i++) if (fabs(A[i + n * k]) > mx) { mx = fabs(A[i + n * k]); p = i; }
@@ -143,10 +153,10 @@ struct Solver {
                             for (int j = k; j < n; j++) { double tt = A[k + n * j]; A[k + n * j] = A[p + n * j]; A[p + n * j] = tt; }
                             double tt = x[k]; x[k] = x[p]; x[p] = tt;
                         }
-                        double piv = A[k + n * k];
+                        const double piv = A[k + n * k];
                         if (piv == 0.0) continue;
                         for (int i = k + 1; i < n; i++) {
-                            double fac = A[i + n * k] / piv;
+                            const double fac = A[i + n * k] / piv;
                             for (int j = k; j < n; j++) A[i + n * j] -= fac * A[k + n * j];
                             x[i] -= fac * x[k];
                         }
@@ -157,16 +167,17 @@ struct Solver {
                         x[k] = A[k + n * k] != 0.0 ? s / A[k + n * k] : 0.0;
                     }
                 }
-                t.sync();
-                vaxpy(t, 1.0, f, z, N);
-                for (int i = 0; i < mk; i++) {
-                    const double gam = gs.b[i];
-                    vaxpy(t, -gam, vec(5 + m + (head + i) % m), z, N);
-                    // β - 1 = 0: the ΔF term adds -(0)·γ·ΔF, kept for operation parity
-                    vaxpy(t, -(1.0 - 1.0) * gam, vec(5 + (head + i) % m), z, N);
+                __syncthreads();
+                // z ← z + f − Σ γ_i ΔG_i  (β = 1: the ΔF term carries a zero factor)
+                for (long long i = t.rank(); i < N; i += t.size()) {
+                    double zi = z[i] + 1.0 * f[i];
+                    for (int k = 0; k < mk; k++) zi += -gs.b[k] * vec(5 + m + (head + k) % m)[i];
+                    z[i] = zi;
                 }
+                t.sync();
             }
-            vcopy(t, fo, f, N); vcopy(t, go, g, N);
+            for (long long i = t.rank(); i < N; i += t.size()) { fo[i] = f[i]; go[i] = g[i]; }
+            t.sync();
         }
         SolveStat s = {iter, resid, conv, rho_estimate(resid0, resid, iter)};
         return s;
@@ -177,7 +188,7 @@ struct Solver {
         const long long N = P.nstate;
         const int m = restart > 1 ? restart : 1;
         SolveStat st = {0, 0.0, 1, CUDART_NAN};
-        double bnorm = norm(rhs);
+        const double bnorm = norm(rhs);
         if (bnorm == 0.0) { vzero(t, z, N); return st; }
         double *r = vec(2), *w = vec(3);
         double *H = gs.H;
@@ -186,17 +197,23 @@ struct Solver {
         double resid = 1.0, resid0 = CUDART_NAN;
         while (iter < maxit && !conv) {
             matvec(r, z); iter++;
-            vlin(t, 1.0, rhs, -1.0, r, N);  // r = c - M z
-            double beta = norm(r);
+            double v1[1] = {0.0};
+            for (long long i = t.rank(); i < N; i += t.size()) {  // r = c − M z
+                const double ri = rhs[i] - r[i];
+                r[i] = ri;
+                v1[0] += ri * ri;
+            }
+            t.template sumk<1>(v1);
+            const double beta = sqrt(v1[0]);
             resid = beta / bnorm;
             if (isnan(resid0)) resid0 = resid;
             if (resid < tol) { conv = 1; break; }
             {
-                double inv = 1.0 / beta;
+                const double inv = 1.0 / beta;
                 double *V0 = vec(4);
                 for (long long i = t.rank(); i < N; i += t.size()) V0[i] = r[i] * inv;
             }
-            if (t.rank() == 0) {
+            if (t.leader()) {
                 for (int i = 0; i <= m; i++) gs.g[i] = 0.0;
                 gs.g[0] = beta;
             }
@@ -205,25 +222,36 @@ struct Solver {
             for (int j = 0; j < m; j++) {
                 if (iter >= maxit) break;
                 matvec(w, vec(4 + j)); iter++;
-                for (int i = 0; i <= j; i++) {  // modified Gram-Schmidt
-                    double h = vdot(t, w, vec(4 + i), N);
-                    if (t.rank() == 0) HH(i, j) = h;
-                    vaxpy(t, -h, vec(4 + i), w, N);
+                // modified Gram-Schmidt, one sweep per basis vector: w ← w − h_i V_i fused with
+                // the dot product of the updated w against V_{i+1} (or against itself at the end)
+                double h = vdot(t, w, vec(4), N);
+                for (int i = 0; i <= j; i++) {
+                    if (t.leader()) HH(i, j) = h;
+                    const double *Vi = vec(4 + i);
+                    const double *Vn = (i < j) ? vec(4 + i + 1) : nullptr;
+                    double acc[1] = {0.0};
+                    for (long long q = t.rank(); q < N; q += t.size()) {
+                        const double wq = w[q] + (-h) * Vi[q];
+                        w[q] = wq;
+                        acc[0] += wq * (Vn ? Vn[q] : wq);
+                    }
+                    t.template sumk<1>(acc);
+                    h = acc[0];
                 }
-                double hjp1 = norm(w);
+                const double hjp1 = sqrt(h);
                 if (hjp1 > 0.0) {
-                    double inv = 1.0 / hjp1;
+                    const double inv = 1.0 / hjp1;
                     double *Vn = vec(4 + j + 1);
-                    for (long long i = t.rank(); i < N; i += t.size()) Vn[i] = w[i] * inv;
+                    for (long long q = t.rank(); q < N; q += t.size()) Vn[q] = w[q] * inv;
                 }
-                if (t.rank() == 0) {
+                if (t.leader()) {
                     HH(j + 1, j) = hjp1;
                     for (int i = 0; i < j; i++) {
-                        double temp = gs.cs[i] * HH(i, j) + gs.sn[i] * HH(i + 1, j);
+                        const double temp = gs.cs[i] * HH(i, j) + gs.sn[i] * HH(i + 1, j);
                         HH(i + 1, j) = -gs.sn[i] * HH(i, j) + gs.cs[i] * HH(i + 1, j);
                         HH(i, j) = temp;
                     }
-                    double denom = hypot(HH(j, j), HH(j + 1, j));
+                    const double denom = hypot(HH(j, j), HH(j + 1, j));
                     if (denom == 0.0) { gs.cs[j] = 1.0; gs.sn[j] = 0.0; }
                     else { gs.cs[j] = HH(j, j) / denom; gs.sn[j] = HH(j + 1, j) / denom; }
                     HH(j, j) = gs.cs[j] * HH(j, j) + gs.sn[j] * HH(j + 1, j);
@@ -237,15 +265,21 @@ struct Solver {
                 if (resid < tol) { conv = 1; break; }
                 if (hjp1 == 0.0) break;
             }
-            if (t.rank() == 0) {
+            if (t.leader()) {
                 for (int i = k - 1; i >= 0; i--) {
                     double s = gs.g[i];
                     for (int l = i + 1; l < k; l++) s -= HH(i, l) * gs.y[l];
                     gs.y[i] = HH(i, i) != 0.0 ? s / HH(i, i) : 0.0;
                 }
             }
+            __syncthreads();
+            // z += Σ y_i V_i, in basis order per element
+            for (long long q = t.rank(); q < N; q += t.size()) {
+                double zq = z[q];
+                for (int i = 0; i < k; i++) zq += gs.y[i] * vec(4 + i)[q];
+                z[q] = zq;
+            }
             t.sync();
-            for (int i = 0; i < k; i++) vaxpy(t, gs.y[i], vec(4 + i), z, N);
             if (conv) break;
         }
 #undef HH
@@ -257,32 +291,40 @@ struct Solver {
     __device__ SolveStat bicgstab(double *z, const double *rhs, int maxit, double tol) {
         const long long N = P.nstate;
         SolveStat st = {0, 0.0, 1, CUDART_NAN};
-        double bnorm = norm(rhs);
+        const double bnorm = norm(rhs);
         if (bnorm == 0.0) { vzero(t, z, N); return st; }
         double *r = vec(2), *rh = vec(3), *p = vec(4), *v = vec(5), *s = vec(6), *tt = vec(7);
         matvec(r, z);
-        vlin(t, 1.0, rhs, -1.0, r, N);
+        double a1[1] = {0.0};
+        for (long long i = t.rank(); i < N; i += t.size()) {
+            const double ri = rhs[i] - r[i];
+            r[i] = ri; rh[i] = ri; p[i] = 0.0; v[i] = 0.0;
+            a1[0] += ri * ri;
+        }
+        t.template sumk<1>(a1);
         int iter = 1, conv = 0;
-        double resid = norm(r) / bnorm, resid0 = resid;
+        double resid = sqrt(a1[0]) / bnorm, resid0 = resid;
         if (resid < tol) { st.iter = iter; st.resid = resid; st.conv = 1; st.rho = CUDART_NAN; return st; }
-        vcopy(t, rh, r, N);
-        vzero(t, p, N); vzero(t, v, N);
         double rho_old = 1.0, alpha = 1.0, omega = 1.0;
         const double tiny = 1e-300;
         while (iter < maxit) {
-            double rho_new = vdot(t, rh, r, N);
+            const double rho_new = vdot(t, rh, r, N);
             if (fabs(rho_new) < tiny) break;
-            double beta = (rho_new / rho_old) * (alpha / omega);
-            // p ← r + β (p − ω v)
+            const double beta = (rho_new / rho_old) * (alpha / omega);
             for (long long i = t.rank(); i < N; i += t.size()) p[i] = r[i] + 1.0 * (beta * (p[i] + (-omega) * v[i]));
             t.sync();
             matvec(v, p); iter++;
-            double denom = vdot(t, rh, v, N);
+            const double denom = vdot(t, rh, v, N);
             if (fabs(denom) < tiny) break;
             alpha = rho_new / denom;
-            for (long long i = t.rank(); i < N; i += t.size()) s[i] = r[i] + (-alpha) * v[i];
-            t.sync();
-            double sn_ = norm(s);
+            double a2[1] = {0.0};
+            for (long long i = t.rank(); i < N; i += t.size()) {
+                const double si = r[i] + (-alpha) * v[i];
+                s[i] = si;
+                a2[0] += si * si;
+            }
+            t.template sumk<1>(a2);
+            const double sn_ = sqrt(a2[0]);
             if (sn_ / bnorm < tol) {
                 vaxpy(t, alpha, p, z, N);
                 resid = sn_ / bnorm;
@@ -290,15 +332,20 @@ struct Solver {
                 break;
             }
             matvec(tt, s); iter++;
-            double ttd = vdot(t, tt, tt, N);
-            if (ttd < tiny) break;
-            omega = vdot(t, tt, s, N) / ttd;
+            double a3[2] = {0.0, 0.0};
+            for (long long i = t.rank(); i < N; i += t.size()) { a3[0] += tt[i] * tt[i]; a3[1] += tt[i] * s[i]; }
+            t.template sumk<2>(a3);
+            if (a3[0] < tiny) break;
+            omega = a3[1] / a3[0];
+            double a4[1] = {0.0};
             for (long long i = t.rank(); i < N; i += t.size()) {
                 z[i] = (z[i] + alpha * p[i]) + omega * s[i];
-                r[i] = s[i] + (-omega) * tt[i];
+                const double ri = s[i] + (-omega) * tt[i];
+                r[i] = ri;
+                a4[0] += ri * ri;
             }
-            t.sync();
-            resid = norm(r) / bnorm;
+            t.template sumk<1>(a4);
+            resid = sqrt(a4[0]) / bnorm;
             if (resid < tol) { conv = 1; break; }
             if (fabs(omega) < tiny) break;
             rho_old = rho_new;
@@ -316,21 +363,21 @@ struct Solver {
         for (int f = 0; f < 2 * P.ndims; f++) {
             const double *src = P.surf[f];
             if (!src) continue;
-            long long fc = P.ndims == 1 ? 1 : 0;  // 1D faces hold one cell
-            for (long long k = t.rank(); k < (long long)P.np_source * fc; k += t.size())
+            for (long long k = t.rank(); k < (long long)P.np_source; k += t.size())
                 if (src[ig + (long long)P.ng * k] != 0.0) any = 1;
         }
         for (long long i = t.rank(); i < nphi; i += t.size()) if (P.qlout[i] != 0.0) any = 1;
         if (P.csd) for (long long i = t.rank(); i < nE; i += t.size()) if (phiE_in[i] != 0.0) any = 1;
         any = t.any(any);
         if (!any) {
-            vzero(t, flux_g, nphi);
-            if (P.csd) vzero(t, phiE_out, nE);
+            for (long long i = t.rank(); i < nphi; i += t.size()) flux_g[i] = 0.0;
+            if (P.csd) for (long long i = t.rank(); i < nE; i += t.size()) phiE_out[i] = 0.0;
+            t.sync();
             SolveStat s = {1, 0.0, 1, CUDART_NAN};
             return s;
         }
         double *z = vec(0);
-        vzero(t, z, N);  // initial state (𝚽l of the group = 0, boundary in-moments = 0)
+        vzero(t, z, N);  // initial state: 𝚽l of the group = 0, boundary in-moments = 0
         SolveStat st;
         if (P.accel == 0 || P.accel == 1) {
             st = livolant(z, P.maxit, P.tol, P.accel == 0 ? 0 : 3);
@@ -338,13 +385,13 @@ struct Solver {
             st = anderson(z, P.depth, P.maxit, P.tol);
         } else {
             double *rhs = vec(1);
-            pass(z, rhs, 0);  // c = T(0)
+            fixedpoint(rhs, z);  // c = T(0)
             if (P.accel == 3) st = gmres(z, rhs, P.restart, P.maxit, P.tol);
             else st = bicgstab(z, rhs, P.maxit, P.tol);
         }
         // reconstruction pass (sn_one_speed.jl:184-187)
         double *out = vec(1);
-        pass(z, out, 0);
+        fixedpoint(out, z);
         vcopy(t, flux_g, out, nphi);
         return st;
     }
@@ -354,7 +401,7 @@ struct Solver {
 // the group loop of compute_flux(::SN) for one problem (sn_flux.jl:146-224)
 // ------------------------------------------------------------------------------------------
 template <class Team>
-__device__ void solve_problem(const Team &t, const DevProblem &P, GroupShared &gs) {
+__device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs) {
     const int ng = P.ng, nmat = P.nmat, np = P.np, nd = P.nd, nm = P.nm5;
     const long long nphi = P.nphi, ncell = P.ncell;
     const long long nE = (long long)nd * P.nm4 * ncell;
@@ -363,8 +410,8 @@ __device__ void solve_problem(const Team &t, const DevProblem &P, GroupShared &g
     if (P.csd) { vzero(t, phiE_in, nE); vzero(t, phiE_out, nE); }
     long long npass = 0;
     for (int ig = 0; ig < ng; ig++) {
-        // per-group constants
-        for (int m = t.rank(); m < nmat; m += t.size()) {
+        // per-group constants, one copy per CTA
+        for (int m = threadIdx.x; m < nmat; m += blockDim.x) {
             gs.sigt[m] = P.sigma_t[ig + (long long)ng * m];
             if (P.csd) {
                 const double dE = P.e_width[ig];
@@ -375,7 +422,7 @@ __device__ void solve_problem(const Team &t, const DevProblem &P, GroupShared &g
             }
             gs.tg[m] = (st_ == 2 || st_ == 4) ? P.t_mom[ig + (long long)ng * m] : 0.0;
         }
-        t.sync();
+        __syncthreads();
         if (P.csd) {  // CSD block of the cell matrix: Σ_w (S_w/ΔE)·K_w + (S⁺/ΔE)·B
             const int nn = nm * nm;
             for (long long o = t.rank(); o < (long long)nmat * nn; o += t.size()) {
@@ -409,9 +456,8 @@ __device__ void solve_problem(const Team &t, const DevProblem &P, GroupShared &g
             const int m = P.mat[c];
             double q = 0.0;
             if (st_ != 4 && st_ != 5) {
-                for (int gi = 0; gi < ig; gi++)
-                    q += P.sigma_s[m + (long long)nmat * (gi + (long long)ng * (ig + (long long)ng * P.pl[p]))] *
-                         P.flux[(long long)gi * nphi + o];
+                const double *ss = P.sigma_s + m + (long long)nmat * (long long)ng * (ig + (long long)ng * P.pl[p]);
+                for (int gi = 0; gi < ig; gi++) q += ss[(long long)nmat * gi] * P.flux[(long long)gi * nphi + o];
             }
             if (P.vol) q += P.vol[(long long)ig * nphi + o];
             P.qlout[o] = q;
@@ -459,21 +505,20 @@ __device__ void solve_problem(const Team &t, const DevProblem &P, GroupShared &g
 }
 
 // ------------------------------------------------------------------------------------------
-// persistent batch kernel: CTAs pull problems from a device work queue
+// persistent batch kernel: clusters pull problems from a device work queue
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(RB_THREADS) solve_batch_kernel(DevProblem *const *probs, int nprob,
                                                                  int *queue) {
-    __shared__ GroupShared gs;
-    __shared__ int next;
-    CtaTeam t{gs.red};
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
+    ClusterTeam t;
+    t.init(&gs.team);
     while (true) {
-        if (threadIdx.x == 0) next = atomicAdd(queue, 1);
-        __syncthreads();
-        const int idx = next;
-        __syncthreads();
+        int idx = 0;
+        if (t.crank == 0 && threadIdx.x == 0) idx = atomicAdd(queue, 1);
+        idx = t.broadcast_from_leader(idx);
         if (idx >= nprob) break;
-        const DevProblem *pp = probs[idx];
-        solve_problem(t, *pp, gs);
+        solve_problem(t, *probs[idx], gs);
     }
 }
 

@@ -1,0 +1,90 @@
+// rb_team.cuh -- the team that owns one problem: one thread-block cluster.
+//
+// Every phase of a transport pass and every vector operation of the in-group accelerators is
+// spread over all threads of the cluster; team barriers are hardware cluster barriers.
+// Reductions are deterministic and give the same bits in every thread of every CTA: each warp
+// reduces by xor butterfly (commutative pairs, identical in all lanes), each CTA sums its warps
+// in a fixed order into a shared slot, and after one cluster barrier every thread adds the CTAs'
+// slots in rank order through distributed shared memory. Slots alternate between two buffers,
+// so a reduction costs one cluster barrier. All threads run the same control flow, which the
+// identical reduction bits guarantee, so no CTA can leave a barrier sequence early.
+#pragma once
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+namespace rb {
+namespace cg = cooperative_groups;
+
+struct TeamShared {
+    double part[2][4];  // per-CTA partial sums, double-buffered, up to 4 values per reduction
+    double warp[32][4];
+    int idx;            // problem index broadcast by the cluster leader
+};
+
+struct ClusterTeam {
+    TeamShared *sh;
+    unsigned crank;   // CTA rank in the cluster
+    unsigned ncta;    // CTAs in the cluster
+    int phase;        // reduction counter (selects the slot)
+
+    __device__ void init(TeamShared *s) {
+        sh = s;
+        cg::cluster_group cl = cg::this_cluster();
+        crank = cl.block_rank();
+        ncta = cl.num_blocks();
+        phase = 0;
+    }
+    __device__ __forceinline__ int rank() const { return (int)(crank * blockDim.x + threadIdx.x); }
+    __device__ __forceinline__ int size() const { return (int)(ncta * blockDim.x); }
+    __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }  // one per CTA
+    __device__ __forceinline__ void sync() const { cg::this_cluster().sync(); }
+
+    // Sum of K values over the team (K <= 4); every thread gets identical bits.
+    template <int K>
+    __device__ void sumk(double (&v)[K]) {
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int k = 0; k < K; k++) sh->warp[w][k] = v[k];
+        __syncthreads();
+        const int slot = phase & 1;
+        phase++;
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                double s = 0.0;
+                for (int i = 0; i < nw; i++) s += sh->warp[i][k];
+                sh->part[slot][k] = s;
+            }
+        }
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();
+#pragma unroll
+        for (int k = 0; k < K; k++) v[k] = 0.0;
+        for (unsigned r = 0; r < ncta; r++) {
+            const double *p = cl.map_shared_rank(&sh->part[slot][0], r);
+#pragma unroll
+            for (int k = 0; k < K; k++) v[k] += p[k];
+        }
+    }
+    __device__ double sum(double v) {
+        double a[1] = {v};
+        sumk<1>(a);
+        return a[0];
+    }
+    __device__ int any(int flag) { return sum(flag ? 1.0 : 0.0) > 0.0; }
+    // Index handed out by the cluster leader (CTA 0, thread 0) to the whole cluster.
+    __device__ int broadcast_from_leader(int v) {
+        cg::cluster_group cl = cg::this_cluster();
+        if (crank == 0 && threadIdx.x == 0) sh->idx = v;
+        cl.sync();
+        const int r = *cl.map_shared_rank(&sh->idx, 0);
+        cl.sync();
+        return r;
+    }
+};
+
+}  // namespace rb
