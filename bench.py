@@ -54,6 +54,8 @@ def workload_tables(seeds, precision, workload="c2"):
     tabs = []
     if workload == "c1":  # small case (profiling): the 1D photon BTE slab, one solve per seed
         return [W.c1_tables(seed=s, precision=precision) for s in seeds]
+    if workload == "c2e8":  # small case (profiling): the electron BFP solve of the workload, 8 groups
+        return [W.c2_tables(seed=s, precision=precision, ng=8) for s in seeds]
     for s in seeds:
         for part in ("photon", "electron", "positron"):
             t = W.c2_tables(seed=s * 3 + {"photon": 0, "electron": 1, "positron": 2}[part], precision=precision,
@@ -299,12 +301,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--seeds", type=int, default=50)
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1"],
-                    help="c2: the benchmark workload; c1: the small photon slab (profiling captures)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2e8"],
+                    help="c2: the benchmark workload; c1 / c2e8: small cases for profiling captures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cluster", type=int, default=0, help="CTAs per problem team (0: library default)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.cluster:
+        os.environ["RB_CLUSTER_SIZE"] = str(args.cluster)
     if args.impl == "reference":
         if rank != 0:
             return 0

@@ -115,14 +115,14 @@ def c1_tables(seed: int = 1, precision: str = "fp64", accel: str = "gmres"):
                        precision=precision)
 
 
-def c2_tables(seed: int = 1, precision: str = "fp64", accel: str = "gmres", particle: str = "electron"):
+def c2_tables(seed: int = 1, precision: str = "fp64", accel: str = "gmres", particle: str = "electron",
+              ng: int = 80):
     """1D slab BFP: water 0-3 cm / bone 3-5 cm / water 5-15 cm, 300 voxels of 0.05 cm,
     80 groups, S32 Gauss-Legendre, P15, linear DG in x and in E, Galerkin (moment-preserving)
     angular Fokker-Planck, normal beam in the group holding 6 MeV."""
     nx = 300
     mats = np.ones(nx, dtype=np.int32)
     mats[60:100] = 2
-    ng = 80
     eb, e, de = log_groups(ng, 20.0, 0.001)
     g6 = int(np.nonzero((eb[:-1] >= 6.0) & (eb[1:] < 6.0))[0][0])
     if particle == "photon":
