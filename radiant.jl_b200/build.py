@@ -27,7 +27,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
+           "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr", "--extended-lambda",
            os.path.join(CSRC, "rb_capi.cu"), "-o", OUT, "-lcudart"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

@@ -388,7 +388,7 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     offs[k++] = L.take<double>(D.nphi);                   // 34 qlout
     offs[k++] = L.take<double>(nq);                       // 35 qnout
     offs[k++] = L.take<double>(nq);                       // 36 psi
-    offs[k++] = L.take<double>((size_t)nmat * nd * np);   // 37 kmat
+    offs[k++] = L.take<double>((size_t)nmat * np);        // 37 kmat (in-group Σs per material and moment)
     offs[k++] = L.take<double>((size_t)nmat * nm5 * nm5); // 38 scsd
     offs[k++] = L.take<double>((size_t)nd * RB_MAXFACE);  // 39 fexit
     offs[k++] = L.take<double>(D.csd ? nE : 0);           // 40 phiE_a

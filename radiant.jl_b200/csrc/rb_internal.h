@@ -63,7 +63,7 @@ struct DevProblem {
     double *qnout;     // [nd*nm5*ncell] Mn·Qlout
     double *psi;       // [nd*nm5*ncell] angular source / angular flux (in place)
     float *psi32;      // [nd*nm5*ncell] mixed form: FP32 angular source / flux
-    double *kmat;      // [nmat][nd][np] per-group Mn·(Σs_l + T·ℳ)
+    double *kmat;      // [nmat][np] per-group in-group Σs of each moment's Legendre order
     double *scsd;      // [nmat][nm5*nm5] per-group CSD part of the cell matrix
     double *fexit;     // [nd][RB_MAXFACE] 1D exit faces
     double *phiE_a, *phiE_b; // [nd*nm4*ncell] energy-face fluxes (in / out, swapped per group)

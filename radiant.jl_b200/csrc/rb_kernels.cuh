@@ -25,26 +25,53 @@
 #define RB_THREADS 256
 #define RB_SCAN_NF 4      // scan path for face-moment counts up to this
 #define RB_MAXCLUSTER 16
+#define RB_TILE_DOUBLES (RB_THREADS * (RB_SCAN_NF * RB_SCAN_NF + 2 * RB_SCAN_NF))
 
 namespace rb {
 
 // ------------------------------------------------------------------------------------------
-// state algebra (krylov_state.jl:53-114) over [𝚽 | boundary in-moments]
+// state algebra (krylov_state.jl:53-114) over [𝚽 | boundary in-moments]. Every loop issues the
+// loads of four strided elements before using them, so each thread keeps four memory requests
+// in flight instead of one.
 // ------------------------------------------------------------------------------------------
+#define RB_VLOOP4(t, N, LOAD, USE)                                                         \
+    {                                                                                      \
+        const long long T_ = (t).size();                                                   \
+        long long q0_ = (t).rank();                                                        \
+        for (; q0_ + 3 * T_ < (N); q0_ += 4 * T_) {                                        \
+            _Pragma("unroll") for (int u_ = 0; u_ < 4; u_++) {                             \
+                const long long q = q0_ + u_ * T_;                                         \
+                LOAD                                                                       \
+            }                                                                              \
+            _Pragma("unroll") for (int u_ = 0; u_ < 4; u_++) {                             \
+                const long long q = q0_ + u_ * T_;                                         \
+                USE                                                                        \
+            }                                                                              \
+        }                                                                                  \
+        for (; q0_ < (N); q0_ += T_) {                                                     \
+            const int u_ = 0;                                                              \
+            const long long q = q0_;                                                       \
+            LOAD                                                                           \
+            USE                                                                            \
+        }                                                                                  \
+    }
+
 template <class Team>
 __device__ double vdot(Team &t, const double *a, const double *b, long long n) {
-    double s = 0.0;
-    for (long long i = t.rank(); i < n; i += t.size()) s += a[i] * b[i];
+    double s = 0.0, xa[4], xb[4];
+    RB_VLOOP4(t, n, { xa[u_] = a[q]; xb[u_] = b[q]; }, { s += xa[u_] * xb[u_]; (void)q; })
     return t.sum(s);
 }
 template <class Team>
 __device__ void vaxpy(Team &t, double al, const double *x, double *y, long long n) {
-    for (long long i = t.rank(); i < n; i += t.size()) y[i] += al * x[i];
+    double xx[4], yy[4];
+    RB_VLOOP4(t, n, { xx[u_] = x[q]; yy[u_] = y[q]; }, { y[q] = yy[u_] + al * xx[u_]; })
     t.sync();
 }
 template <class Team>
 __device__ void vcopy(Team &t, double *d, const double *s, long long n) {
-    for (long long i = t.rank(); i < n; i += t.size()) d[i] = s[i];
+    double xx[4];
+    RB_VLOOP4(t, n, { xx[u_] = s[q]; }, { d[q] = xx[u_]; })
     t.sync();
 }
 template <class Team>
@@ -55,7 +82,8 @@ __device__ void vzero(Team &t, double *d, long long n) {
 // y = a·x + b·y
 template <class Team>
 __device__ void vlin(Team &t, double a, const double *x, double b, double *y, long long n) {
-    for (long long i = t.rank(); i < n; i += t.size()) y[i] = a * x[i] + b * y[i];
+    double xx[4], yy[4];
+    RB_VLOOP4(t, n, { xx[u_] = x[q]; yy[u_] = y[q]; }, { y[q] = a * xx[u_] + b * yy[u_]; })
     t.sync();
 }
 
@@ -145,7 +173,7 @@ __device__ void lu_solve_rt(R *S, R *q, int n) {  // S is n×n, leading dimensio
 // ------------------------------------------------------------------------------------------
 // per-CTA shared state
 // ------------------------------------------------------------------------------------------
-struct GroupShared {
+struct alignas(16) GroupShared {
     double sigt[RB_MAXMAT];
     double sp[RB_MAXMAT];   // S⁺/ΔE
     double sm[RB_MAXMAT];   // S⁻/ΔE
@@ -154,10 +182,16 @@ struct GroupShared {
     double H[(RB_MAXRESTART + 1) * RB_MAXRESTART];
     double cs[RB_MAXRESTART], sn[RB_MAXRESTART], g[RB_MAXRESTART + 1], y[RB_MAXRESTART];
     double A[RB_MAXDEPTH * RB_MAXDEPTH], b[RB_MAXDEPTH];
-    // sweep scan: per thread-chunk affine map (A: NF×NF, b: NF) and the chunk's incoming flux
-    double chA[RB_THREADS][RB_SCAN_NF * RB_SCAN_NF];
-    double chb[RB_THREADS][RB_SCAN_NF];
-    double chF[RB_THREADS][RB_SCAN_NF];
+    union alignas(16) {
+        // sweep scan: per thread-chunk affine map (A: NF×NF, b: NF) and the chunk's incoming flux
+        struct {
+            double chA[RB_THREADS][RB_SCAN_NF * RB_SCAN_NF];
+            double chb[RB_THREADS][RB_SCAN_NF];
+            double chF[RB_THREADS][RB_SCAN_NF];
+        };
+        // M2D / D2M: a tile of columns of the moment or angular arrays
+        double tile[RB_TILE_DOUBLES];
+    };
     TeamShared team;
 };
 
@@ -500,6 +534,139 @@ __device__ void sweep1d(Team &t, const DevProblem &P, GroupShared &gs, const dou
 }
 
 // ------------------------------------------------------------------------------------------
+// moment <-> discrete products over column tiles. A column is one (is, c) pair; the moment array
+// 𝚽[p,col] and the angular array ψ[n,col] store a column contiguously, so a tile of TC columns
+// is one contiguous block, staged in shared memory with coalesced loads. The small operators
+// (Mn, Mn·ℳ, Dn) are read through the read-only cache. Tiles are dealt to the team's CTAs.
+// ------------------------------------------------------------------------------------------
+// Team-wide product over column tiles: acc[i,col] = Σ_k A[i + lda·k]·w(k,col)·X[k + ldx·col],
+// optionally with a second operator B applied to the unscaled X. Output tiles of TR rows × TC
+// columns are dealt to the team's CTAs; each thread owns a 4×4 block of a tile and the operand
+// panels are staged in shared memory 16 rows of k at a time.
+struct ProductArgs {
+    const double *A, *B;   // [ni + lda·k] operators (B may be null)
+    int lda, ni, nk;
+    const double *X;       // [k + ldx·col]
+    int ldx;
+    long long ncol;
+};
+
+template <class Team, class Scale, class Store>
+__device__ void team_product(Team &t, GroupShared &gs, const ProductArgs &a, Scale scale, Store store) {
+    constexpr int KC = 16;
+    const int ni4 = (a.ni + 3) & ~3;
+    const int TR = ni4 < 64 ? ni4 : 64;
+    int TC = 4096 / TR;
+    if (TC > 128) TC = 128;
+    const int nrb = (a.ni + TR - 1) / TR;
+    const long long ncb = (a.ncol + TC - 1) / TC;
+    const bool two = a.B != nullptr;
+    double *As = gs.tile, *Bs = As + KC * TR, *Xs = Bs + (two ? KC * TR : 0), *Zs = Xs + KC * TC;
+    const int ib = threadIdx.x % (TR / 4), cb = threadIdx.x / (TR / 4);
+    const bool owner = cb < TC / 4;
+    for (long long tl = t.crank; tl < (long long)nrb * ncb; tl += t.ncta) {
+        const int i0 = (int)(tl % nrb) * TR;
+        const long long c0 = (tl / nrb) * TC;
+        double acc[4][4], accb[4][4];
+#pragma unroll
+        for (int x = 0; x < 4; x++)
+#pragma unroll
+            for (int y = 0; y < 4; y++) { acc[x][y] = 0.0; accb[x][y] = 0.0; }
+        for (int k0 = 0; k0 < a.nk; k0 += KC) {
+            __syncthreads();
+            for (int e = threadIdx.x; e < KC * TR; e += blockDim.x) {
+                const int ii = e % TR, kk = e / TR, i = i0 + ii, k = k0 + kk;
+                const bool in = i < a.ni && k < a.nk;
+                As[e] = in ? a.A[i + (long long)a.lda * k] : 0.0;
+                if (two) Bs[e] = in ? a.B[i + (long long)a.lda * k] : 0.0;
+            }
+            for (int e = threadIdx.x; e < KC * TC; e += blockDim.x) {
+                const int kk = e % KC, cc = e / KC, k = k0 + kk;
+                const long long col = c0 + cc;
+                const bool in = k < a.nk && col < a.ncol;
+                const double v = in ? a.X[k + (long long)a.ldx * col] : 0.0;
+                Xs[kk * TC + cc] = in ? scale(k, col) * v : 0.0;
+                if (two) Zs[kk * TC + cc] = v;
+            }
+            __syncthreads();
+            if (owner) {
+#pragma unroll 4
+                for (int kk = 0; kk < KC; kk++) {
+                    const double2 a01 = *reinterpret_cast<const double2 *>(As + kk * TR + ib * 4);
+                    const double2 a23 = *reinterpret_cast<const double2 *>(As + kk * TR + ib * 4 + 2);
+                    const double2 x01 = *reinterpret_cast<const double2 *>(Xs + kk * TC + cb * 4);
+                    const double2 x23 = *reinterpret_cast<const double2 *>(Xs + kk * TC + cb * 4 + 2);
+                    const double o[4] = {a01.x, a01.y, a23.x, a23.y};
+                    const double v[4] = {x01.x, x01.y, x23.x, x23.y};
+#pragma unroll
+                    for (int x = 0; x < 4; x++)
+#pragma unroll
+                        for (int y = 0; y < 4; y++) acc[x][y] += o[x] * v[y];
+                    if (two) {
+                        const double2 b01 = *reinterpret_cast<const double2 *>(Bs + kk * TR + ib * 4);
+                        const double2 b23 = *reinterpret_cast<const double2 *>(Bs + kk * TR + ib * 4 + 2);
+                        const double2 z01 = *reinterpret_cast<const double2 *>(Zs + kk * TC + cb * 4);
+                        const double2 z23 = *reinterpret_cast<const double2 *>(Zs + kk * TC + cb * 4 + 2);
+                        const double ob[4] = {b01.x, b01.y, b23.x, b23.y};
+                        const double vz[4] = {z01.x, z01.y, z23.x, z23.y};
+#pragma unroll
+                        for (int x = 0; x < 4; x++)
+#pragma unroll
+                            for (int y = 0; y < 4; y++) accb[x][y] += ob[x] * vz[y];
+                    }
+                }
+            }
+        }
+        if (owner) {
+#pragma unroll
+            for (int y = 0; y < 4; y++) {
+                const long long col = c0 + cb * 4 + y;
+                if (col >= a.ncol) continue;
+#pragma unroll
+                for (int x = 0; x < 4; x++) {
+                    const int i = i0 + ib * 4 + x;
+                    if (i < a.ni) store(i, col, acc[x][y], accb[x][y]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// ψ[n,col] = add[n,col] + Σ_p Mn[n,p]·ys[mat,p]·𝚽[p,col] + T[mat]·Σ_p (Mn·ℳ)[n,p]·𝚽[p,col]
+// (scaled == 0: ψ = Mn·src, the Mn·Qlout product of the group set-up)
+template <class Team>
+__device__ void m2d_tiles(Team &t, const DevProblem &P, GroupShared &gs, const double *src, const double *add,
+                          int scaled) {
+    const int nd = P.nd, np = P.np, nm = P.nm5;
+    ProductArgs a{P.mn, (scaled && P.mnfp) ? P.mnfp : nullptr, nd, nd, np, src, np, (long long)nm * P.ncell};
+    const int *mat = P.mat;
+    const double *ys = P.kmat;
+    double *psi = P.psi;
+    team_product(
+        t, gs, a,
+        [=] __device__(int k, long long col) { return scaled ? ys[(long long)mat[col / nm] * np + k] : 1.0; },
+        [=, &gs] __device__(int i, long long col, double v, double vb) {
+            const long long o = col * nd + i;
+            const double tm = (scaled && P.mnfp) ? gs.tg[mat[col / nm]] : 0.0;
+            psi[o] = (add ? add[o] : 0.0) + v + tm * vb;
+        });
+}
+
+// zout[p,col] = Σ_n Dn[p,n]·ψ[n,col]   (matvec: zout = zin − that)
+template <class Team>
+__device__ void d2m_tiles(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, double *zout, int matvec) {
+    const int nd = P.nd, np = P.np, nm = P.nm5;
+    ProductArgs a{P.dn, nullptr, np, np, nd, P.psi, nd, (long long)nm * P.ncell};
+    team_product(
+        t, gs, a, [] __device__(int, long long) { return 1.0; },
+        [=] __device__(int i, long long col, double v, double) {
+            const long long o = col * np + i;
+            zout[o] = matvec ? zin[o] - v : v;
+        });
+}
+
+// ------------------------------------------------------------------------------------------
 // the pass T(z) = A·z + c (homogeneous: A·z), sn_inner_pass.jl:17-137, for 1D problems.
 // matvec != 0 writes zout = zin − A·zin instead (the Krylov operator of sn_one_speed.jl:147).
 // ------------------------------------------------------------------------------------------
@@ -509,33 +676,8 @@ __device__ void pass1d(Team &t, const DevProblem &P, GroupShared &gs, const doub
     const int nd = P.nd, np = P.np, nm = P.nm5;
     const long long ncell = P.ncell;
     const long long ncol = (long long)nm * ncell;  // (is, c) columns
-    // M2D: 4 directions per thread share the loads of 𝚽[:,r]
-    {
-        const int nb4 = (nd + 3) >> 2;
-        const long long nwork = (long long)nb4 * ncol;
-        for (long long o = t.rank(); o < nwork; o += t.size()) {
-            const int n0 = (int)(o % nb4) * 4;
-            const long long r = o / nb4;
-            const long long c = r / nm;
-            const int m = P.mat[c];
-            const double *ph = zin + r * np;
-            const double *K = P.kmat + ((long long)m * nd) * np;
-            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-            const int n1 = min(n0 + 1, nd - 1), n2 = min(n0 + 2, nd - 1), n3 = min(n0 + 3, nd - 1);
-            const double *K0 = K + (long long)n0 * np, *K1 = K + (long long)n1 * np;
-            const double *K2 = K + (long long)n2 * np, *K3 = K + (long long)n3 * np;
-            for (int p = 0; p < np; p++) {
-                const double v = ph[p];
-                s0 += K0[p] * v; s1 += K1[p] * v; s2 += K2[p] * v; s3 += K3[p] * v;
-            }
-            double *out = P.psi + r * nd;
-            const double *qo = P.qnout + r * nd;
-            out[n0] = (homog ? 0.0 : qo[n0]) + s0;
-            if (n0 + 1 < nd) out[n0 + 1] = (homog ? 0.0 : qo[n0 + 1]) + s1;
-            if (n0 + 2 < nd) out[n0 + 2] = (homog ? 0.0 : qo[n0 + 2]) + s2;
-            if (n0 + 3 < nd) out[n0 + 3] = (homog ? 0.0 : qo[n0 + 3]) + s3;
-        }
-    }
+    // M2D over column tiles staged in shared memory
+    m2d_tiles(t, P, gs, zin, homog ? nullptr : P.qnout, 1);
     t.sync();
     // sweep; homogeneous passes see no surface source and a zero incoming energy flux
     // (sn_inner_pass.jl:37-38)
@@ -544,35 +686,8 @@ __device__ void pass1d(Team &t, const DevProblem &P, GroupShared &gs, const doub
     const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
     sweep1d(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
     t.sync();
-    // D2M: 4 moments per thread share the loads of ψ[:,r]; direction order kept per output
-    {
-        const int nb4 = (np + 3) >> 2;
-        const long long nwork = (long long)nb4 * ncol;
-        for (long long o = t.rank(); o < nwork; o += t.size()) {
-            const int p0 = (int)(o % nb4) * 4;
-            const long long r = o / nb4;
-            const double *ps = P.psi + r * nd;
-            double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-            const int p1 = min(p0 + 1, np - 1), p2 = min(p0 + 2, np - 1), p3 = min(p0 + 3, np - 1);
-            for (int n = 0; n < nd; n++) {
-                const double v = ps[n];
-                const double *D = P.dn + (long long)np * n;
-                s0 += D[p0] * v; s1 += D[p1] * v; s2 += D[p2] * v; s3 += D[p3] * v;
-            }
-            const long long b = r * np;
-            if (matvec) {
-                zout[b + p0] = zin[b + p0] - s0;
-                if (p0 + 1 < np) zout[b + p0 + 1] = zin[b + p0 + 1] - s1;
-                if (p0 + 2 < np) zout[b + p0 + 2] = zin[b + p0 + 2] - s2;
-                if (p0 + 3 < np) zout[b + p0 + 3] = zin[b + p0 + 3] - s3;
-            } else {
-                zout[b + p0] = s0;
-                if (p0 + 1 < np) zout[b + p0 + 1] = s1;
-                if (p0 + 2 < np) zout[b + p0 + 2] = s2;
-                if (p0 + 3 < np) zout[b + p0 + 3] = s3;
-            }
-        }
-    }
+    // D2M over column tiles staged in shared memory; direction order kept per output
+    d2m_tiles(t, P, gs, zin, zout, matvec);
     // outgoing boundary moments: side 1 (X+) collects μ ≥ 0, side 0 (X-) μ < 0
     const int nf = P.nmf[0], nps = P.npsurf;
     const long long nb = P.nb[0];

@@ -230,10 +230,13 @@ struct Solver {
                     const double *Vi = vec(4 + i);
                     const double *Vn = (i < j) ? vec(4 + i + 1) : nullptr;
                     double acc[1] = {0.0};
-                    for (long long q = t.rank(); q < N; q += t.size()) {
-                        const double wq = w[q] + (-h) * Vi[q];
-                        w[q] = wq;
-                        acc[0] += wq * (Vn ? Vn[q] : wq);
+                    double xw[4], xv[4], xn[4];
+                    if (Vn) {
+                        RB_VLOOP4(t, N, { xw[u_] = w[q]; xv[u_] = Vi[q]; xn[u_] = Vn[q]; },
+                                  { const double wq = xw[u_] + (-h) * xv[u_]; w[q] = wq; acc[0] += wq * xn[u_]; })
+                    } else {
+                        RB_VLOOP4(t, N, { xw[u_] = w[q]; xv[u_] = Vi[q]; },
+                                  { const double wq = xw[u_] + (-h) * xv[u_]; w[q] = wq; acc[0] += wq * wq; })
                     }
                     t.template sumk<1>(acc);
                     h = acc[0];
@@ -274,10 +277,13 @@ struct Solver {
             }
             __syncthreads();
             // z += Σ y_i V_i, in basis order per element
-            for (long long q = t.rank(); q < N; q += t.size()) {
-                double zq = z[q];
-                for (int i = 0; i < k; i++) zq += gs.y[i] * vec(4 + i)[q];
-                z[q] = zq;
+            {
+                double xz[4];
+                RB_VLOOP4(t, N, { xz[u_] = z[q]; }, {
+                    double zq = xz[u_];
+                    for (int i = 0; i < k; i++) zq += gs.y[i] * vec(4 + i)[q];
+                    z[q] = zq;
+                })
             }
             t.sync();
             if (conv) break;
@@ -434,19 +440,13 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs) {
                 P.scsd[o] = v;
             }
         }
-        // K[m][n][p] = Mn[n,p]·Σs_in[m,pl[p]] + T[m]·(Mn·ℳ)[n,p]
+        // ys[m][p] = Σs_in[m, pl[p]]: the in-group scattering source of moment p (zero for the
+        // solvers without it, sn_inner_pass.jl:21); T[m] scales the Fokker-Planck product
         const bool scat = (st_ != 4 && st_ != 5 && st_ != 6);
-        for (long long o = t.rank(); o < (long long)nmat * nd * np; o += t.size()) {
+        for (long long o = t.rank(); o < (long long)nmat * np; o += t.size()) {
             const int p = (int)(o % np);
-            const int n = (int)((o / np) % nd);
-            const int m = (int)(o / ((long long)np * nd));
-            double v = 0.0;
-            if (scat) {
-                const double sv = P.sigma_s[m + (long long)nmat * (ig + (long long)ng * (ig + (long long)ng * P.pl[p]))];
-                v = P.mn[n + (long long)nd * p] * sv;
-            }
-            if (P.mnfp) v += gs.tg[m] * P.mnfp[n + (long long)nd * p];
-            P.kmat[o] = v;
+            const int m = (int)(o / np);
+            P.kmat[o] = scat ? P.sigma_s[m + (long long)nmat * (ig + (long long)ng * (ig + (long long)ng * P.pl[p]))] : 0.0;
         }
         // Qlout = Σ_{gi≠ig} Σs[mat,gi,ig,l]·𝚽[gi] + volume source (scattering_source.jl:59-68;
         // groups above ig are still zero in the single outer iteration, sn_flux.jl:150,157)
@@ -467,16 +467,10 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs) {
             for (long long i = t.rank(); i < nE; i += t.size()) phiE_in[i] = phiE_in[i] * r1 / r0;
         }
         t.sync();
-        // Mn·Qlout
-        const long long nq = (long long)nd * nm * ncell;
-        for (long long o = t.rank(); o < nq; o += t.size()) {
-            const int n = (int)(o % nd);
-            const long long r = o / nd;
-            double s = 0.0;
-            for (int p = 0; p < np; p++) s += P.mn[n + (long long)nd * p] * P.qlout[p + (long long)np * r];
-            P.qnout[o] = s;
-        }
+        // Mn·Qlout into ψ, then kept as Qnout for the passes of this group
+        m2d_tiles(t, P, gs, P.qlout, nullptr, 0);
         t.sync();
+        vcopy(t, P.qnout, P.psi, (long long)nd * nm * ncell);
         Solver<Team> S{t, P, gs, ig, phiE_in, phiE_out, 0};
         SolveStat s = S.one_speed(P.flux + (long long)ig * nphi);
         npass += S.npass;
@@ -507,7 +501,7 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs) {
 // ------------------------------------------------------------------------------------------
 // persistent batch kernel: clusters pull problems from a device work queue
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(RB_THREADS) solve_batch_kernel(DevProblem *const *probs, int nprob,
+__global__ void __launch_bounds__(RB_THREADS, 2) solve_batch_kernel(DevProblem *const *probs, int nprob,
                                                                  int *queue) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
