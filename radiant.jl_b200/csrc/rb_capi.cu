@@ -42,6 +42,8 @@ struct rb_context {
     int device = 0;
     int nsm = 0;
     int cluster = 0;  // CTAs per problem team (0 = sized per batch); RB_CLUSTER_SIZE overrides
+    int md_cluster = 0;  // 2D/3D problems on cluster teams instead of the whole GPU (RB_MD_TEAM=cluster)
+    double *d_gpart = nullptr;  // grid-team reduction partials
     uint64_t budget = 0;
     uint64_t used = 0;
     cudaStream_t stream = nullptr;
@@ -168,7 +170,7 @@ int nvec_for(const rb_sn_problem *P) {
 struct Derived {
     Moments M;
     int ns[3];
-    long long ncell, nphi, nstate, off_b[3], nb[3];
+    long long ncell, nphi, nstate, off_b[3], nb[3], fcells[3];
     int csd;
     std::vector<int> mat0;
     std::vector<double> cosv, mnfp, frow_m, frow_d, G, Gsrc, Gout, Kcsd, Bcsd, EsA, EsB, Eout, vol;
@@ -180,8 +182,6 @@ struct Derived {
 int validate_and_derive(rb_context *ctx, const rb_sn_problem *P, Derived &D) {
     if (!P) return fail(ctx, RB_ERR_INVALID, "null problem");
     if (P->ndims < 1 || P->ndims > 3) return fail(ctx, RB_ERR_INVALID, "ndims must be 1, 2 or 3 (got %d)", P->ndims);
-    if (P->ndims != 1)
-        return fail(ctx, RB_ERR_UNSUPPORTED, "ndims=%d: only the 1D sweep is built in this library version", P->ndims);
     if (P->is_adaptive) return fail(ctx, RB_ERR_UNSUPPORTED, "adaptive (AWD) closures are not built");
     if (P->is_em) return fail(ctx, RB_ERR_UNSUPPORTED, "external electromagnetic fields are not built");
     if (P->solver_type < 1 || P->solver_type > 6) return fail(ctx, RB_ERR_INVALID, "solver_type %d", P->solver_type);
@@ -232,6 +232,20 @@ int validate_and_derive(rb_context *ctx, const rb_sn_problem *P, Derived &D) {
     }
     for (long long c = 0; c < D.ns[0]; c++)
         if (!(P->dx[c] > 0)) return fail(ctx, RB_ERR_INVALID, "dx[%lld] must be > 0", c);
+    if (P->ndims >= 2) {
+        if (!P->dy || !P->eta) return fail(ctx, RB_ERR_INVALID, "2D problem without dy / eta");
+        for (long long c = 0; c < D.ns[1]; c++)
+            if (!(P->dy[c] > 0)) return fail(ctx, RB_ERR_INVALID, "dy[%lld] must be > 0", c);
+        if ((long long)D.ns[0] * P->nm[1] > RB_TILE_DOUBLES)
+            return fail(ctx, RB_ERR_UNSUPPORTED, "nx x face moments = %lld exceeds the wavefront's shared slots (%d)",
+                        (long long)D.ns[0] * P->nm[1], RB_TILE_DOUBLES);
+    }
+    if (P->ndims == 3) {
+        if (!P->dz || !P->xi) return fail(ctx, RB_ERR_INVALID, "3D problem without dz / xi");
+        for (long long c = 0; c < D.ns[2]; c++)
+            if (!(P->dz[c] > 0)) return fail(ctx, RB_ERR_INVALID, "dz[%lld] must be > 0", c);
+    }
+    for (int d = 0; d < 3; d++) D.fcells[d] = d < P->ndims ? face_cells(P->ndims, D.ns, d) : 0;
     // directions
     D.cosv.assign(3 * (size_t)nd, 0.0);
     for (int n = 0; n < nd; n++) {
@@ -390,7 +404,12 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     offs[k++] = L.take<double>(nq);                       // 36 psi
     offs[k++] = L.take<double>((size_t)nmat * np);        // 37 kmat (in-group Σs per material and moment)
     offs[k++] = L.take<double>((size_t)nmat * nm5 * nm5); // 38 scsd
-    offs[k++] = L.take<double>((size_t)nd * RB_MAXFACE);  // 39 fexit
+    {
+        const long long md = (long long)nd * ((long long)D.ns[1] * D.ns[2] + (long long)D.ns[0] * D.ns[2] +
+                                              2LL * D.ns[0] * D.ns[1]) * D.nfmax;
+        const long long one = (long long)nd * RB_MAXFACE;
+        offs[k++] = L.take<double>(P->ndims == 1 ? one : md);  // 39 fexit / multi-D face scratch
+    }
     offs[k++] = L.take<double>(D.csd ? nE : 0);           // 40 phiE_a
     offs[k++] = L.take<double>(D.csd ? nE : 0);           // 41 phiE_b
     offs[k++] = L.take<double>(D.csd ? D.nphi : 0);       // 42 cutoff
@@ -398,6 +417,8 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     offs[k++] = L.take<int>(2 * (size_t)ng);              // 44 iters, conv
     offs[k++] = L.take<long long>(1);                     // 45 passes
     offs[k++] = L.take<int>(1);                           // 46 status
+    offs[k++] = L.take<double>(D.ns[1]);                  // 47 dy
+    offs[k++] = L.take<double>(D.ns[2]);                  // 48 dz
     return k;
 }
 
@@ -430,6 +451,21 @@ int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm,
     return RB_OK;
 }
 
+// One 2D/3D problem on every SM: a cooperative launch of two CTAs per SM (the team is the grid).
+int launch_grid(rb_context *ctx, DevProblem *prob, cudaStream_t s) {
+    const size_t smem = sizeof(rb::GroupShared);
+    CK(cudaFuncSetAttribute(rb::solve_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb::solve_grid_kernel, RB_THREADS, smem));
+    if (per_sm < 1) return fail(ctx, RB_ERR_CUDA, "the grid solve kernel does not fit on an SM");
+    if (per_sm > 2) per_sm = 2;
+    const int grid = ctx->nsm * per_sm;
+    if (!ctx->d_gpart) CK(cudaMalloc(&ctx->d_gpart, sizeof(double) * 2 * 4 * 4096));
+    void *args[] = {(void *)&prob, (void *)&ctx->d_gpart};
+    CK(cudaLaunchCooperativeKernel((void *)rb::solve_grid_kernel, dim3(grid), dim3(RB_THREADS), args, smem, s));
+    return RB_OK;
+}
+
 int ensure_launch_scratch(rb_context *ctx, int n) {
     if (n > ctx->list_cap) {
         if (ctx->d_list) cudaFree(ctx->d_list);
@@ -451,13 +487,29 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
     CK(cudaMemcpyAsync(ctx->d_list, ptrs.data(), sizeof(DevProblem *) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), s));
     for (auto *r : recs) CK(cudaMemsetAsync(r->h.status, 0, sizeof(int), s));
-    int cluster = ctx->cluster;
-    if (cluster <= 0) {  // one cluster per problem, sized to the problem's directions
-        const DevProblem &h0 = recs[0]->h;
-        cluster = h0.nd >= 32 ? 8 : (h0.nd >= 16 ? 4 : (h0.nd >= 8 ? 2 : 1));
+    // 1D problems (and 2D/3D ones when RB_MD_TEAM=cluster) share one persistent cluster launch;
+    // 2D/3D problems otherwise get the whole GPU each, one cooperative launch after another
+    std::vector<DevProblem *> small;
+    std::vector<ProblemRec *> large;
+    for (auto *r : recs) {
+        if (r->h.ndims == 1 || ctx->md_cluster) small.push_back(r->d);
+        else large.push_back(r);
     }
-    int st2 = launch_solve(ctx, ctx->d_list, n, ctx->d_queue, ctx->nsm, cluster, s);
-    if (st2) return st2;
+    if (!small.empty()) {
+        if ((int)small.size() != n)
+            CK(cudaMemcpyAsync(ctx->d_list, small.data(), sizeof(DevProblem *) * small.size(), cudaMemcpyHostToDevice, s));
+        int cluster = ctx->cluster;
+        if (cluster <= 0) {  // one cluster per problem, sized to the problem's directions
+            const DevProblem &h0 = recs[0]->h;
+            cluster = h0.nd >= 32 ? 4 : (h0.nd >= 16 ? 4 : (h0.nd >= 8 ? 2 : 1));
+        }
+        int st2 = launch_solve(ctx, ctx->d_list, (int)small.size(), ctx->d_queue, ctx->nsm, cluster, s);
+        if (st2) return st2;
+    }
+    for (auto *r : large) {
+        int st3 = launch_grid(ctx, r->d, s);
+        if (st3) return st3;
+    }
     for (auto *r : recs) { r->stream = s; r->solved = true; }
     return RB_OK;
 }
@@ -503,9 +555,13 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     h.cutoff = D.csd ? DP(double, 42) : nullptr;
     h.rho = DP(double, 43); h.resid = h.rho + ng; h.iters = DP(int, 44); h.conv = h.iters + ng;
     h.passes = DP(long long, 45); h.status = DP(int, 46);
+    h.dy = P->ndims >= 2 ? DP(double, 47) : nullptr; h.dz = P->ndims >= 3 ? DP(double, 48) : nullptr;
+    for (int d = 0; d < 3; d++) h.fcells[d] = D.fcells[d];
     int r = RB_OK;
 #define PUT(T, k, src, n) if ((r = put<T>(ctx, b, o[k], src, n, s)) != RB_OK) return r;
     PUT(double, 1, P->dx, D.ns[0]);
+    if (P->ndims >= 2) PUT(double, 47, P->dy, D.ns[1]);
+    if (P->ndims >= 3) PUT(double, 48, P->dz, D.ns[2]);
     PUT(int, 2, D.mat0.data(), D.mat0.size());
     PUT(double, 3, D.cosv.data(), D.cosv.size());
     PUT(double, 4, P->mn, (size_t)nd * np);
@@ -571,6 +627,7 @@ int32_t rb_create(int32_t device, uint64_t hbm_budget_bytes, rb_context **out) {
     cudaMemGetInfo(&fr, &tot);
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)(fr * 0.9);
     if (const char *cs = getenv("RB_CLUSTER_SIZE")) c->cluster = atoi(cs);
+    if (const char *mt = getenv("RB_MD_TEAM")) c->md_cluster = strcmp(mt, "cluster") == 0;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete c; return fail(nullptr, RB_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
     *out = c;
@@ -586,6 +643,7 @@ int32_t rb_destroy(rb_context *ctx) {
     if (ctx->d_list) cudaFree(ctx->d_list);
     if (ctx->d_queue) cudaFree(ctx->d_queue);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
+    if (ctx->d_gpart) cudaFree(ctx->d_gpart);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return RB_OK;

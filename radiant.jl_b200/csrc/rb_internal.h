@@ -26,6 +26,7 @@ struct DevProblem {
     double tol;
     int np_source;
     long long nphi, nstate, off_b[3], nb[3];
+    long long fcells[3];  // boundary face cells per axis
     int nvec;          // Krylov vectors allocated in `vecs`
     // ---- tables (device pointers) --------------------------------------------------------
     const double *dx, *dy, *dz;
@@ -65,7 +66,7 @@ struct DevProblem {
     float *psi32;      // [nd*nm5*ncell] mixed form: FP32 angular source / flux
     double *kmat;      // [nmat][np] per-group in-group Σs of each moment's Legendre order
     double *scsd;      // [nmat][nm5*nm5] per-group CSD part of the cell matrix
-    double *fexit;     // [nd][RB_MAXFACE] 1D exit faces
+    double *fexit;     // 1D: [nd][RB_MAXFACE] exit faces; 2D/3D: per-direction exits and z-face plane
     double *phiE_a, *phiE_b; // [nd*nm4*ncell] energy-face fluxes (in / out, swapped per group)
     double *cutoff;    // [nphi]
     // ---- results ------------------------------------------------------------------------

@@ -11,6 +11,7 @@
 #include <math_constants.h>
 
 #include "rb_kernels.cuh"
+#include "rb_sweep_md.cuh"
 
 namespace rb {
 
@@ -39,15 +40,14 @@ struct Solver {
     __device__ double *vec(int k) const { return P.vecs + (long long)k * P.nstate; }
 
     // load_and_pass! (sn_one_speed.jl:138-143): out <- T(zin)
-    __device__ void fixedpoint(double *out, const double *zin) {
-        pass1d(t, P, gs, zin, out, 0, 0, ig, phiE_in, phiE_out);
+    __device__ void pass(const double *zin, double *out, int homog, int mv) {
+        if (P.ndims == 1) pass1d(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out);
+        else pass_md(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out);
         npass++;
     }
+    __device__ void fixedpoint(double *out, const double *zin) { pass(zin, out, 0, 0); }
     // matvec! (sn_one_speed.jl:147): out <- zin − A·zin
-    __device__ void matvec(double *out, const double *zin) {
-        pass1d(t, P, gs, zin, out, 1, 1, ig, phiE_in, phiE_out);
-        npass++;
-    }
+    __device__ void matvec(double *out, const double *zin) { pass(zin, out, 1, 1); }
     __device__ double norm(const double *a) { return sqrt(vdot(t, a, a, P.nstate)); }
 
     // ---------------------------------------------------------------- livolant (and "none")
@@ -369,7 +369,7 @@ struct Solver {
         for (int f = 0; f < 2 * P.ndims; f++) {
             const double *src = P.surf[f];
             if (!src) continue;
-            for (long long k = t.rank(); k < (long long)P.np_source; k += t.size())
+            for (long long k = t.rank(); k < (long long)P.np_source * P.fcells[f / 2]; k += t.size())
                 if (src[ig + (long long)P.ng * k] != 0.0) any = 1;
         }
         for (long long i = t.rank(); i < nphi; i += t.size()) if (P.qlout[i] != 0.0) any = 1;
@@ -514,6 +514,15 @@ __global__ void __launch_bounds__(RB_THREADS, 2) solve_batch_kernel(DevProblem *
         if (idx >= nprob) break;
         solve_problem(t, *probs[idx], gs);
     }
+}
+
+// one large (2D/3D) problem on the whole GPU: a cooperative launch, one team of every CTA
+__global__ void __launch_bounds__(RB_THREADS, 2) solve_grid_kernel(DevProblem *prob, double *gpart) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
+    GridTeam t;
+    t.init(&gs.team, gpart);
+    solve_problem(t, *prob, gs);
 }
 
 // [ng][nphi] (group-major) -> [ng, nphi] (group fastest, the reference's layout)

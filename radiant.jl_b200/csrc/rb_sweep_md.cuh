@@ -1,0 +1,244 @@
+// rb_sweep_md.cuh -- the 2D and 3D sweeps (sn_sweep_2D.jl:54-183, sn_sweep_3D.jl:57-239) and
+// their cell closures (flux_2D/3D_BTE/BFP, sn_2D_bte.jl:35-116, sn_2D_bfp.jl:45-154,
+// sn_3D_bte.jl:42-152, sn_3D_bfp.jl:52-191).
+//
+// Ordering: a cell needs the outgoing faces of its upwind x, y (and z) neighbours. Planes are
+// taken in z sweep order; inside a plane the rows form a skewed pipeline (KBA wavefront on
+// ix + iy): at step s, the thread of row r solves column s − r, so its upwind x face is the one it
+// produced at step s − 1 (kept in registers) and its upwind y face is the one row r − 1 produced
+// at step s − 1 (handed over through shared memory, one slot per column). The z face comes from
+// the previous plane (a per-direction scratch plane in global memory). Several directions share
+// a CTA when the rows are fewer than its threads; directions are dealt to the team's CTAs.
+// Results equal the reference's lexicographic order exactly in exact arithmetic, because every
+// cell still sees the same upwind faces.
+#pragma once
+#include "rb_kernels.cuh"
+
+namespace rb {
+
+// Incoming face flux of direction n through the boundary face `face` at face cell `fcell`:
+// surface source into moment 1 plus the lagged reflective / periodic in-moments of that face
+// (sn_sweep_2D.jl:71-99, sn_sweep_3D.jl:80-163).
+__device__ __forceinline__ void boundary_in_md(const DevProblem &P, int n, int axis, bool fwd, long long fcell,
+                                               const double *zin, int np_source, int ig, double *f0, int nf) {
+    const int face = 2 * axis + (fwd ? 0 : 1), side = fwd ? 0 : 1;
+    const double *mrow = P.frow_m + ((long long)axis * P.nd + n) * P.npsurf;
+    for (int f = 0; f < nf; f++) f0[f] = 0.0;
+    const double *src = P.surf[face];
+    if (src)
+        for (int p = 0; p < np_source; p++)
+            f0[0] += mrow[p] * src[ig + (long long)P.ng * (p + (long long)P.np_source * fcell)];
+    const int bcv = P.bc[face];
+    if (bcv != 0) {
+        const int rside = (bcv == 1) ? side : 1 - side;
+        const double *b = zin + P.off_b[axis];
+        for (int p = 0; p < P.npsurf; p++)
+            for (int is = 0; is < nf; is++)
+                f0[is] += mrow[p] * b[p + (long long)P.npsurf * (is + (long long)nf * (rside + 2 * fcell))];
+    }
+}
+
+// The closure of one cell with the run-time shapes of the problem (nm ≤ RB_MAXNM). F[a] holds the
+// incoming face moments of axis a and receives the outgoing ones; FE likewise for the energy face.
+struct CellMDrt {
+    __device__ static void step(const DevProblem &P, const GroupShared &gs, int n, int nax, const double *h,
+                                const bool *tang_unused, int m, double *Qn, double (*F)[RB_MAXFACE], double *FE) {
+        const int nm = P.nm5;
+        double S[RB_MAXNM * RB_MAXNM], q[RB_MAXNM];
+#pragma unroll 1
+        for (int e = 0; e < nm * nm; e++) S[e] = P.csd ? P.scsd[(long long)m * nm * nm + e] : 0.0;
+#pragma unroll 1
+        for (int i = 0; i < nm; i++) { S[i + nm * i] += gs.sigt[m]; q[i] = Qn[i]; }
+#pragma unroll 1
+        for (int a = 0; a < nax; a++) {
+            const long long blk = (long long)n * 3 + a;
+            const double *Gr = P.G + blk * nm * nm, *Gs = P.Gsrc + blk * nm * P.nfmax;
+            const int nf = P.nmf[a];
+#pragma unroll 1
+            for (int e = 0; e < nm * nm; e++) S[e] += h[a] * Gr[e];
+#pragma unroll 1
+            for (int j = 0; j < nm; j++) {
+                double s = 0.0;
+#pragma unroll 1
+                for (int f = 0; f < nf; f++) s += Gs[j + nm * f] * F[a][f];
+                q[j] += h[a] * s;
+            }
+        }
+        if (P.csd) {
+            const int ne = P.nm4;
+#pragma unroll 1
+            for (int j = 0; j < nm; j++) {
+                double s = 0.0;
+#pragma unroll 1
+                for (int e = 0; e < ne; e++) s += (P.EsA[j + nm * e] * gs.sp[m] - P.EsB[j + nm * e] * gs.sm[m]) * FE[e];
+                q[j] -= s;
+            }
+        }
+        lu_solve_rt<double>(S, q, nm);
+#pragma unroll 1
+        for (int a = 0; a < nax; a++) {
+            const long long blk = (long long)n * 3 + a;
+            const double *Go = P.Gout + blk * nm * P.nfmax;
+            const int nf = P.nmf[a];
+            double Fo[RB_MAXFACE];
+#pragma unroll 1
+            for (int f = 0; f < nf; f++) {
+                double s = P.w1[a] * F[a][f];
+#pragma unroll 1
+                for (int j = 0; j < nm; j++) s += Go[f + nf * j] * q[j];
+                Fo[f] = s;
+            }
+#pragma unroll 1
+            for (int f = 0; f < nf; f++) F[a][f] = Fo[f];
+        }
+        if (P.csd) {
+            const int ne = P.nm4;
+            double Eo[RB_MAXFACE];
+#pragma unroll 1
+            for (int e = 0; e < ne; e++) {
+                double s = P.w1[3] * FE[e];
+#pragma unroll 1
+                for (int j = 0; j < nm; j++) s += P.Eout[e + ne * j] * q[j];
+                Eo[e] = s;
+            }
+#pragma unroll 1
+            for (int e = 0; e < ne; e++) FE[e] = Eo[e];
+        }
+#pragma unroll 1
+        for (int j = 0; j < nm; j++) Qn[j] = q[j];
+    }
+};
+
+// Scratch layout per direction (global): x exits [ny·nz], y exits [nx·nz], z exits [nx·ny],
+// z faces of the previous plane [nx·ny], each × nfmax doubles.
+__device__ __forceinline__ long long md_scratch_stride(const DevProblem &P) {
+    return ((long long)P.ny * P.nz + (long long)P.nx * P.nz + 2LL * P.nx * P.ny) * P.nfmax;
+}
+
+template <class Team>
+__device__ void sweep_md(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, int np_source,
+                         const double *phiE_in, double *phiE_out, int ig) {
+    const int nd = P.nd, nx = P.nx, ny = P.ny, nz = P.nz, nm = P.nm5, nax = P.ndims, nfm = P.nfmax;
+    const int ncta = (int)t.ncta, crank = (int)t.crank;
+    const int my_dirs = (nd - crank + ncta - 1) / ncta;
+    const int R = ny < (int)blockDim.x ? ny : (int)blockDim.x;   // rows per direction
+    int D = (int)blockDim.x / R;                                  // directions per round,
+    const int dmax = RB_TILE_DOUBLES / (nx * P.nmf[1]);           // bounded by the y-face slots
+    if (D > dmax) D = dmax;
+    const int nrb = (ny + R - 1) / R;
+    const long long sstride = md_scratch_stride(P);
+    double *yface = gs.tile;  // [D][nx][nf_y]
+    const int nfy = P.nmf[1];
+    for (int k0 = 0; k0 < my_dirs; k0 += D) {
+        const int dl = threadIdx.x / R, r = threadIdx.x % R;
+        const bool active = dl < D && k0 + dl < my_dirs;
+        const int n = crank + (k0 + dl) * ncta;
+        const double mu = active ? P.cosv[n] : 0.0, eta = active ? P.cosv[nd + n] : 0.0;
+        const double xi = (active && nax == 3) ? P.cosv[2 * nd + n] : 0.0;
+        const bool fx = mu >= 0.0, fy = eta >= 0.0, fz = xi >= 0.0;
+        double *scr = P.fexit + (active ? (long long)n * sstride : 0);
+        double *exx = scr, *exy = exx + (long long)ny * nz * nfm, *exz = exy + (long long)nx * nz * nfm;
+        double *zfc = exz + (long long)nx * ny * nfm;
+        double *yf = yface + (long long)dl * nx * nfy;
+        for (int izz = 0; izz < nz; izz++) {
+            const int iz = fz ? izz : nz - 1 - izz;
+            for (int rb = 0; rb < nrb; rb++) {
+                const int iyy = rb * R + r;
+                const bool row = active && iyy < ny;
+                const int iy = fy ? iyy : ny - 1 - iyy;
+                double F[3][RB_MAXFACE], FE[RB_MAXFACE], Qn[RB_MAXNM];
+                for (int s = 0; s < nx + R - 1; s++) {
+                    const int ixx = s - r;
+                    if (row && ixx >= 0 && ixx < nx) {
+                        const int ix = fx ? ixx : nx - 1 - ixx;
+                        const long long c = ix + (long long)nx * (iy + (long long)ny * iz);
+                        if (ixx == 0)  // X face of the row (sn_sweep_2D.jl:103-132)
+                            boundary_in_md(P, n, 0, fx, iy + (long long)ny * iz, zin, np_source, ig, F[0], P.nmf[0]);
+                        if (iyy == 0)  // Y face of the column (sn_sweep_2D.jl:71-99)
+                            boundary_in_md(P, n, 1, fy, ix + (long long)nx * iz, zin, np_source, ig, F[1], nfy);
+                        else
+                            for (int f = 0; f < nfy; f++) F[1][f] = yf[(long long)ixx * nfy + f];
+                        if (nax == 3) {
+                            if (izz == 0)  // Z face (sn_sweep_3D.jl:80-108)
+                                boundary_in_md(P, n, 2, fz, ix + (long long)nx * iy, zin, np_source, ig, F[2], P.nmf[2]);
+                            else
+                                for (int f = 0; f < P.nmf[2]; f++) F[2][f] = zfc[(ix + (long long)nx * iy) * nfm + f];
+                        }
+                        const int m = P.mat[c];
+                        double h[3];
+                        h[0] = fabs(mu) / P.dx[ix];
+                        h[1] = fabs(eta) / P.dy[iy];
+                        h[2] = nax == 3 ? fabs(xi) / P.dz[iz] : 0.0;
+                        double *pc = P.psi + n + (long long)nd * nm * c;
+                        for (int j = 0; j < nm; j++) Qn[j] = pc[(long long)nd * j];
+                        if (P.csd)
+                            for (int e = 0; e < P.nm4; e++)
+                                FE[e] = phiE_in ? phiE_in[n + (long long)nd * (e + (long long)P.nm4 * c)] : 0.0;
+                        CellMDrt::step(P, gs, n, nax, h, nullptr, m, Qn, F, FE);
+                        for (int j = 0; j < nm; j++) pc[(long long)nd * j] = Qn[j];
+                        if (P.csd)
+                            for (int e = 0; e < P.nm4; e++) phiE_out[n + (long long)nd * (e + (long long)P.nm4 * c)] = FE[e];
+                        for (int f = 0; f < nfy; f++) yf[(long long)ixx * nfy + f] = F[1][f];
+                        if (nax == 3) {
+                            if (izz < nz - 1)
+                                for (int f = 0; f < P.nmf[2]; f++) zfc[(ix + (long long)nx * iy) * nfm + f] = F[2][f];
+                            else
+                                for (int f = 0; f < P.nmf[2]; f++) exz[(ix + (long long)nx * iy) * nfm + f] = F[2][f];
+                        }
+                        if (ixx == nx - 1)
+                            for (int f = 0; f < P.nmf[0]; f++) exx[(iy + (long long)ny * iz) * nfm + f] = F[0][f];
+                        if (iyy == ny - 1)
+                            for (int f = 0; f < nfy; f++) exy[(ix + (long long)nx * iz) * nfm + f] = F[1][f];
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+    }
+}
+
+// Outgoing boundary moments of every face: b[p,is,side,cell] = Σ_n Dn_face[n][p]·exit[n][cell][is]
+// over the directions leaving through that side (sn_sweep_2D.jl:146-179, accumulated over n in
+// order as sn_inner_pass.jl:127-129 does).
+template <class Team>
+__device__ void boundary_out_md(Team &t, const DevProblem &P, const double *zin, double *zout, int matvec) {
+    const int nd = P.nd, nps = P.npsurf, nfm = P.nfmax;
+    const long long sstride = md_scratch_stride(P);
+    for (int a = 0; a < P.ndims; a++) {
+        const int nf = P.nmf[a];
+        const long long ncell = P.nb[a] / ((long long)nps * nf * 2);
+        const long long off = a == 0 ? 0 : (a == 1 ? (long long)P.ny * P.nz * nfm : ((long long)P.ny * P.nz + (long long)P.nx * P.nz) * nfm);
+        for (long long o = t.rank(); o < P.nb[a]; o += t.size()) {
+            const int p = (int)(o % nps);
+            const int is = (int)((o / nps) % nf);
+            const int side = (int)((o / ((long long)nps * nf)) % 2);
+            const long long cell = o / ((long long)nps * nf * 2);
+            double s = 0.0;
+            for (int n = 0; n < nd; n++) {
+                const bool fwd = P.cosv[(long long)a * nd + n] >= 0.0;
+                if ((side == 1) == fwd)
+                    s += P.frow_d[((long long)a * nd + n) * nps + p] * P.fexit[(long long)n * sstride + off + cell * nfm + is];
+            }
+            const long long k = P.off_b[a] + o;
+            zout[k] = matvec ? zin[k] - s : s;
+        }
+        (void)ncell;
+    }
+}
+
+// the pass for 2D and 3D problems
+template <class Team>
+__device__ void pass_md(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, double *zout, int homog,
+                        int matvec, int ig, const double *phiE_in, double *phiE_out) {
+    m2d_tiles(t, P, gs, zin, homog ? nullptr : P.qnout, 1);
+    t.sync();
+    const int np_source = homog ? 0 : P.np_source;
+    const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
+    sweep_md(t, P, gs, zin, np_source, pE, phiE_out, ig);
+    t.sync();
+    d2m_tiles(t, P, gs, zin, zout, matvec);
+    boundary_out_md(t, P, zin, zout, matvec);
+    t.sync();
+}
+
+}  // namespace rb

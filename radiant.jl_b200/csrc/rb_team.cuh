@@ -87,4 +87,69 @@ struct ClusterTeam {
     }
 };
 
+
+// A team of every CTA of a cooperative launch (one problem on the whole GPU, for 2D and 3D
+// solves). Barriers are grid barriers; a reduction writes one partial per CTA into a
+// double-buffered global slot, and after the barrier every CTA adds all partials in CTA order,
+// so every thread of the grid sees the same bits.
+struct GridTeam {
+    TeamShared *sh;
+    double *gpart;    // [2][ncta][4] partial sums
+    unsigned crank;
+    unsigned ncta;
+    int phase;
+
+    __device__ void init(TeamShared *s, double *gp) {
+        sh = s;
+        gpart = gp;
+        crank = blockIdx.x;
+        ncta = gridDim.x;
+        phase = 0;
+    }
+    __device__ __forceinline__ int rank() const { return (int)(crank * blockDim.x + threadIdx.x); }
+    __device__ __forceinline__ int size() const { return (int)(ncta * blockDim.x); }
+    __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
+    __device__ __forceinline__ void sync() const { cg::this_grid().sync(); }
+
+    template <int K>
+    __device__ void sumk(double (&v)[K]) {
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+        const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int k = 0; k < K; k++) sh->warp[w][k] = v[k];
+        __syncthreads();
+        const int slot = phase & 1;
+        phase++;
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                double s = 0.0;
+                for (int i = 0; i < nw; i++) s += sh->warp[i][k];
+                gpart[((long long)slot * ncta + crank) * 4 + k] = s;
+            }
+        }
+        cg::this_grid().sync();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                double s = 0.0;
+                for (unsigned r = 0; r < ncta; r++) s += gpart[((long long)slot * ncta + r) * 4 + k];
+                sh->part[slot][k] = s;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < K; k++) v[k] = sh->part[slot][k];
+    }
+    __device__ double sum(double v) {
+        double a[1] = {v};
+        sumk<1>(a);
+        return a[0];
+    }
+    __device__ int any(int flag) { return sum(flag ? 1.0 : 0.0) > 0.0; }
+};
+
 }  // namespace rb

@@ -170,3 +170,75 @@ def random_slab_tables(seed: int, precision: str = "fp64", max_cells: int = 2000
     xs = synthetic_xs(ng, 4, L, seed + 7919, csd=bfp)
     return slab_tables(nx, np.full(nx, width / nx), mats, ng, 4, seed, sn, L, beam_group=0, csd=bfp,
                        precision=precision, xs=xs)
+
+
+def surface_source_md(ndims, ns, ds, positions, Om, w, L: int, btype: str, Qdims: int, ng: int, group: int,
+                      face: str, direction, aperture=None, intensity: float = 1.0):
+    """Moments of a monodirectional beam through one face of a 2D/3D grid (surface_source.jl:
+    129-188 for 2D, :189-276 for 3D): the half-range moments times the face-cell area, inside
+    the aperture ({axis: (lo, hi)}, voxel midpoints compared as the reference does).
+    Returns per-face arrays [ng, Np, face cells] (None for the other faces)."""
+    from .sphere import surface_source_moments
+
+    q, pl, pm = surface_source_moments(Om, w, L, btype, Qdims, face, direction, intensity)
+    Np = len(q)
+    axis = "XYZ".index(face[0])
+    others = [a for a in range(ndims) if a != axis]
+    shape = [ns[a] for a in others]
+    arr = np.zeros((ng, Np, int(np.prod(shape))))
+    mus, etas, xis = direction
+    cosv = [mus, etas, xis][axis]
+    ok_dir = (face[1] == "-" and cosv > 0) or (face[1] == "+" and cosv < 0)
+    if ok_dir:
+        idx = np.ndindex(*shape)
+        for k, cell in enumerate(np.ndindex(*shape[::-1])):
+            cell = cell[::-1]
+            inside, area = True, 1.0
+            for j, a in enumerate(others):
+                pos = positions[a][cell[j]]
+                if aperture and a in aperture and not (aperture[a][0] <= pos <= aperture[a][1]):
+                    inside = False
+                area *= ds[a][cell[j]]
+            if inside:
+                flat = 0
+                stride = 1
+                for j in range(len(shape)):
+                    flat += cell[j] * stride
+                    stride *= shape[j]
+                arr[group, :, flat] = q * area
+        del idx
+    faces = [None] * (2 * ndims)
+    faces["XYZ".index(face[0]) * 2 + (0 if face[1] == "-" else 1)] = arr
+    return faces
+
+
+def grid_tables(ndims, ns, widths, mats, ng, nmat, seed, sn: SNSettings, L_xs: int, beam=None, volume=None,
+                bc=(0, 0, 0, 0, 0, 0), csd=False, precision="fp64", xs: MultigroupXS | None = None):
+    """A 2D/3D Cartesian grid: `widths` per axis, `mats` [nx,ny(,nz)] 1-based; `beam` =
+    (face, group, direction, aperture) and `volume` = (group, {axis: (lo, hi)}) as in the
+    reference's Surface_Source / Volume_Source."""
+    xs = xs or synthetic_xs(ng, nmat, L_xs, seed, csd=csd)
+    ns = list(ns)
+    ds = [np.asarray(wd, dtype=float) for wd in widths]
+    positions = [np.cumsum(d) - d / 2 for d in ds]
+    Qdims = sn.qdims(ndims)
+    Om, w = T.quadrature(sn.quadrature_order, sn.quadrature_type, ndims, Qdims)
+    surf = None
+    if beam is not None:
+        face, group, direction, aperture = beam
+        surf = surface_source_md(ndims, ns, ds, positions, Om, w, min(64, sn.legendre_order), sn.angular_boltzmann,
+                                 Qdims, ng, group, face, direction, aperture)
+    vol = None
+    if volume is not None:
+        group, box = volume
+        full = ns + [1] * (3 - ndims)
+        vol = np.zeros((ng, 1, 1, *full))
+        for idx in np.ndindex(*ns):
+            inside = all(box[a][0] <= positions[a][idx[a]] <= box[a][1] for a in range(ndims) if a in box)
+            if inside:
+                vol[(group, 0, 0) + tuple(idx) + (0,) * (3 - ndims)] = 1.0
+    full = ns + [1] * (3 - ndims)
+    tabs = prepare_sn_tables(xs, ndims, ns, ds, np.asarray(mats).reshape(full, order="F"), list(bc), sn,
+                             volume_sources=vol, surface_sources=surf, precision=precision)
+    tabs["xs"] = xs
+    return tabs
