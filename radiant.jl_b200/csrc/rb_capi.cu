@@ -405,7 +405,7 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     offs[k++] = L.take<double>((size_t)nmat * np);        // 37 kmat (in-group Σs per material and moment)
     offs[k++] = L.take<double>((size_t)nmat * nm5 * nm5); // 38 scsd
     {
-        const long long md = (long long)nd * ((long long)D.ns[1] * D.ns[2] + (long long)D.ns[0] * D.ns[2] +
+        const long long md = (long long)nd * (2LL * D.ns[1] * D.ns[2] + 2LL * D.ns[0] * D.ns[2] +
                                               2LL * D.ns[0] * D.ns[1]) * D.nfmax;
         const long long one = (long long)nd * RB_MAXFACE;
         offs[k++] = L.take<double>(P->ndims == 1 ? one : md);  // 39 fexit / multi-D face scratch
@@ -458,7 +458,7 @@ int launch_grid(rb_context *ctx, DevProblem *prob, cudaStream_t s) {
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb::solve_grid_kernel, RB_THREADS, smem));
     if (per_sm < 1) return fail(ctx, RB_ERR_CUDA, "the grid solve kernel does not fit on an SM");
-    if (per_sm > 2) per_sm = 2;
+    if (per_sm > 1) per_sm = 1;
     const int grid = ctx->nsm * per_sm;
     if (!ctx->d_gpart) CK(cudaMalloc(&ctx->d_gpart, sizeof(double) * 2 * 4 * 4096));
     void *args[] = {(void *)&prob, (void *)&ctx->d_gpart};

@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(RB_THREADS, 2) solve_batch_kernel(DevProblem *
 }
 
 // one large (2D/3D) problem on the whole GPU: a cooperative launch, one team of every CTA
-__global__ void __launch_bounds__(RB_THREADS, 2) solve_grid_kernel(DevProblem *prob, double *gpart) {
+__global__ void __launch_bounds__(RB_THREADS, 1) solve_grid_kernel(DevProblem *prob, double *gpart) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
     GridTeam t;

@@ -109,16 +109,168 @@ struct CellMDrt {
     }
 };
 
+// The same closure with compile-time shapes (NM cell moments, NF face moments per axis, NE
+// energy-face moments): everything stays in registers.
+template <int NM, int NF, int NE, bool CSD, int NAX>
+struct CellMDfix {
+    __device__ static void step(const DevProblem &P, const GroupShared &gs, int n, const double *h, int m,
+                                double (&Qn)[NM], double (&F)[3][NF], double (&FE)[NE]) {
+        double S[NM * NM], q[1][NM];
+#pragma unroll
+        for (int e = 0; e < NM * NM; e++) S[e] = CSD ? P.scsd[(long long)m * NM * NM + e] : 0.0;
+#pragma unroll
+        for (int i = 0; i < NM; i++) { S[i + NM * i] += gs.sigt[m]; q[0][i] = Qn[i]; }
+#pragma unroll
+        for (int a = 0; a < NAX; a++) {
+            const long long blk = (long long)n * 3 + a;
+            const double *Gr = P.G + blk * NM * NM, *Gs = P.Gsrc + blk * NM * P.nfmax;
+#pragma unroll
+            for (int e = 0; e < NM * NM; e++) S[e] += h[a] * __ldg(Gr + e);
+#pragma unroll
+            for (int j = 0; j < NM; j++) {
+                double s = 0.0;
+#pragma unroll
+                for (int f = 0; f < NF; f++) s += __ldg(Gs + j + NM * f) * F[a][f];
+                q[0][j] += h[a] * s;
+            }
+        }
+        if (CSD) {
+#pragma unroll
+            for (int j = 0; j < NM; j++) {
+                double s = 0.0;
+#pragma unroll
+                for (int e = 0; e < NE; e++) s += (__ldg(P.EsA + j + NM * e) * gs.sp[m] - __ldg(P.EsB + j + NM * e) * gs.sm[m]) * FE[e];
+                q[0][j] -= s;
+            }
+        }
+        lu_solve<double, NM, 1>(S, q);
+#pragma unroll
+        for (int a = 0; a < NAX; a++) {
+            const double *Go = P.Gout + ((long long)n * 3 + a) * NM * P.nfmax;
+            double Fo[NF];
+#pragma unroll
+            for (int f = 0; f < NF; f++) {
+                double s = P.w1[a] * F[a][f];
+#pragma unroll
+                for (int j = 0; j < NM; j++) s += __ldg(Go + f + NF * j) * q[0][j];
+                Fo[f] = s;
+            }
+#pragma unroll
+            for (int f = 0; f < NF; f++) F[a][f] = Fo[f];
+        }
+        if (CSD) {
+            double Eo[NE];
+#pragma unroll
+            for (int e = 0; e < NE; e++) {
+                double s = P.w1[3] * FE[e];
+#pragma unroll
+                for (int j = 0; j < NM; j++) s += __ldg(P.Eout + e + NE * j) * q[0][j];
+                Eo[e] = s;
+            }
+#pragma unroll
+            for (int e = 0; e < NE; e++) FE[e] = Eo[e];
+        }
+#pragma unroll
+        for (int j = 0; j < NM; j++) Qn[j] = q[0][j];
+    }
+};
+
+// Run-time shapes routed through CellMDrt, with the arrays of the largest shapes.
+struct CellMDgen {
+    __device__ static void step(const DevProblem &P, const GroupShared &gs, int n, const double *h, int m,
+                                double (&Qn)[RB_MAXNM], double (&F)[3][RB_MAXFACE], double (&FE)[RB_MAXFACE]) {
+        CellMDrt::step(P, gs, n, P.ndims, h, nullptr, m, Qn, F, FE);
+    }
+};
+
 // Scratch layout per direction (global): x exits [ny·nz], y exits [nx·nz], z exits [nx·ny],
-// z faces of the previous plane [nx·ny], each × nfmax doubles.
+// the z-face plane [nx·ny] and (3D) the y-face plane [nx·nz], each × nfmax doubles.
 __device__ __forceinline__ long long md_scratch_stride(const DevProblem &P) {
-    return ((long long)P.ny * P.nz + (long long)P.nx * P.nz + 2LL * P.nx * P.ny) * P.nfmax;
+    return (2LL * P.ny * P.nz + 2LL * P.nx * P.nz + 2LL * P.nx * P.ny) * P.nfmax;
 }
 
-template <class Team>
+// 3D: pencils along x in tiles of TY×TZ (one thread per pencil). Inside a tile the cells form a
+// hyperplane wavefront on ix + iy + iz: at step s the pencil (jy, jz) solves column s − jy − jz,
+// reading the y face its lower neighbour wrote at step s − 1 and the z face its back neighbour
+// wrote at step s − 1, both through per-direction face planes (L2-resident). Tiles are taken in
+// an order that finishes both upwind tiles first (z-tiles outer, y-tiles inner, in sweep order).
+template <class Cell, int AM, int AF, int AE, class Team>
+__device__ void sweep_3d_tiles(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, int np_source,
+                               const double *phiE_in, double *phiE_out, int ig) {
+    const int nd = P.nd, nx = P.nx, ny = P.ny, nz = P.nz, nfm = P.nfmax;
+    const int nm = AM == 1 ? 1 : P.nm5, ne = AE == 1 ? 1 : P.nm4;  // compile-time 1 on the register path
+    const int ncta = (int)t.ncta, crank = (int)t.crank;
+    const int my_dirs = (nd - crank + ncta - 1) / ncta;
+    const int TY = ny < 16 ? ny : 16, TZ = nz < 16 ? nz : 16;
+    const int ntile_y = (ny + TY - 1) / TY, ntile_z = (nz + TZ - 1) / TZ;
+    const int pen = TY * TZ;                               // pencils per tile
+    int D = (int)blockDim.x / pen;                         // directions per round
+    if (D < 1) D = 1;
+    const long long sstride = md_scratch_stride(P);
+    const int nfx = AF == 1 ? 1 : P.nmf[0], nfy = AF == 1 ? 1 : P.nmf[1], nfz = AF == 1 ? 1 : P.nmf[2];
+    for (int k0 = 0; k0 < my_dirs; k0 += D) {
+        const int dl = threadIdx.x / pen, pl = threadIdx.x % pen;
+        const int jy = pl % TY, jz = pl / TY;
+        const bool active = dl < D && k0 + dl < my_dirs;
+        const int n = crank + (k0 + dl) * ncta;
+        const double mu = active ? P.cosv[n] : 0.0, eta = active ? P.cosv[nd + n] : 0.0;
+        const double xi = active ? P.cosv[2 * nd + n] : 0.0;
+        const bool fx = mu >= 0.0, fy = eta >= 0.0, fz = xi >= 0.0;
+        double *scr = P.fexit + (active ? (long long)n * sstride : 0);
+        double *exx = scr, *exy = exx + (long long)ny * nz * nfm, *exz = exy + (long long)nx * nz * nfm;
+        double *zfc = exz + (long long)nx * ny * nfm, *yfc = zfc + (long long)nx * ny * nfm;
+        for (int tz = 0; tz < ntile_z; tz++) {
+            for (int ty = 0; ty < ntile_y; ty++) {
+                const int iyy = ty * TY + jy, izz = tz * TZ + jz;
+                const bool pcl = active && iyy < ny && izz < nz;
+                const int iy = fy ? iyy : ny - 1 - iyy, iz = fz ? izz : nz - 1 - izz;
+                double F[3][AF], FE[AE], Qn[AM];
+                for (int s = 0; s < nx + TY + TZ - 2; s++) {
+                    const int ixx = s - jy - jz;
+                    if (pcl && ixx >= 0 && ixx < nx) {
+                        const int ix = fx ? ixx : nx - 1 - ixx;
+                        const long long c = ix + (long long)nx * (iy + (long long)ny * iz);
+                        const long long yk = (ix + (long long)nx * iz) * nfm, zk = (ix + (long long)nx * iy) * nfm;
+                        if (ixx == 0)
+                            boundary_in_md(P, n, 0, fx, iy + (long long)ny * iz, zin, np_source, ig, F[0], nfx);
+                        if (iyy == 0)
+                            boundary_in_md(P, n, 1, fy, ix + (long long)nx * iz, zin, np_source, ig, F[1], nfy);
+                        else
+                            for (int f = 0; f < nfy; f++) F[1][f] = yfc[yk + f];
+                        if (izz == 0)
+                            boundary_in_md(P, n, 2, fz, ix + (long long)nx * iy, zin, np_source, ig, F[2], nfz);
+                        else
+                            for (int f = 0; f < nfz; f++) F[2][f] = zfc[zk + f];
+                        const int m = P.mat[c];
+                        double h[3] = {fabs(mu) / P.dx[ix], fabs(eta) / P.dy[iy], fabs(xi) / P.dz[iz]};
+                        double *pc = P.psi + n + (long long)nd * nm * c;
+                        for (int j = 0; j < nm; j++) Qn[j] = pc[(long long)nd * j];
+                        if (P.csd)
+                            for (int e = 0; e < ne; e++)
+                                FE[e] = phiE_in ? phiE_in[n + (long long)nd * (e + (long long)ne * c)] : 0.0;
+                        Cell::step(P, gs, n, h, m, Qn, F, FE);
+                        for (int j = 0; j < nm; j++) pc[(long long)nd * j] = Qn[j];
+                        if (P.csd)
+                            for (int e = 0; e < ne; e++) phiE_out[n + (long long)nd * (e + (long long)ne * c)] = FE[e];
+                        if (iyy < ny - 1) for (int f = 0; f < nfy; f++) yfc[yk + f] = F[1][f];
+                        else for (int f = 0; f < nfy; f++) exy[yk + f] = F[1][f];
+                        if (izz < nz - 1) for (int f = 0; f < nfz; f++) zfc[zk + f] = F[2][f];
+                        else for (int f = 0; f < nfz; f++) exz[zk + f] = F[2][f];
+                        if (ixx == nx - 1) for (int f = 0; f < nfx; f++) exx[(iy + (long long)ny * iz) * nfm + f] = F[0][f];
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+    }
+}
+
+template <class Cell, int AM, int AF, int AE, class Team>
 __device__ void sweep_md(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, int np_source,
                          const double *phiE_in, double *phiE_out, int ig) {
-    const int nd = P.nd, nx = P.nx, ny = P.ny, nz = P.nz, nm = P.nm5, nax = P.ndims, nfm = P.nfmax;
+    const int nd = P.nd, nx = P.nx, ny = P.ny, nz = P.nz, nax = P.ndims, nfm = P.nfmax;
+    const int nm = AM == 1 ? 1 : P.nm5, ne = AE == 1 ? 1 : P.nm4;  // compile-time 1 on the register path
+    const int nfx = AF == 1 ? 1 : P.nmf[0], nfz = AF == 1 ? 1 : P.nmf[2];
     const int ncta = (int)t.ncta, crank = (int)t.crank;
     const int my_dirs = (nd - crank + ncta - 1) / ncta;
     const int R = ny < (int)blockDim.x ? ny : (int)blockDim.x;   // rows per direction
@@ -128,7 +280,7 @@ __device__ void sweep_md(Team &t, const DevProblem &P, GroupShared &gs, const do
     const int nrb = (ny + R - 1) / R;
     const long long sstride = md_scratch_stride(P);
     double *yface = gs.tile;  // [D][nx][nf_y]
-    const int nfy = P.nmf[1];
+    const int nfy = AF == 1 ? 1 : P.nmf[1];
     for (int k0 = 0; k0 < my_dirs; k0 += D) {
         const int dl = threadIdx.x / R, r = threadIdx.x % R;
         const bool active = dl < D && k0 + dl < my_dirs;
@@ -146,23 +298,23 @@ __device__ void sweep_md(Team &t, const DevProblem &P, GroupShared &gs, const do
                 const int iyy = rb * R + r;
                 const bool row = active && iyy < ny;
                 const int iy = fy ? iyy : ny - 1 - iyy;
-                double F[3][RB_MAXFACE], FE[RB_MAXFACE], Qn[RB_MAXNM];
+                double F[3][AF], FE[AE], Qn[AM];
                 for (int s = 0; s < nx + R - 1; s++) {
                     const int ixx = s - r;
                     if (row && ixx >= 0 && ixx < nx) {
                         const int ix = fx ? ixx : nx - 1 - ixx;
                         const long long c = ix + (long long)nx * (iy + (long long)ny * iz);
                         if (ixx == 0)  // X face of the row (sn_sweep_2D.jl:103-132)
-                            boundary_in_md(P, n, 0, fx, iy + (long long)ny * iz, zin, np_source, ig, F[0], P.nmf[0]);
+                            boundary_in_md(P, n, 0, fx, iy + (long long)ny * iz, zin, np_source, ig, F[0], nfx);
                         if (iyy == 0)  // Y face of the column (sn_sweep_2D.jl:71-99)
                             boundary_in_md(P, n, 1, fy, ix + (long long)nx * iz, zin, np_source, ig, F[1], nfy);
                         else
                             for (int f = 0; f < nfy; f++) F[1][f] = yf[(long long)ixx * nfy + f];
                         if (nax == 3) {
                             if (izz == 0)  // Z face (sn_sweep_3D.jl:80-108)
-                                boundary_in_md(P, n, 2, fz, ix + (long long)nx * iy, zin, np_source, ig, F[2], P.nmf[2]);
+                                boundary_in_md(P, n, 2, fz, ix + (long long)nx * iy, zin, np_source, ig, F[2], nfz);
                             else
-                                for (int f = 0; f < P.nmf[2]; f++) F[2][f] = zfc[(ix + (long long)nx * iy) * nfm + f];
+                                for (int f = 0; f < nfz; f++) F[2][f] = zfc[(ix + (long long)nx * iy) * nfm + f];
                         }
                         const int m = P.mat[c];
                         double h[3];
@@ -172,21 +324,21 @@ __device__ void sweep_md(Team &t, const DevProblem &P, GroupShared &gs, const do
                         double *pc = P.psi + n + (long long)nd * nm * c;
                         for (int j = 0; j < nm; j++) Qn[j] = pc[(long long)nd * j];
                         if (P.csd)
-                            for (int e = 0; e < P.nm4; e++)
-                                FE[e] = phiE_in ? phiE_in[n + (long long)nd * (e + (long long)P.nm4 * c)] : 0.0;
-                        CellMDrt::step(P, gs, n, nax, h, nullptr, m, Qn, F, FE);
+                            for (int e = 0; e < ne; e++)
+                                FE[e] = phiE_in ? phiE_in[n + (long long)nd * (e + (long long)ne * c)] : 0.0;
+                        Cell::step(P, gs, n, h, m, Qn, F, FE);
                         for (int j = 0; j < nm; j++) pc[(long long)nd * j] = Qn[j];
                         if (P.csd)
-                            for (int e = 0; e < P.nm4; e++) phiE_out[n + (long long)nd * (e + (long long)P.nm4 * c)] = FE[e];
+                            for (int e = 0; e < ne; e++) phiE_out[n + (long long)nd * (e + (long long)ne * c)] = FE[e];
                         for (int f = 0; f < nfy; f++) yf[(long long)ixx * nfy + f] = F[1][f];
                         if (nax == 3) {
                             if (izz < nz - 1)
-                                for (int f = 0; f < P.nmf[2]; f++) zfc[(ix + (long long)nx * iy) * nfm + f] = F[2][f];
+                                for (int f = 0; f < nfz; f++) zfc[(ix + (long long)nx * iy) * nfm + f] = F[2][f];
                             else
-                                for (int f = 0; f < P.nmf[2]; f++) exz[(ix + (long long)nx * iy) * nfm + f] = F[2][f];
+                                for (int f = 0; f < nfz; f++) exz[(ix + (long long)nx * iy) * nfm + f] = F[2][f];
                         }
                         if (ixx == nx - 1)
-                            for (int f = 0; f < P.nmf[0]; f++) exx[(iy + (long long)ny * iz) * nfm + f] = F[0][f];
+                            for (int f = 0; f < nfx; f++) exx[(iy + (long long)ny * iz) * nfm + f] = F[0][f];
                         if (iyy == ny - 1)
                             for (int f = 0; f < nfy; f++) exy[(ix + (long long)nx * iz) * nfm + f] = F[1][f];
                     }
@@ -234,7 +386,16 @@ __device__ void pass_md(Team &t, const DevProblem &P, GroupShared &gs, const dou
     t.sync();
     const int np_source = homog ? 0 : P.np_source;
     const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
-    sweep_md(t, P, gs, zin, np_source, pE, phiE_out, ig);
+    const bool one = P.nm5 == 1 && P.nmf[0] == 1 && P.nmf[1] == 1 && (P.ndims < 3 || P.nmf[2] == 1) && P.nm4 == 1;
+    if (P.ndims == 3) {
+        if (one && !P.csd) sweep_3d_tiles<CellMDfix<1, 1, 1, false, 3>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+        else if (one) sweep_3d_tiles<CellMDfix<1, 1, 1, true, 3>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+        else sweep_3d_tiles<CellMDgen, RB_MAXNM, RB_MAXFACE, RB_MAXFACE>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+    } else {
+        if (one && !P.csd) sweep_md<CellMDfix<1, 1, 1, false, 2>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+        else if (one) sweep_md<CellMDfix<1, 1, 1, true, 2>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+        else sweep_md<CellMDgen, RB_MAXNM, RB_MAXFACE, RB_MAXFACE>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+    }
     t.sync();
     d2m_tiles(t, P, gs, zin, zout, matvec);
     boundary_out_md(t, P, zin, zout, matvec);

@@ -242,3 +242,70 @@ def grid_tables(ndims, ns, widths, mats, ng, nmat, seed, sn: SNSettings, L_xs: i
                              volume_sources=vol, surface_sources=surf, precision=precision)
     tabs["xs"] = xs
     return tabs
+
+
+def c3_tables(seed: int = 1, particle: str = "photon", precision: str = "fp64", n: int = 128, ng: int = 60,
+              quad: int = 12, accel: str = "gmres"):
+    """2D Cartesian photon-electron solve: 128×128 voxels over 20×20 cm, water plus 12 seeded
+    circular inclusions (centres uniform, radii U(0.5, 2) cm, bone or 0.3 g/cc water with
+    probability 1/2), 60 groups per particle 10 keV-10 MeV, level-symmetric S12 (168
+    directions), P5, diamond difference, 2 MeV photon beam on the left face over a 4 cm
+    aperture."""
+    rng = np.random.default_rng(seed)
+    L = 20.0
+    dx = L / n
+    xc = (np.arange(n) + 0.5) * dx
+    mats = np.ones((n, n), dtype=np.int32)
+    for _ in range(12):
+        cx, cy = rng.uniform(0, L, size=2)
+        r = rng.uniform(0.5, 2.0)
+        tag = 2 if rng.uniform() < 0.5 else 3
+        X, Y = np.meshgrid(xc, xc, indexing="ij")
+        mats[(X - cx) ** 2 + (Y - cy) ** 2 <= r * r] = tag
+    eb, e, de = log_groups(ng, 10.0, 0.01)
+    g2 = int(np.nonzero((eb[:-1] >= 2.0) & (eb[1:] < 2.0))[0][0])
+    csd = particle != "photon"
+    st = {"x": "DD", "y": "DD"}
+    so = {"x": 1, "y": 1}
+    if csd:
+        st["E"] = "DD"
+        so["E"] = 1
+    sn = SNSettings(solver_type="BFP" if csd else "BTE", quadrature_type="carlson", quadrature_order=quad,
+                    legendre_order=5, scheme_type=st, scheme_order=so, acceleration=accel,
+                    convergence_criterion=1e-7, angular_fokker_planck="galerkin")
+    xs = synthetic_xs(ng, 3, 5, seed * 11 + (1 if csd else 0), csd=csd, e_top=10.0, e_cut=0.01)
+    beam = ("X-", g2, (1.0, 0.0, 0.0), {1: (8.0, 12.0)}) if not csd else None
+    vol = None if not csd else (g2, {0: (0.0, 4.0), 1: (8.0, 12.0)})
+    return grid_tables(2, [n, n], [np.full(n, dx), np.full(n, dx)], mats, ng, 3, seed, sn, 5, beam=beam,
+                       volume=vol, csd=csd, precision=precision, xs=xs)
+
+
+def c4_tables(seed: int = 1, particle: str = "photon", precision: str = "fp64", n: int = 64, ng: int = 40,
+              quad: int = 8):
+    """3D Cartesian photon-electron solve: 64³ voxels over a 16 cm cube, water with a seeded
+    16³-voxel bone block at a random offset, 40 groups per particle 10 keV-6 MeV,
+    level-symmetric S8 (80 directions), P3, reflective at z=0 (Z-), void elsewhere, isotropic
+    volume source of unit strength in the top group inside the central 8³ voxels, BiCGStab to
+    1e-6."""
+    rng = np.random.default_rng(seed)
+    L = 16.0
+    dx = L / n
+    mats = np.ones((n, n, n), dtype=np.int32)
+    b = max(1, n // 4)
+    o = rng.integers(0, n - b + 1, size=3)
+    mats[o[0]:o[0] + b, o[1]:o[1] + b, o[2]:o[2] + b] = 2
+    csd = particle != "photon"
+    st = {"x": "DD", "y": "DD", "z": "DD"}
+    so = {"x": 1, "y": 1, "z": 1}
+    if csd:
+        st["E"] = "DD"
+        so["E"] = 1
+    sn = SNSettings(solver_type="BFP" if csd else "BTE", quadrature_type="carlson", quadrature_order=quad,
+                    legendre_order=3, scheme_type=st, scheme_order=so, acceleration="bicgstab",
+                    convergence_criterion=1e-6, angular_fokker_planck="galerkin")
+    xs = synthetic_xs(ng, 2, 3, seed * 13 + (1 if csd else 0), csd=csd, e_top=6.0, e_cut=0.01)
+    c = L / 2
+    h = 8 * dx / 2
+    vol = (0, {0: (c - h, c + h), 1: (c - h, c + h), 2: (c - h, c + h)})
+    return grid_tables(3, [n, n, n], [np.full(n, dx)] * 3, mats, ng, 2, seed, sn, 3, volume=vol,
+                       bc=(0, 0, 0, 0, 1, 0), csd=csd, precision=precision, xs=xs)
