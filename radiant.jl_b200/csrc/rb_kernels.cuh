@@ -218,7 +218,7 @@ __device__ __forceinline__ void boundary_in_1d(const DevProblem &P, int n, const
 
 // One cell of the closure in compile-time shapes. map() keeps the face dependence symbolic:
 // F_out = A·F_in + b. step() updates F in place and writes ψ (𝚽n) and the energy-face outputs.
-template <typename R, int NM, int NF, int NE, bool CSD>
+template <typename R, int NM, int NF, int NE, bool CSD, typename PS = double>
 struct Cell1D {
     const DevProblem &P;
     const GroupShared &gs;
@@ -244,7 +244,7 @@ struct Cell1D {
     }
 
     // assemble S and the face-independent part q0 = Qn − E·F_E of cell c
-    __device__ __forceinline__ void assemble(int c, const double *psi, R (&S)[NM * NM], R (&q0)[NM], R &h,
+    __device__ __forceinline__ void assemble(int c, const PS *psi, R (&S)[NM * NM], R (&q0)[NM], R &h,
                                              R (&FE)[NE]) const {
         const int m = P.mat[c];
         h = tang ? R(0) : (R)(amu / P.dx[c]);
@@ -253,7 +253,7 @@ struct Cell1D {
         for (int i = 0; i < NM; i++)
 #pragma unroll
             for (int j = 0; j < NM; j++) S[i + NM * j] = (i == j ? sig : R(0)) + h * Gr[i + NM * j];
-        const double *pc = psi + n + (long long)nd * NM * c;
+        const PS *pc = psi + n + (long long)nd * NM * c;
 #pragma unroll
         for (int j = 0; j < NM; j++) q0[j] = (R)pc[(long long)nd * j];
         if (CSD) {
@@ -273,7 +273,7 @@ struct Cell1D {
         }
     }
 
-    __device__ __forceinline__ void map(int c, const double *psi, R (&A)[NF * NF], R (&b)[NF]) const {
+    __device__ __forceinline__ void map(int c, const PS *psi, R (&A)[NF * NF], R (&b)[NF]) const {
         R S[NM * NM], q[NF + 1][NM], h, FE[NE];
         assemble(c, psi, S, q[0], h, FE);
 #pragma unroll
@@ -306,7 +306,7 @@ struct Cell1D {
         }
     }
 
-    __device__ __forceinline__ void step(int c, double *psi, R (&F)[NF]) const {
+    __device__ __forceinline__ void step(int c, PS *psi, R (&F)[NF]) const {
         R S[NM * NM], q[1][NM], h, FE[NE];
         assemble(c, psi, S, q[0], h, FE);
 #pragma unroll
@@ -338,17 +338,17 @@ struct Cell1D {
                 phiE_out[n + (long long)nd * (e + (long long)NE * c)] = (double)a;
             }
         }
-        double *pc = psi + n + (long long)nd * NM * c;
+        PS *pc = psi + n + (long long)nd * NM * c;
 #pragma unroll
-        for (int j = 0; j < NM; j++) pc[(long long)nd * j] = (double)q[0][j];
+        for (int j = 0; j < NM; j++) pc[(long long)nd * j] = (PS)q[0][j];
     }
 };
 
 // The sweep phase with the chunked scan. Directions are dealt to the CTAs of the team round
 // robin; within a CTA the directions it owns share its threads, `chunks` threads each.
-template <typename R, int NM, int NF, int NE, bool CSD, class Team>
+template <typename R, int NM, int NF, int NE, bool CSD, class Team, typename PS = double>
 __device__ void sweep1d_scan(Team &t, const DevProblem &P, GroupShared &gs, const double *zin_b, int np_source,
-                             const double *phiE_in, double *phiE_out, int ig) {
+                             const double *phiE_in, double *phiE_out, int ig, PS *psi) {
     const int nd = P.nd, nx = P.nx;
     const int ncta = (int)t.ncta, crank = (int)t.crank;
     const int my_dirs = (nd - crank + ncta - 1) / ncta;  // directions n = crank + k·ncta
@@ -366,7 +366,7 @@ __device__ void sweep1d_scan(Team &t, const DevProblem &P, GroupShared &gs, cons
         const int kb = min(nx, ch * L), ke = min(nx, kb + L);
         const bool fwd = active ? (P.cosv[n] >= 0.0) : true;
         if (active) {
-            Cell1D<R, NM, NF, NE, CSD> cell(P, gs, n, phiE_in, phiE_out);
+            Cell1D<R, NM, NF, NE, CSD, PS> cell(P, gs, n, phiE_in, phiE_out);
             R Ac[NF * NF], bc[NF];
 #pragma unroll
             for (int f = 0; f < NF; f++) {
@@ -376,7 +376,7 @@ __device__ void sweep1d_scan(Team &t, const DevProblem &P, GroupShared &gs, cons
             }
             for (int k = kb; k < ke; k++) {
                 R A[NF * NF], b[NF];
-                cell.map(fwd ? k : nx - 1 - k, P.psi, A, b);
+                cell.map(fwd ? k : nx - 1 - k, psi, A, b);
                 R An[NF * NF], bn[NF];  // (A,b)∘(Ac,bc)
 #pragma unroll
                 for (int f = 0; f < NF; f++) {
@@ -433,11 +433,11 @@ __device__ void sweep1d_scan(Team &t, const DevProblem &P, GroupShared &gs, cons
         __syncthreads();
         // re-sweep every chunk from its incoming flux
         if (active) {
-            Cell1D<R, NM, NF, NE, CSD> cell(P, gs, n, phiE_in, phiE_out);
+            Cell1D<R, NM, NF, NE, CSD, PS> cell(P, gs, n, phiE_in, phiE_out);
             R F[NF];
 #pragma unroll
             for (int f = 0; f < NF; f++) F[f] = (R)gs.chF[threadIdx.x][f];
-            for (int k = kb; k < ke; k++) cell.step(fwd ? k : nx - 1 - k, P.psi, F);
+            for (int k = kb; k < ke; k++) cell.step(fwd ? k : nx - 1 - k, psi, F);
             if (ch == chunks - 1)
 #pragma unroll
                 for (int f = 0; f < NF; f++) P.fexit[(long long)n * RB_MAXFACE + f] = (double)F[f];
@@ -515,20 +515,38 @@ __device__ void sweep1d_dir_rt(const DevProblem &P, const GroupShared &gs, int n
     for (int f = 0; f < nf; f++) P.fexit[(long long)n * RB_MAXFACE + f] = F[f];
 }
 
-template <class Team>
-__device__ void sweep1d(Team &t, const DevProblem &P, GroupShared &gs, const double *zin_b, int np_source,
-                        const double *pE, double *phiE_out, int ig) {
+template <typename R, typename PS, class Team>
+__device__ bool sweep1d_fixed(Team &t, const DevProblem &P, GroupShared &gs, const double *zin_b, int np_source,
+                              const double *pE, double *phiE_out, int ig, PS *psi) {
     const int nm = P.nm5, nf = P.nmf[0], ne = P.nm4;
     if (!P.csd) {
-        if (nm == 1 && nf == 1) return sweep1d_scan<double, 1, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
-        if (nm == 2 && nf == 1) return sweep1d_scan<double, 2, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
-        if (nm == 3 && nf == 1) return sweep1d_scan<double, 3, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
+        if (nm == 1 && nf == 1) { sweep1d_scan<R, 1, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, psi); return true; }
+        if (nm == 2 && nf == 1) { sweep1d_scan<R, 2, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, psi); return true; }
+        if (nm == 3 && nf == 1) { sweep1d_scan<R, 3, 1, 1, false>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, psi); return true; }
     } else {
-        if (nm == 1 && nf == 1 && ne == 1) return sweep1d_scan<double, 1, 1, 1, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
-        if (nm == 2 && nf == 1 && ne == 2) return sweep1d_scan<double, 2, 1, 2, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
-        if (nm == 2 && nf == 2 && ne == 1) return sweep1d_scan<double, 2, 2, 1, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
-        if (nm == 4 && nf == 2 && ne == 2) return sweep1d_scan<double, 4, 2, 2, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
+        if (nm == 1 && nf == 1 && ne == 1) { sweep1d_scan<R, 1, 1, 1, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, psi); return true; }
+        if (nm == 2 && nf == 1 && ne == 2) { sweep1d_scan<R, 2, 1, 2, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, psi); return true; }
+        if (nm == 2 && nf == 2 && ne == 1) { sweep1d_scan<R, 2, 2, 1, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, psi); return true; }
+        if (nm == 4 && nf == 2 && ne == 2) { sweep1d_scan<R, 4, 2, 2, true>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, psi); return true; }
     }
+    return false;
+}
+
+template <class Team>
+__device__ void sweep1d(Team &t, const DevProblem &P, GroupShared &gs, const double *zin_b, int np_source,
+                        const double *pE, double *phiE_out, int ig, int mixed) {
+    if (mixed) {  // mixed form: FP32 sweep on the FP32 angular buffer
+        if (sweep1d_fixed<float>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, P.psi32)) return;
+        // other shapes: widen the buffer, sweep in FP64, narrow it back
+        const long long nq = (long long)P.nd * P.nm5 * P.ncell;
+        for (long long i = t.rank(); i < nq; i += t.size()) P.psi[i] = (double)P.psi32[i];
+        t.sync();
+        for (int n = t.rank(); n < P.nd; n += t.size()) sweep1d_dir_rt(P, gs, n, zin_b, np_source, pE, phiE_out, P.psi, ig);
+        t.sync();
+        for (long long i = t.rank(); i < nq; i += t.size()) P.psi32[i] = (float)P.psi[i];
+        return;
+    }
+    if (sweep1d_fixed<double>(t, P, gs, zin_b, np_source, pE, phiE_out, ig, P.psi)) return;
     // other shapes: one thread per direction over the whole team
     for (int n = t.rank(); n < P.nd; n += t.size()) sweep1d_dir_rt(P, gs, n, zin_b, np_source, pE, phiE_out, P.psi, ig);
 }
@@ -542,17 +560,33 @@ __device__ void sweep1d(Team &t, const DevProblem &P, GroupShared &gs, const dou
 // Team-wide product over column tiles: acc[i,col] = Σ_k A[i + lda·k]·w(k,col)·X[k + ldx·col],
 // optionally with a second operator B applied to the unscaled X. Output tiles of TR rows × TC
 // columns are dealt to the team's CTAs; each thread owns a 4×4 block of a tile and the operand
-// panels are staged in shared memory 16 rows of k at a time.
+// panels are staged in shared memory 16 rows of k at a time, converted to the compute type T
+// (double for the plain form, float for the mixed form).
+template <class TX>
 struct ProductArgs {
     const double *A, *B;   // [ni + lda·k] operators (B may be null)
     int lda, ni, nk;
-    const double *X;       // [k + ldx·col]
+    const TX *X;           // [k + ldx·col]
     int ldx;
     long long ncol;
 };
 
-template <class Team, class Scale, class Store>
-__device__ void team_product(Team &t, GroupShared &gs, const ProductArgs &a, Scale scale, Store store) {
+template <typename T> struct Vec4;
+template <> struct Vec4<double> {
+    __device__ static void load(const double *p, double (&o)[4]) {
+        const double2 a = *reinterpret_cast<const double2 *>(p), b = *reinterpret_cast<const double2 *>(p + 2);
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+};
+template <> struct Vec4<float> {
+    __device__ static void load(const float *p, float (&o)[4]) {
+        const float4 a = *reinterpret_cast<const float4 *>(p);
+        o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+    }
+};
+
+template <typename T, class TX, class Team, class Scale, class Store>
+__device__ void team_product(Team &t, GroupShared &gs, const ProductArgs<TX> &a, Scale scale, Store store) {
     constexpr int KC = 16;
     const int ni4 = (a.ni + 3) & ~3;
     const int TR = ni4 < 64 ? ni4 : 64;
@@ -561,54 +595,48 @@ __device__ void team_product(Team &t, GroupShared &gs, const ProductArgs &a, Sca
     const int nrb = (a.ni + TR - 1) / TR;
     const long long ncb = (a.ncol + TC - 1) / TC;
     const bool two = a.B != nullptr;
-    double *As = gs.tile, *Bs = As + KC * TR, *Xs = Bs + (two ? KC * TR : 0), *Zs = Xs + KC * TC;
+    T *As = reinterpret_cast<T *>(gs.tile), *Bs = As + KC * TR, *Xs = Bs + (two ? KC * TR : 0), *Zs = Xs + KC * TC;
     const int ib = threadIdx.x % (TR / 4), cb = threadIdx.x / (TR / 4);
     const bool owner = cb < TC / 4;
     for (long long tl = t.crank; tl < (long long)nrb * ncb; tl += t.ncta) {
         const int i0 = (int)(tl % nrb) * TR;
         const long long c0 = (tl / nrb) * TC;
-        double acc[4][4], accb[4][4];
+        T acc[4][4], accb[4][4];
 #pragma unroll
         for (int x = 0; x < 4; x++)
 #pragma unroll
-            for (int y = 0; y < 4; y++) { acc[x][y] = 0.0; accb[x][y] = 0.0; }
+            for (int y = 0; y < 4; y++) { acc[x][y] = T(0); accb[x][y] = T(0); }
         for (int k0 = 0; k0 < a.nk; k0 += KC) {
             __syncthreads();
             for (int e = threadIdx.x; e < KC * TR; e += blockDim.x) {
                 const int ii = e % TR, kk = e / TR, i = i0 + ii, k = k0 + kk;
                 const bool in = i < a.ni && k < a.nk;
-                As[e] = in ? a.A[i + (long long)a.lda * k] : 0.0;
-                if (two) Bs[e] = in ? a.B[i + (long long)a.lda * k] : 0.0;
+                As[e] = in ? (T)a.A[i + (long long)a.lda * k] : T(0);
+                if (two) Bs[e] = in ? (T)a.B[i + (long long)a.lda * k] : T(0);
             }
             for (int e = threadIdx.x; e < KC * TC; e += blockDim.x) {
                 const int kk = e % KC, cc = e / KC, k = k0 + kk;
                 const long long col = c0 + cc;
                 const bool in = k < a.nk && col < a.ncol;
-                const double v = in ? a.X[k + (long long)a.ldx * col] : 0.0;
-                Xs[kk * TC + cc] = in ? scale(k, col) * v : 0.0;
-                if (two) Zs[kk * TC + cc] = v;
+                const double v = in ? (double)a.X[k + (long long)a.ldx * col] : 0.0;
+                Xs[kk * TC + cc] = in ? (T)(scale(k, col) * v) : T(0);
+                if (two) Zs[kk * TC + cc] = (T)v;
             }
             __syncthreads();
             if (owner) {
 #pragma unroll 4
                 for (int kk = 0; kk < KC; kk++) {
-                    const double2 a01 = *reinterpret_cast<const double2 *>(As + kk * TR + ib * 4);
-                    const double2 a23 = *reinterpret_cast<const double2 *>(As + kk * TR + ib * 4 + 2);
-                    const double2 x01 = *reinterpret_cast<const double2 *>(Xs + kk * TC + cb * 4);
-                    const double2 x23 = *reinterpret_cast<const double2 *>(Xs + kk * TC + cb * 4 + 2);
-                    const double o[4] = {a01.x, a01.y, a23.x, a23.y};
-                    const double v[4] = {x01.x, x01.y, x23.x, x23.y};
+                    T o[4], v[4];
+                    Vec4<T>::load(As + kk * TR + ib * 4, o);
+                    Vec4<T>::load(Xs + kk * TC + cb * 4, v);
 #pragma unroll
                     for (int x = 0; x < 4; x++)
 #pragma unroll
                         for (int y = 0; y < 4; y++) acc[x][y] += o[x] * v[y];
                     if (two) {
-                        const double2 b01 = *reinterpret_cast<const double2 *>(Bs + kk * TR + ib * 4);
-                        const double2 b23 = *reinterpret_cast<const double2 *>(Bs + kk * TR + ib * 4 + 2);
-                        const double2 z01 = *reinterpret_cast<const double2 *>(Zs + kk * TC + cb * 4);
-                        const double2 z23 = *reinterpret_cast<const double2 *>(Zs + kk * TC + cb * 4 + 2);
-                        const double ob[4] = {b01.x, b01.y, b23.x, b23.y};
-                        const double vz[4] = {z01.x, z01.y, z23.x, z23.y};
+                        T ob[4], vz[4];
+                        Vec4<T>::load(Bs + kk * TR + ib * 4, ob);
+                        Vec4<T>::load(Zs + kk * TC + cb * 4, vz);
 #pragma unroll
                         for (int x = 0; x < 4; x++)
 #pragma unroll
@@ -625,7 +653,7 @@ __device__ void team_product(Team &t, GroupShared &gs, const ProductArgs &a, Sca
 #pragma unroll
                 for (int x = 0; x < 4; x++) {
                     const int i = i0 + ib * 4 + x;
-                    if (i < a.ni) store(i, col, acc[x][y], accb[x][y]);
+                    if (i < a.ni) store(i, col, (double)acc[x][y], (double)accb[x][y]);
                 }
             }
         }
@@ -634,36 +662,51 @@ __device__ void team_product(Team &t, GroupShared &gs, const ProductArgs &a, Sca
 }
 
 // ψ[n,col] = add[n,col] + Σ_p Mn[n,p]·ys[mat,p]·𝚽[p,col] + T[mat]·Σ_p (Mn·ℳ)[n,p]·𝚽[p,col]
-// (scaled == 0: ψ = Mn·src, the Mn·Qlout product of the group set-up)
+// (scaled == 0: ψ = Mn·src, the Mn·Qlout product of the group set-up). The mixed form computes
+// it in FP32 into the FP32 angular buffer (the FP64 Mn·Qlout term is added before rounding).
 template <class Team>
 __device__ void m2d_tiles(Team &t, const DevProblem &P, GroupShared &gs, const double *src, const double *add,
-                          int scaled) {
+                          int scaled, int mixed = 0) {
     const int nd = P.nd, np = P.np, nm = P.nm5;
-    ProductArgs a{P.mn, (scaled && P.mnfp) ? P.mnfp : nullptr, nd, nd, np, src, np, (long long)nm * P.ncell};
+    ProductArgs<double> a{P.mn, (scaled && P.mnfp) ? P.mnfp : nullptr, nd, nd, np, src, np, (long long)nm * P.ncell};
     const int *mat = P.mat;
     const double *ys = P.kmat;
-    double *psi = P.psi;
-    team_product(
-        t, gs, a,
-        [=] __device__(int k, long long col) { return scaled ? ys[(long long)mat[col / nm] * np + k] : 1.0; },
-        [=, &gs] __device__(int i, long long col, double v, double vb) {
+    auto sc = [=] __device__(int k, long long col) { return scaled ? ys[(long long)mat[col / nm] * np + k] : 1.0; };
+    if (mixed && scaled) {
+        float *psi = P.psi32;
+        team_product<float>(t, gs, a, sc, [=, &gs] __device__(int i, long long col, double v, double vb) {
             const long long o = col * nd + i;
-            const double tm = (scaled && P.mnfp) ? gs.tg[mat[col / nm]] : 0.0;
-            psi[o] = (add ? add[o] : 0.0) + v + tm * vb;
+            const double tm = P.mnfp ? gs.tg[mat[col / nm]] : 0.0;
+            psi[o] = (float)((add ? add[o] : 0.0) + v + tm * vb);
         });
+        return;
+    }
+    double *psi = P.psi;
+    team_product<double>(t, gs, a, sc, [=, &gs] __device__(int i, long long col, double v, double vb) {
+        const long long o = col * nd + i;
+        const double tm = (scaled && P.mnfp) ? gs.tg[mat[col / nm]] : 0.0;
+        psi[o] = (add ? add[o] : 0.0) + v + tm * vb;
+    });
 }
 
-// zout[p,col] = Σ_n Dn[p,n]·ψ[n,col]   (matvec: zout = zin − that)
+// zout[p,col] = Σ_n Dn[p,n]·ψ[n,col]   (matvec: zout = zin − that); FP32 product in the mixed
+// form, written to the FP64 state.
 template <class Team>
-__device__ void d2m_tiles(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, double *zout, int matvec) {
+__device__ void d2m_tiles(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, double *zout, int matvec,
+                          int mixed = 0) {
     const int nd = P.nd, np = P.np, nm = P.nm5;
-    ProductArgs a{P.dn, nullptr, np, np, nd, P.psi, nd, (long long)nm * P.ncell};
-    team_product(
-        t, gs, a, [] __device__(int, long long) { return 1.0; },
-        [=] __device__(int i, long long col, double v, double) {
-            const long long o = col * np + i;
-            zout[o] = matvec ? zin[o] - v : v;
-        });
+    auto one = [] __device__(int, long long) { return 1.0; };
+    auto st = [=] __device__(int i, long long col, double v, double) {
+        const long long o = col * np + i;
+        zout[o] = matvec ? zin[o] - v : v;
+    };
+    if (mixed) {
+        ProductArgs<float> a{P.dn, nullptr, np, np, nd, P.psi32, nd, (long long)nm * P.ncell};
+        team_product<float>(t, gs, a, one, st);
+    } else {
+        ProductArgs<double> a{P.dn, nullptr, np, np, nd, P.psi, nd, (long long)nm * P.ncell};
+        team_product<double>(t, gs, a, one, st);
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -672,22 +715,22 @@ __device__ void d2m_tiles(Team &t, const DevProblem &P, GroupShared &gs, const d
 // ------------------------------------------------------------------------------------------
 template <class Team>
 __device__ void pass1d(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, double *zout, int homog,
-                       int matvec, int ig, const double *phiE_in, double *phiE_out) {
+                       int matvec, int ig, const double *phiE_in, double *phiE_out, int mixed = 0) {
     const int nd = P.nd, np = P.np, nm = P.nm5;
     const long long ncell = P.ncell;
     const long long ncol = (long long)nm * ncell;  // (is, c) columns
     // M2D over column tiles staged in shared memory
-    m2d_tiles(t, P, gs, zin, homog ? nullptr : P.qnout, 1);
+    m2d_tiles(t, P, gs, zin, homog ? nullptr : P.qnout, 1, mixed);
     t.sync();
     // sweep; homogeneous passes see no surface source and a zero incoming energy flux
     // (sn_inner_pass.jl:37-38)
     const int np_source = homog ? 0 : P.np_source;
     const double *zin_b = zin + P.off_b[0];
     const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
-    sweep1d(t, P, gs, zin_b, np_source, pE, phiE_out, ig);
+    sweep1d(t, P, gs, zin_b, np_source, pE, phiE_out, ig, mixed);
     t.sync();
     // D2M over column tiles staged in shared memory; direction order kept per output
-    d2m_tiles(t, P, gs, zin, zout, matvec);
+    d2m_tiles(t, P, gs, zin, zout, matvec, mixed);
     // outgoing boundary moments: side 1 (X+) collects μ ≥ 0, side 0 (X-) μ < 0
     const int nf = P.nmf[0], nps = P.npsurf;
     const long long nb = P.nb[0];

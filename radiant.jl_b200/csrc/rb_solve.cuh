@@ -40,8 +40,12 @@ struct Solver {
     __device__ double *vec(int k) const { return P.vecs + (long long)k * P.nstate; }
 
     // load_and_pass! (sn_one_speed.jl:138-143): out <- T(zin)
-    __device__ void pass(const double *zin, double *out, int homog, int mv) {
-        if (P.ndims == 1) pass1d(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out);
+    // The mixed form runs every pass with FP32 angular arithmetic except the reconstruction
+    // pass of each group (final = 1), which is FP64: it produces the returned flux moments and
+    // the energy-face flux carried into the next group (the outer defect-correction update).
+    __device__ void pass(const double *zin, double *out, int homog, int mv, int final = 0) {
+        const int mixed = (P.precision == 1 && !final) ? 1 : 0;
+        if (P.ndims == 1) pass1d(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
         else pass_md(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out);
         npass++;
     }
@@ -397,7 +401,7 @@ struct Solver {
         }
         // reconstruction pass (sn_one_speed.jl:184-187)
         double *out = vec(1);
-        fixedpoint(out, z);
+        pass(z, out, 0, 0, 1);
         vcopy(t, flux_g, out, nphi);
         return st;
     }
