@@ -76,6 +76,17 @@ def algorithmic_bytes(t, passes, w=8):
     return b * passes
 
 
+def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
+    """The largest value over all ranks (every rank gets it): timings are max over ranks."""
+    if world <= 1:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -162,11 +173,7 @@ def run_ours(args, rank, world):
             step()
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
     value = updates * world / (ms / 1e3)
 
     # e2e through the C ABI with host buffers: upload + solve + download per step
@@ -194,11 +201,37 @@ def run_ours(args, rank, world):
     for _ in range(e2e_steps):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, world)
+
+    # the mixed-precision form on the same batch (FP32 angular work, FP64 Krylov; 1e-5 contract)
+    mixed = None
+    if args.precision == "fp64" and not args.no_mixed:
+        mtabs = workload_tables(seeds, "mixed", args.workload)
+        mpacks = [PackedProblem(t) for t in mtabs]
+        mh = [ctx.upload(p) for p in mpacks]
+        for _ in range(max(1, args.warmup)):
+            ctx.solve_batch(mh, sptr)
+        torch.cuda.synchronize()
+        mrbs = [ResultBuffers(p) for p in mpacks]
+        for h, rb in zip(mh, mrbs):
+            ctx.download(h, rb)
+        mupd = sum(rb.passes * int(np.prod(t["ns"])) * t["nd"] for rb, t in zip(mrbs, mtabs))
+        err = max(float(np.linalg.norm(a.flux - b.flux) / max(np.linalg.norm(b.flux), 1e-300)) for a, b in zip(mrbs, rbs))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.solve_batch(mh, sptr)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        mms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+        for h in mh:
+            ctx.release(h)
+        mixed = {"value": mupd * world / (mms / 1e3), "unit": "updates/s", "ms_per_step": mms,
+                 "solves_per_s": len(mtabs) * world / (mms / 1e3), "fp64_solves_per_s": len(tabs) * world / (ms / 1e3),
+                 "max_rel_l2_vs_fp64": err, "passes": int(sum(rb.passes for rb in mrbs)),
+                 "fp64_passes": int(sum(rb.passes for rb in rbs))}
+
+    serving = run_serving(args, ctx, dev) if (args.serve > 0 and rank == 0) else None
     ctx.close()
 
     peak, pk = peaks()
@@ -222,7 +255,54 @@ def run_ours(args, rank, world):
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
     }
+    if mixed:
+        line["mixed_form"] = mixed
+    if serving:
+        line["serving"] = serving
     return line
+
+
+def run_serving(args, ctx, dev):
+    """A bounded serving run: a seeded Poisson stream of requests from the serving mix through
+    rb_submit / rb_poll (continuous batching, mixed form for 1D requests), against plain FP64
+    per-request solves of the same requests, one at a time."""
+    from radiant_b200 import serving as S
+    from radiant_b200 import workloads as W
+    from radiant_b200._abi import PackedProblem, ResultBuffers
+
+    n = args.serve
+    reqs_t = W.serving_stream(n, seed=2024, precision="mixed", max_cells=args.serve_cells,
+                              max_groups=args.serve_groups, max_side=args.serve_side)
+    arrivals = S.poisson_arrivals(n, args.serve_rate, seed=7)
+    # warm the request path once
+    S.ServingLoop(ctx).run([S.Request(0, reqs_t[0], 0.0)])
+    reqs = [S.Request(i, t, float(a)) for i, (t, a) in enumerate(zip(reqs_t, arrivals))]
+    S.ServingLoop(ctx).run(reqs)
+    served = S.latency_summary(reqs)
+    upd = sum(r.result.passes * int(np.prod(r.tables["ns"])) * r.tables["nd"] for r in reqs)
+    span = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
+    served["updates_per_s"] = upd / span
+    # plain FP64, one request at a time (per-request drop-in solves)
+    base_t = [dict(t, precision="fp64") for t in reqs_t]
+    lat = []
+    t_all = time.perf_counter()
+    bupd = 0
+    for t in base_t:
+        pp = PackedProblem(t)
+        rb = ResultBuffers(pp)
+        t0 = time.perf_counter()
+        h = ctx.upload(pp)
+        ctx.solve(h)
+        ctx.download(h, rb)
+        ctx.release(h)
+        lat.append(time.perf_counter() - t0)
+        bupd += rb.passes * int(np.prod(t["ns"])) * t["nd"]
+    t_all = time.perf_counter() - t_all
+    lat = np.array(lat)
+    return {"requests": n, "arrival_rate_per_s": args.serve_rate, "mix": "70% 1D slabs / 30% 2D grids (seeded)",
+            "served": served,
+            "fp64_per_request": {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                                 "solves_per_s": n / t_all, "updates_per_s": bupd / t_all}}
 
 
 def p_bytes(t):
@@ -305,6 +385,12 @@ def main():
                     help="c2: the benchmark workload; c1 / c2e8: small cases for profiling captures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per problem team (0: library default)")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--serve", type=int, default=60, help="requests of the serving run (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serve-cells", type=int, default=2000)
+    ap.add_argument("--serve-groups", type=int, default=120)
+    ap.add_argument("--serve-side", type=int, default=128)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -309,3 +309,41 @@ def c4_tables(seed: int = 1, particle: str = "photon", precision: str = "fp64", 
     vol = (0, {0: (c - h, c + h), 1: (c - h, c + h), 2: (c - h, c + h)})
     return grid_tables(3, [n, n, n], [np.full(n, dx)] * 3, mats, ng, 2, seed, sn, 3, volume=vol,
                        bc=(0, 0, 0, 0, 1, 0), csd=csd, precision=precision, xs=xs)
+
+
+def random_grid_tables(seed: int, precision: str = "fp64", max_side: int = 128):
+    """One 2D request of the serving stream: square grid of side U(32, max_side), level-symmetric
+    S4-S12, photon transport (BTE), 1-4 materials in vertical layers, beam on the left face."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(32, max_side + 1))
+    N = int(rng.choice([4, 6, 8, 10, 12]))
+    L = int(rng.integers(1, 4))
+    ng = int(rng.integers(10, 41))
+    nmat = int(rng.integers(1, 5))
+    mats = np.ones((n, n), dtype=np.int32)
+    cuts = np.linspace(0, n, nmat + 1).astype(int)
+    for k in range(nmat):
+        mats[cuts[k]:cuts[k + 1], :] = k + 1
+    sn = SNSettings(solver_type="BTE", quadrature_type="carlson", quadrature_order=N, legendre_order=L,
+                    scheme_type={"x": "DD", "y": "DD"}, scheme_order={"x": 1, "y": 1}, acceleration="gmres",
+                    convergence_criterion=1e-7, angular_boltzmann="standard")
+    width = rng.uniform(5.0, 20.0)
+    d = width / n
+    xs = synthetic_xs(ng, nmat, L, seed + 104729, e_top=10.0, e_cut=0.01)
+    return grid_tables(2, [n, n], [np.full(n, d), np.full(n, d)], mats, ng, nmat, seed, sn, L,
+                       beam=("X-", 0, (1.0, 0.0, 0.0), {1: (0.25 * width, 0.75 * width)}), precision=precision, xs=xs)
+
+
+def serving_stream(n: int, seed: int, precision: str = "mixed", max_cells: int = 2000, max_groups: int = 120,
+                   max_side: int = 128):
+    """The serving request mix: 70 % 1D slabs (random_slab_tables) and 30 % 2D grids
+    (random_grid_tables), seeded; 1D requests in `precision`, 2D requests in FP64."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        s = int(rng.integers(0, 2 ** 31 - 1))
+        if rng.uniform() < 0.7:
+            out.append(random_slab_tables(s, precision=precision, max_cells=max_cells, max_groups=max_groups))
+        else:
+            out.append(random_grid_tables(s, max_side=max_side))
+    return out
