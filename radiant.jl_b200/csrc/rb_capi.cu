@@ -7,6 +7,7 @@
 // point returns a status and records a message for rb_last_error.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstdarg>
@@ -48,6 +49,7 @@ struct rb_context {
     int nsm = 0;
     int cluster = 0;  // CTAs per problem team (0 = sized per batch); RB_CLUSTER_SIZE overrides
     int md_cluster = 0;  // 2D/3D problems on cluster teams instead of the whole GPU (RB_MD_TEAM=cluster)
+    int local1d = 1;     // 1D problems take the cell-split local pass where it fits (RB_LOCAL1D=0: never)
     double *d_gpart = nullptr;  // grid-team reduction partials
     uint64_t budget = 0;
     uint64_t used = 0;
@@ -407,7 +409,7 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
         offs[k++] = L.take<double>((f < 2 * P->ndims && P->surface_sources[f])
                                        ? (size_t)ng * P->np_source * face_cells(P->ndims, D.ns, f / 2) : 0);
     offs[k++] = L.take<double>((size_t)ng * D.nphi);      // 32 flux
-    offs[k++] = L.take<double>((size_t)nvec_for(P) * D.nstate); // 33 vecs
+    offs[k++] = L.take<double>((size_t)nvec_for(P) * ((D.nstate + 1) & ~1LL)); // 33 vecs (even stride)
     offs[k++] = L.take<double>(D.nphi);                   // 34 qlout
     offs[k++] = L.take<double>(nq);                       // 35 qnout
     offs[k++] = L.take<double>(nq);                       // 36 psi
@@ -434,12 +436,51 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     return k;
 }
 
+// Shared memory of the batch kernel (one CTA per SM): GroupShared plus the local region of the
+// 1D local pass, sized for the largest 1D problem of the launch that qualifies. When `widen` is
+// set the cluster may grow (up to 4×, at most RB_MAXCLUSTER CTAs) until that region fits.
+// Problems whose region does not fit take the team-wide pass.
+struct LaunchShape {
+    int cluster;
+    long long local_bytes;
+    size_t smem;
+};
+
+static LaunchShape choose_shape(const std::vector<const DevProblem *> &hs, int cluster, bool widen) {
+    int dev = 0, per_sm = 0, reserved = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const long long gsz = (long long)sizeof(rb::GroupShared);
+    const long long b1 = std::min<long long>(optin, (long long)per_sm - reserved) - gsz;
+    auto need = [&](int C) {
+        long long m = 0;
+        for (const DevProblem *h : hs)
+            if (rb::local1d_ok(*h, C, 1LL << 40)) m = std::max(m, rb::local1d_bytes(*h, C));
+        return m;
+    };
+    LaunchShape sh{cluster, 0, (size_t)gsz};
+    if (need(cluster) == 0 || b1 <= 0) return sh;
+    sh.local_bytes = b1;  // problems larger than the whole region take the team-wide pass
+    for (int C = cluster; C <= (widen ? std::min(RB_MAXCLUSTER, 4 * cluster) : cluster); C *= 2)
+        if (need(C) <= b1) { sh.cluster = C; sh.local_bytes = need(C); break; }
+    sh.local_bytes = (sh.local_bytes + 15) & ~15LL;
+    sh.smem = (size_t)(gsz + sh.local_bytes);
+    return sh;
+}
+
 // Launches the persistent solve kernel as clusters of `cluster` CTAs (one team per problem),
-// as many clusters as fit on the device at once, capped by the number of problems.
-int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm, int cluster, cudaStream_t s) {
+// as many clusters as fit on the device at once, capped by the number of problems. `hs` holds
+// host copies of the problems' records (sizes only) for the shared-memory plan.
+int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm, int cluster, cudaStream_t s,
+                 const std::vector<const DevProblem *> &hs, bool widen) {
     if (cluster < 1) cluster = 1;
     if (cluster > RB_MAXCLUSTER) cluster = RB_MAXCLUSTER;
-    const size_t smem = sizeof(rb::GroupShared);
+    const LaunchShape sh = choose_shape((ctx && !ctx->local1d) ? std::vector<const DevProblem *>() : hs, cluster, widen);
+    cluster = sh.cluster;
+    const size_t smem = sh.smem;
+    const int local_bytes = (int)sh.local_bytes;
     CK(cudaFuncSetAttribute(rb::solve_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (cluster > 8) CK(cudaFuncSetAttribute(rb::solve_batch_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
@@ -459,7 +500,7 @@ int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm,
     if (max_clusters < 1) return fail(ctx, RB_ERR_CUDA, "no cluster of %d CTAs fits on the device", cluster);
     int nclusters = max_clusters < n ? max_clusters : n;
     cfg.gridDim = dim3(cluster * nclusters, 1, 1);
-    CK(cudaLaunchKernelEx(&cfg, rb::solve_batch_kernel, (DevProblem *const *)list, n, queue));
+    CK(cudaLaunchKernelEx(&cfg, rb::solve_batch_kernel, (DevProblem *const *)list, n, queue, local_bytes));
     return RB_OK;
 }
 
@@ -502,9 +543,10 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
     // 1D problems (and 2D/3D ones when RB_MD_TEAM=cluster) share one persistent cluster launch;
     // 2D/3D problems otherwise get the whole GPU each, one cooperative launch after another
     std::vector<DevProblem *> small;
+    std::vector<const DevProblem *> small_h;
     std::vector<ProblemRec *> large;
     for (auto *r : recs) {
-        if (r->h.ndims == 1 || ctx->md_cluster) small.push_back(r->d);
+        if (r->h.ndims == 1 || ctx->md_cluster) { small.push_back(r->d); small_h.push_back(&r->h); }
         else large.push_back(r);
     }
     if (!small.empty()) {
@@ -515,7 +557,8 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
             const DevProblem &h0 = recs[0]->h;
             cluster = h0.nd >= 32 ? 4 : (h0.nd >= 16 ? 4 : (h0.nd >= 8 ? 2 : 1));
         }
-        int st2 = launch_solve(ctx, ctx->d_list, (int)small.size(), ctx->d_queue, ctx->nsm, cluster, s);
+        int st2 = launch_solve(ctx, ctx->d_list, (int)small.size(), ctx->d_queue, ctx->nsm, cluster, s, small_h,
+                               ctx->cluster <= 0);
         if (st2) return st2;
     }
     for (auto *r : large) {
@@ -547,6 +590,7 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     h.nphi = D.nphi; h.nstate = D.nstate;
     for (int d = 0; d < 3; d++) { h.off_b[d] = D.off_b[d]; h.nb[d] = D.nb[d]; }
     h.nvec = nvec_for(P);
+    h.vstride = (D.nstate + 1) & ~1LL;
     for (int a = 0; a < 4; a++) h.w1[a] = D.w1[a];
     for (int f = 0; f < 6; f++) h.bc[f] = P->bc[f];
 #define DP(T, k) (reinterpret_cast<T *>(b + o[k]))
@@ -645,6 +689,7 @@ int32_t rb_create(int32_t device, uint64_t hbm_budget_bytes, rb_context **out) {
     c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)(fr * 0.9);
     if (const char *cs = getenv("RB_CLUSTER_SIZE")) c->cluster = atoi(cs);
     if (const char *mt = getenv("RB_MD_TEAM")) c->md_cluster = strcmp(mt, "cluster") == 0;
+    if (const char *lo = getenv("RB_LOCAL1D")) c->local1d = atoi(lo) != 0;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete c; return fail(nullptr, RB_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
     *out = c;
@@ -827,7 +872,7 @@ int32_t rb_submit(rb_context *ctx, const rb_sn_problem *prob, rb_handle *out) {
     CK(cudaMemsetAsync(r->own_queue, 0, sizeof(int), s));
     CK(cudaMemsetAsync(r->h.status, 0, sizeof(int), s));
     int cluster = ctx->cluster > 0 ? ctx->cluster : (r->h.ndims > 1 ? 16 : (r->h.nd >= 16 ? 4 : 2));
-    st = launch_solve(ctx, r->own_list, 1, r->own_queue, ctx->nsm, cluster, s);
+    st = launch_solve(ctx, r->own_list, 1, r->own_queue, ctx->nsm, cluster, s, {&r->h}, ctx->cluster <= 0);
     if (st) return st;
     CK(cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming));
     CK(cudaEventRecord(r->done, s));
@@ -936,7 +981,7 @@ extern "C" int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_resul
     CK(cudaMemcpyAsync(d_list, &d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(d_queue, 0, sizeof(int), s));
     CK(cudaMemsetAsync(h.status, 0, sizeof(int), s));
-    st = launch_solve(nullptr, d_list, 1, d_queue, 1, 1, s);
+    st = launch_solve(nullptr, d_list, 1, d_queue, 1, 1, s, {&h}, false);
     if (st) return st;
     const int ng = prob->ng;
     if (res->flux) {

@@ -28,6 +28,7 @@ struct DevProblem {
     long long nphi, nstate, off_b[3], nb[3];
     long long fcells[3];  // boundary face cells per axis
     int nvec;          // Krylov vectors allocated in `vecs`
+    long long vstride; // distance between Krylov vectors: nstate rounded up to even (the pad stays 0)
     // ---- tables (device pointers) --------------------------------------------------------
     const double *dx, *dy, *dz;
     const int *mat;    // [ncell] 0-based material
@@ -59,7 +60,7 @@ struct DevProblem {
     int bc[6];
     // ---- work ---------------------------------------------------------------------------
     double *flux;      // [ng][nphi] group-major flux moments
-    double *vecs;      // [nvec][nstate] Krylov / fixed-point vectors
+    double *vecs;      // [nvec][vstride] Krylov / fixed-point vectors
     double *qlout;     // [nphi] out-of-group + volume source of the current group
     double *qnout;     // [nd*nm5*ncell] Mn·Qlout
     double *psi;       // [nd*nm5*ncell] angular source / angular flux (in place)

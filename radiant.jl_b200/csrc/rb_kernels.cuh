@@ -23,55 +23,85 @@
 #define RB_MAXRESTART 48
 #define RB_MAXDEPTH 16
 #define RB_THREADS 256
-#define RB_SCAN_NF 4      // scan path for face-moment counts up to this
+#define RB_SCAN_NF 2      // scan path for face-moment counts up to this (every fixed 1D shape)
 #define RB_MAXCLUSTER 16
-#define RB_TILE_DOUBLES (RB_THREADS * (RB_SCAN_NF * RB_SCAN_NF + 2 * RB_SCAN_NF))
+#define RB_TILE_DOUBLES 5120  // largest staging of team_product (16-deep panels, 32x128 tile)
 
 namespace rb {
 
 // ------------------------------------------------------------------------------------------
 // state algebra (krylov_state.jl:53-114) over [𝚽 | boundary in-moments]. Every loop issues the
-// loads of four strided elements before using them, so each thread keeps four memory requests
-// in flight instead of one.
+// loads of RB_VU strided elements before using them, so each thread keeps that many memory
+// requests in flight instead of one.
 // ------------------------------------------------------------------------------------------
-#define RB_VLOOP4(t, N, LOAD, USE)                                                         \
+#define RB_VU 16  // elements per thread whose loads are in flight together in a vector loop
+#define RB_VLOOP(t, N, LOAD, USE)                                                          \
     {                                                                                      \
         const long long T_ = (t).size();                                                   \
-        long long q0_ = (t).rank();                                                        \
-        for (; q0_ + 3 * T_ < (N); q0_ += 4 * T_) {                                        \
-            _Pragma("unroll") for (int u_ = 0; u_ < 4; u_++) {                             \
+        for (long long q0_ = (t).rank(); q0_ < (N); q0_ += RB_VU * T_) {                   \
+            _Pragma("unroll") for (int u_ = 0; u_ < RB_VU; u_++) {                         \
                 const long long q = q0_ + u_ * T_;                                         \
-                LOAD                                                                       \
+                if (q < (N)) { LOAD }                                                      \
             }                                                                              \
-            _Pragma("unroll") for (int u_ = 0; u_ < 4; u_++) {                             \
+            _Pragma("unroll") for (int u_ = 0; u_ < RB_VU; u_++) {                         \
                 const long long q = q0_ + u_ * T_;                                         \
-                USE                                                                        \
+                if (q < (N)) { USE }                                                       \
             }                                                                              \
-        }                                                                                  \
-        for (; q0_ < (N); q0_ += T_) {                                                     \
-            const int u_ = 0;                                                              \
-            const long long q = q0_;                                                       \
-            LOAD                                                                           \
-            USE                                                                            \
         }                                                                                  \
     }
 
+// Krylov vectors: element pairs (16-byte loads) over [0, vstride), vstride even and every
+// vector 16-byte aligned. CTA r of the team takes the contiguous pair range
+// [np·r/C, np·(r+1)/C) and its threads stride through it, RB_VU2 pairs each in flight.
+#define RB_VU2 8
+#define RB_VPAIRS(t, NP, LOAD, USE)                                                         \
+    {                                                                                      \
+        const long long np_ = (NP);                                                        \
+        const long long p1_ = np_ * ((t).crank + 1) / (t).ncta;                            \
+        for (long long b_ = np_ * (t).crank / (t).ncta + threadIdx.x; b_ < p1_;           \
+             b_ += RB_VU2 * blockDim.x) {                                                  \
+            _Pragma("unroll") for (int u_ = 0; u_ < RB_VU2; u_++) {                        \
+                const long long q = b_ + u_ * blockDim.x;                                  \
+                if (q < p1_) { LOAD }                                                      \
+            }                                                                              \
+            _Pragma("unroll") for (int u_ = 0; u_ < RB_VU2; u_++) {                        \
+                const long long q = b_ + u_ * blockDim.x;                                  \
+                if (q < p1_) { USE }                                                       \
+            }                                                                              \
+        }                                                                                  \
+    }
+#define RB_D2(p) reinterpret_cast<double2 *>(p)
+#define RB_CD2(p) reinterpret_cast<const double2 *>(p)
+
+// dot product of two Krylov vectors (np pairs)
+template <class Team>
+__device__ double vdot2(Team &t, const double *a, const double *b, long long np) {
+    const double2 *a2 = RB_CD2(a), *b2 = RB_CD2(b);
+    double s = 0.0;
+    double2 xa[RB_VU2], xb[RB_VU2];
+    RB_VPAIRS(t, np, { xa[u_] = a2[q]; xb[u_] = b2[q]; }, {
+        s += xa[u_].x * xb[u_].x;
+        s += xa[u_].y * xb[u_].y;
+    })
+    return t.sum(s);
+}
+
 template <class Team>
 __device__ double vdot(Team &t, const double *a, const double *b, long long n) {
-    double s = 0.0, xa[4], xb[4];
-    RB_VLOOP4(t, n, { xa[u_] = a[q]; xb[u_] = b[q]; }, { s += xa[u_] * xb[u_]; (void)q; })
+    double s = 0.0, xa[RB_VU], xb[RB_VU];
+    RB_VLOOP(t, n, { xa[u_] = a[q]; xb[u_] = b[q]; }, { s += xa[u_] * xb[u_]; (void)q; })
     return t.sum(s);
 }
 template <class Team>
 __device__ void vaxpy(Team &t, double al, const double *x, double *y, long long n) {
-    double xx[4], yy[4];
-    RB_VLOOP4(t, n, { xx[u_] = x[q]; yy[u_] = y[q]; }, { y[q] = yy[u_] + al * xx[u_]; })
+    double xx[RB_VU], yy[RB_VU];
+    RB_VLOOP(t, n, { xx[u_] = x[q]; yy[u_] = y[q]; }, { y[q] = yy[u_] + al * xx[u_]; })
     t.sync();
 }
 template <class Team>
 __device__ void vcopy(Team &t, double *d, const double *s, long long n) {
-    double xx[4];
-    RB_VLOOP4(t, n, { xx[u_] = s[q]; }, { d[q] = xx[u_]; })
+    double xx[RB_VU];
+    RB_VLOOP(t, n, { xx[u_] = s[q]; }, { d[q] = xx[u_]; })
     t.sync();
 }
 template <class Team>
@@ -82,8 +112,8 @@ __device__ void vzero(Team &t, double *d, long long n) {
 // y = a·x + b·y
 template <class Team>
 __device__ void vlin(Team &t, double a, const double *x, double b, double *y, long long n) {
-    double xx[4], yy[4];
-    RB_VLOOP4(t, n, { xx[u_] = x[q]; yy[u_] = y[q]; }, { y[q] = a * xx[u_] + b * yy[u_]; })
+    double xx[RB_VU], yy[RB_VU];
+    RB_VLOOP(t, n, { xx[u_] = x[q]; yy[u_] = y[q]; }, { y[q] = a * xx[u_] + b * yy[u_]; })
     t.sync();
 }
 
@@ -229,9 +259,17 @@ struct Cell1D {
     R w1x, w1E;
     const double *phiE_in;
     double *phiE_out;
+    long long ld;   // ψ element (n, j, c) sits at psi[n + ld·(j + NM·(c − c0))]
+    int c0;
+    const int *matp;       // material of cell c at matp[c − c0] (the cell tables start at cell c0)
+    const double *dxp;     // width of cell c at dxp[c − c0]
+    const double *scsdp;   // CSD block of the cell matrix per material
 
-    __device__ Cell1D(const DevProblem &P_, const GroupShared &gs_, int n_, const double *pEi, double *pEo)
-        : P(P_), gs(gs_), n(n_), nd(P_.nd), phiE_in(pEi), phiE_out(pEo) {
+    __device__ Cell1D(const DevProblem &P_, const GroupShared &gs_, int n_, const double *pEi, double *pEo,
+                      long long ld_ = -1, int c0_ = 0, const int *matp_ = nullptr, const double *dxp_ = nullptr,
+                      const double *scsdp_ = nullptr)
+        : P(P_), gs(gs_), n(n_), nd(P_.nd), phiE_in(pEi), phiE_out(pEo), ld(ld_ < 0 ? P_.nd : ld_), c0(c0_),
+          matp(matp_ ? matp_ : P_.mat + c0_), dxp(dxp_ ? dxp_ : P_.dx + c0_), scsdp(scsdp_ ? scsdp_ : P_.scsd) {
         tang = P.tang[n] != 0;
         amu = fabs(P.cosv[n]);
         const long long tb = (long long)n * 3;  // axis-0 block of direction n
@@ -246,18 +284,18 @@ struct Cell1D {
     // assemble S and the face-independent part q0 = Qn − E·F_E of cell c
     __device__ __forceinline__ void assemble(int c, const PS *psi, R (&S)[NM * NM], R (&q0)[NM], R &h,
                                              R (&FE)[NE]) const {
-        const int m = P.mat[c];
-        h = tang ? R(0) : (R)(amu / P.dx[c]);
+        const int m = matp[c - c0];
+        h = tang ? R(0) : (R)(amu / dxp[c - c0]);
         const R sig = (R)gs.sigt[m];
 #pragma unroll
         for (int i = 0; i < NM; i++)
 #pragma unroll
             for (int j = 0; j < NM; j++) S[i + NM * j] = (i == j ? sig : R(0)) + h * Gr[i + NM * j];
-        const PS *pc = psi + n + (long long)nd * NM * c;
+        const PS *pc = psi + n + ld * NM * (c - c0);
 #pragma unroll
-        for (int j = 0; j < NM; j++) q0[j] = (R)pc[(long long)nd * j];
+        for (int j = 0; j < NM; j++) q0[j] = (R)pc[ld * j];
         if (CSD) {
-            const double *Sc = P.scsd + (long long)m * NM * NM;
+            const double *Sc = scsdp + (long long)m * NM * NM;
 #pragma unroll
             for (int k2 = 0; k2 < NM * NM; k2++) S[k2] += (R)Sc[k2];
 #pragma unroll
@@ -338,9 +376,9 @@ struct Cell1D {
                 phiE_out[n + (long long)nd * (e + (long long)NE * c)] = (double)a;
             }
         }
-        PS *pc = psi + n + (long long)nd * NM * c;
+        PS *pc = psi + n + ld * NM * (c - c0);
 #pragma unroll
-        for (int j = 0; j < NM; j++) pc[(long long)nd * j] = (PS)q[0][j];
+        for (int j = 0; j < NM; j++) pc[ld * j] = (PS)q[0][j];
     }
 };
 
@@ -557,11 +595,14 @@ __device__ void sweep1d(Team &t, const DevProblem &P, GroupShared &gs, const dou
 // is one contiguous block, staged in shared memory with coalesced loads. The small operators
 // (Mn, Mn·ℳ, Dn) are read through the read-only cache. Tiles are dealt to the team's CTAs.
 // ------------------------------------------------------------------------------------------
-// Team-wide product over column tiles: acc[i,col] = Σ_k A[i + lda·k]·w(k,col)·X[k + ldx·col],
-// optionally with a second operator B applied to the unscaled X. Output tiles of TR rows × TC
-// columns are dealt to the team's CTAs; each thread owns a 4×4 block of a tile and the operand
-// panels are staged in shared memory 16 rows of k at a time, converted to the compute type T
-// (double for the plain form, float for the mixed form).
+// Team-wide product over column tiles: acc[i,col] = Σ_k Op[i,k]·w(k,col)·X[k mod nk, col] with
+// Op = [A | B] (B optional, then k runs over 2·nk): a second operator applied to X under its own
+// per-column scale is one longer contraction. In FP64 one accumulator serves both parts; in
+// FP32 each part has its own and they are added in FP64, so a large Fokker-Planck term and
+// the scattering term it nearly cancels are not summed in single precision. Output tiles of
+// TR rows × TC columns are dealt to the team's CTAs; each thread owns a 4×4 block of a tile and
+// the operand panels are staged in shared memory 16 values of k at a time, converted to the
+// compute type T (double for the plain form, float for the mixed form).
 template <class TX>
 struct ProductArgs {
     const double *A, *B;   // [ni + lda·k] operators (B may be null)
@@ -585,42 +626,73 @@ template <> struct Vec4<float> {
     }
 };
 
-template <typename T, class TX, class Team, class Scale, class Store>
-__device__ void team_product(Team &t, GroupShared &gs, const ProductArgs<TX> &a, Scale scale, Store store) {
+template <typename T, class TX, class Team, class Scale, class Pre, class Store>
+__device__ void team_product(Team &t, GroupShared &gs, const ProductArgs<TX> &a, Scale scale, Pre pre, Store store) {
     constexpr int KC = 16;
+    constexpr int EA = (KC * 64 + RB_THREADS - 1) / RB_THREADS;   // operator elements per thread
+    constexpr int EX = (KC * 128 + RB_THREADS - 1) / RB_THREADS;  // column elements per thread
     const int ni4 = (a.ni + 3) & ~3;
     const int TR = ni4 < 64 ? ni4 : 64;
-    int TC = 4096 / TR;
+    int TC = (4096 / TR) & ~3;  // a multiple of 4: the 4-column blocks stay 16-byte aligned
     if (TC > 128) TC = 128;
     const int nrb = (a.ni + TR - 1) / TR;
     const long long ncb = (a.ncol + TC - 1) / TC;
-    const bool two = a.B != nullptr;
-    T *As = reinterpret_cast<T *>(gs.tile), *Bs = As + KC * TR, *Xs = Bs + (two ? KC * TR : 0), *Zs = Xs + KC * TC;
+    const int nk = a.nk, nkt = a.B ? 2 * a.nk : a.nk;
+    // padded row of the column panel (16 bytes more in FP64, 16 in FP32): the transposing
+    // stores spread over the banks and every 4-column block stays 16-byte aligned
+    const int TCP = TC + (sizeof(T) == 8 ? 2 : 4);
+    T *As = reinterpret_cast<T *>(gs.tile), *Xs = As + KC * TR;
     const int ib = threadIdx.x % (TR / 4), cb = threadIdx.x / (TR / 4);
     const bool owner = cb < TC / 4;
     for (long long tl = t.crank; tl < (long long)nrb * ncb; tl += t.ncta) {
         const int i0 = (int)(tl % nrb) * TR;
         const long long c0 = (tl / nrb) * TC;
-        T acc[4][4], accb[4][4];
+        constexpr bool SPLIT = sizeof(T) < 8;
+        T acc[4][4], accb[SPLIT ? 4 : 1][SPLIT ? 4 : 1];
 #pragma unroll
         for (int x = 0; x < 4; x++)
 #pragma unroll
-            for (int y = 0; y < 4; y++) { acc[x][y] = T(0); accb[x][y] = T(0); }
-        for (int k0 = 0; k0 < a.nk; k0 += KC) {
-            __syncthreads();
-            for (int e = threadIdx.x; e < KC * TR; e += blockDim.x) {
-                const int ii = e % TR, kk = e / TR, i = i0 + ii, k = k0 + kk;
-                const bool in = i < a.ni && k < a.nk;
-                As[e] = in ? (T)a.A[i + (long long)a.lda * k] : T(0);
-                if (two) Bs[e] = in ? (T)a.B[i + (long long)a.lda * k] : T(0);
+            for (int y = 0; y < 4; y++) acc[x][y] = T(0);
+        if (SPLIT)
+#pragma unroll
+            for (int x = 0; x < 4; x++)
+#pragma unroll
+                for (int y = 0; y < 4; y++) accb[SPLIT ? x : 0][SPLIT ? y : 0] = T(0);
+        // panels of the A part cover k < nk, those of the B part start at nk
+        const int npa = (nk + KC - 1) / KC, npanel = a.B ? 2 * npa : npa;
+        for (int ip = 0; ip < npanel; ip++) {
+            const bool partb = ip >= npa;
+            const int k0 = partb ? nk + (ip - npa) * KC : ip * KC;
+            const int kend = partb ? nkt : nk;
+            // every load of the panel is issued before the first shared-memory store
+            double av[EA], xv[EX], sv[EX];
+#pragma unroll
+            for (int u = 0; u < EA; u++) {
+                const int e = threadIdx.x + u * RB_THREADS;
+                const int i = i0 + e % TR, k = k0 + e / TR;
+                const bool in = e < KC * TR && i < a.ni && k < kend;
+                const double *op = k < nk ? a.A : a.B;
+                av[u] = in ? op[i + (long long)a.lda * (k < nk ? k : k - nk)] : 0.0;
             }
-            for (int e = threadIdx.x; e < KC * TC; e += blockDim.x) {
-                const int kk = e % KC, cc = e / KC, k = k0 + kk;
-                const long long col = c0 + cc;
-                const bool in = k < a.nk && col < a.ncol;
-                const double v = in ? (double)a.X[k + (long long)a.ldx * col] : 0.0;
-                Xs[kk * TC + cc] = in ? (T)(scale(k, col) * v) : T(0);
-                if (two) Zs[kk * TC + cc] = (T)v;
+#pragma unroll
+            for (int u = 0; u < EX; u++) {
+                const int e = threadIdx.x + u * RB_THREADS;
+                const int k = k0 + e % KC;
+                const long long col = c0 + e / KC;
+                const bool in = e < KC * TC && k < kend && col < a.ncol;
+                xv[u] = in ? (double)a.X[(k < nk ? k : k - nk) + (long long)a.ldx * col] : 0.0;
+                sv[u] = in ? scale(k, col) : 0.0;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < EA; u++) {
+                const int e = threadIdx.x + u * RB_THREADS;
+                if (e < KC * TR) As[e] = (T)av[u];
+            }
+#pragma unroll
+            for (int u = 0; u < EX; u++) {
+                const int e = threadIdx.x + u * RB_THREADS;
+                if (e < KC * TC) Xs[(e % KC) * TCP + e / KC] = (T)(sv[u] * xv[u]);
             }
             __syncthreads();
             if (owner) {
@@ -628,24 +700,31 @@ __device__ void team_product(Team &t, GroupShared &gs, const ProductArgs<TX> &a,
                 for (int kk = 0; kk < KC; kk++) {
                     T o[4], v[4];
                     Vec4<T>::load(As + kk * TR + ib * 4, o);
-                    Vec4<T>::load(Xs + kk * TC + cb * 4, v);
-#pragma unroll
-                    for (int x = 0; x < 4; x++)
-#pragma unroll
-                        for (int y = 0; y < 4; y++) acc[x][y] += o[x] * v[y];
-                    if (two) {
-                        T ob[4], vz[4];
-                        Vec4<T>::load(Bs + kk * TR + ib * 4, ob);
-                        Vec4<T>::load(Zs + kk * TC + cb * 4, vz);
+                    Vec4<T>::load(Xs + kk * TCP + cb * 4, v);
+                    if (SPLIT && partb) {
 #pragma unroll
                         for (int x = 0; x < 4; x++)
 #pragma unroll
-                            for (int y = 0; y < 4; y++) accb[x][y] += ob[x] * vz[y];
+                            for (int y = 0; y < 4; y++) accb[SPLIT ? x : 0][SPLIT ? y : 0] += o[x] * v[y];
+                    } else {
+#pragma unroll
+                        for (int x = 0; x < 4; x++)
+#pragma unroll
+                            for (int y = 0; y < 4; y++) acc[x][y] += o[x] * v[y];
                     }
                 }
             }
         }
-        if (owner) {
+        if (owner) {  // epilogue: the loads `pre` makes for the 16 outputs first, then the stores
+            double pv[4][4];
+#pragma unroll
+            for (int y = 0; y < 4; y++)
+#pragma unroll
+                for (int x = 0; x < 4; x++) {
+                    const long long col = c0 + cb * 4 + y;
+                    const int i = i0 + ib * 4 + x;
+                    pv[x][y] = (col < a.ncol && i < a.ni) ? pre(i, col) : 0.0;
+                }
 #pragma unroll
             for (int y = 0; y < 4; y++) {
                 const long long col = c0 + cb * 4 + y;
@@ -653,7 +732,9 @@ __device__ void team_product(Team &t, GroupShared &gs, const ProductArgs<TX> &a,
 #pragma unroll
                 for (int x = 0; x < 4; x++) {
                     const int i = i0 + ib * 4 + x;
-                    if (i < a.ni) store(i, col, (double)acc[x][y], (double)accb[x][y]);
+                    if (i < a.ni)
+                        store(i, col, SPLIT ? (double)acc[x][y] + (double)accb[SPLIT ? x : 0][SPLIT ? y : 0] : (double)acc[x][y],
+                              pv[x][y]);
                 }
             }
         }
@@ -661,7 +742,7 @@ __device__ void team_product(Team &t, GroupShared &gs, const ProductArgs<TX> &a,
     __syncthreads();
 }
 
-// ψ[n,col] = add[n,col] + Σ_p Mn[n,p]·ys[mat,p]·𝚽[p,col] + T[mat]·Σ_p (Mn·ℳ)[n,p]·𝚽[p,col]
+// ψ[n,col] = add[n,col] + Σ_p Mn[n,p]·ys[mat,p]·𝚽[p,col] + Σ_p (Mn·ℳ)[n,p]·T[mat]·𝚽[p,col]
 // (scaled == 0: ψ = Mn·src, the Mn·Qlout product of the group set-up). The mixed form computes
 // it in FP32 into the FP32 angular buffer (the FP64 Mn·Qlout term is added before rounding).
 template <class Team>
@@ -671,21 +752,22 @@ __device__ void m2d_tiles(Team &t, const DevProblem &P, GroupShared &gs, const d
     ProductArgs<double> a{P.mn, (scaled && P.mnfp) ? P.mnfp : nullptr, nd, nd, np, src, np, (long long)nm * P.ncell};
     const int *mat = P.mat;
     const double *ys = P.kmat;
-    auto sc = [=] __device__(int k, long long col) { return scaled ? ys[(long long)mat[col / nm] * np + k] : 1.0; };
+    auto sc = [=, &gs] __device__(int k, long long col) {
+        if (!scaled) return 1.0;
+        const int m = mat[col / nm];
+        return k < np ? ys[(long long)m * np + k] : gs.tg[m];
+    };
+    auto pre = [=] __device__(int i, long long col) { return add ? add[col * nd + i] : 0.0; };
     if (mixed && scaled) {
         float *psi = P.psi32;
-        team_product<float>(t, gs, a, sc, [=, &gs] __device__(int i, long long col, double v, double vb) {
-            const long long o = col * nd + i;
-            const double tm = P.mnfp ? gs.tg[mat[col / nm]] : 0.0;
-            psi[o] = (float)((add ? add[o] : 0.0) + v + tm * vb);
+        team_product<float>(t, gs, a, sc, pre, [=] __device__(int i, long long col, double v, double ad) {
+            psi[col * nd + i] = (float)(ad + v);
         });
         return;
     }
     double *psi = P.psi;
-    team_product<double>(t, gs, a, sc, [=, &gs] __device__(int i, long long col, double v, double vb) {
-        const long long o = col * nd + i;
-        const double tm = (scaled && P.mnfp) ? gs.tg[mat[col / nm]] : 0.0;
-        psi[o] = (add ? add[o] : 0.0) + v + tm * vb;
+    team_product<double>(t, gs, a, sc, pre, [=] __device__(int i, long long col, double v, double ad) {
+        psi[col * nd + i] = ad + v;
     });
 }
 
@@ -696,16 +778,14 @@ __device__ void d2m_tiles(Team &t, const DevProblem &P, GroupShared &gs, const d
                           int mixed = 0) {
     const int nd = P.nd, np = P.np, nm = P.nm5;
     auto one = [] __device__(int, long long) { return 1.0; };
-    auto st = [=] __device__(int i, long long col, double v, double) {
-        const long long o = col * np + i;
-        zout[o] = matvec ? zin[o] - v : v;
-    };
+    auto pre = [=] __device__(int i, long long col) { return matvec ? zin[col * np + i] : 0.0; };
+    auto st = [=] __device__(int i, long long col, double v, double z) { zout[col * np + i] = matvec ? z - v : v; };
     if (mixed) {
         ProductArgs<float> a{P.dn, nullptr, np, np, nd, P.psi32, nd, (long long)nm * P.ncell};
-        team_product<float>(t, gs, a, one, st);
+        team_product<float>(t, gs, a, one, pre, st);
     } else {
         ProductArgs<double> a{P.dn, nullptr, np, np, nd, P.psi, nd, (long long)nm * P.ncell};
-        team_product<double>(t, gs, a, one, st);
+        team_product<double>(t, gs, a, one, pre, st);
     }
 }
 
@@ -716,9 +796,7 @@ __device__ void d2m_tiles(Team &t, const DevProblem &P, GroupShared &gs, const d
 template <class Team>
 __device__ void pass1d(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, double *zout, int homog,
                        int matvec, int ig, const double *phiE_in, double *phiE_out, int mixed = 0) {
-    const int nd = P.nd, np = P.np, nm = P.nm5;
-    const long long ncell = P.ncell;
-    const long long ncol = (long long)nm * ncell;  // (is, c) columns
+    const int nd = P.nd;
     // M2D over column tiles staged in shared memory
     m2d_tiles(t, P, gs, zin, homog ? nullptr : P.qnout, 1, mixed);
     t.sync();

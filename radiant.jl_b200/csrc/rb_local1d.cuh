@@ -1,0 +1,349 @@
+// rb_local1d.cuh -- the 1D transport pass with the cells split over the CTAs of the cluster.
+//
+// CTA r of a C-CTA cluster owns the contiguous cells [r·Lc, min(Nx, (r+1)·Lc)), Lc = ⌈Nx/C⌉,
+// and keeps the angular array ψ of its cells in shared memory for the whole pass:
+//   M2D    ψ[n, is, c] of its cells from the moments in HBM (a CTA-local tiled product),
+//   sweep  every direction over its own cells: each thread composes the affine face map
+//          F_out = A·F_in + b of a chunk of cells (sn_sweep_1D.jl:93-112 with the closure of
+//          flux_1D_BTE / flux_1D_BFP), the chunk maps of a direction are composed into the
+//          CTA's map, the CTA maps are exchanged through distributed shared memory (the one
+//          cluster barrier inside the pass), every CTA chains the maps of the CTAs upstream of
+//          it from the boundary flux (sn_sweep_1D.jl:60-91) and re-sweeps its chunks,
+//   D2M    𝚽 = Dn·ψ of its cells straight into the output state.
+// CTA 0 chains every CTA's map, which gives the exit flux of each direction, and writes the
+// outgoing boundary moments (sn_sweep_1D.jl:115-121, lagged as sn_inner_pass.jl:127-134).
+// So ψ never leaves the SM and a pass costs two cluster barriers (the map exchange and the
+// end of the pass). The per-cell tables (material, width, the group's CSD blocks and in-group
+// Σs) are copied into shared memory once per group.
+#pragma once
+#include <type_traits>
+
+#include "rb_kernels.cuh"
+
+namespace rb {
+
+#define RB_LMAP (RB_SCAN_NF * RB_SCAN_NF + RB_SCAN_NF)  // doubles of one face map
+
+// a CTA-local team: team_product over this CTA's columns only
+struct CtaTeam {
+    unsigned crank = 0, ncta = 1;
+};
+
+// shape of the fixed-size cell systems (the instantiated closures)
+__host__ __device__ __forceinline__ bool local1d_shape(const DevProblem &P) {
+    const int nm = P.nm5, nf = P.nmf[0], ne = P.nm4;
+    if (!P.csd) return nf == 1 && (nm == 1 || nm == 2 || nm == 3);
+    return (nm == 1 && nf == 1 && ne == 1) || (nm == 2 && nf == 1 && ne == 2) || (nm == 2 && nf == 2 && ne == 1) ||
+           (nm == 4 && nf == 2 && ne == 2);
+}
+
+// bytes of the local region a problem needs on a cluster of `ncta` CTAs: face maps, exit
+// fluxes, the group's in-group Σs per material and moment, the CSD cell blocks per material,
+// the width and material of each owned cell, then ψ of the owned cells
+__host__ __device__ __forceinline__ long long local1d_bytes(const DevProblem &P, int ncta) {
+    const long long lc = (P.nx + ncta - 1) / ncta, nd = P.nd, nm = P.nm5;
+    return nd * (RB_LMAP + RB_SCAN_NF) * 8 + (long long)P.nmat * P.np * 8 + (long long)P.nmat * nm * nm * 8 +
+           lc * 8 + ((lc * 4 + 15) & ~15LL) + (nd + 1) * nm * lc * 8;
+}
+
+// whether a problem takes the local pass on a cluster of `ncta` CTAs with `local_bytes` of
+// shared memory beyond the per-CTA state
+__host__ __device__ __forceinline__ bool local1d_ok(const DevProblem &P, int ncta, long long local_bytes) {
+    return P.ndims == 1 && local1d_shape(P) && P.nd <= RB_THREADS && local1d_bytes(P, ncta) <= local_bytes;
+}
+
+struct Local1D {
+    double *cmap;   // [nd][RB_LMAP] this CTA's face map per direction (A column-major, then b)
+    double *fx;     // [nd][RB_SCAN_NF] exit flux per direction (CTA 0)
+    double *kmat;   // [nmat][np] in-group Σs of each moment's Legendre order (this group)
+    double *scsd;   // [nmat][nm·nm] CSD block of the cell matrix (this group)
+    double *dx;     // [lc] widths of the owned cells
+    int *mat;       // [lc] materials of the owned cells
+    void *psi;      // [ncl][ldp] ψ of the local columns (double or float)
+    long long ldp;  // leading dimension of ψ (nd + 1: odd, so column accesses spread over banks)
+    int cb, ce;     // owned cells [cb, ce)
+
+    __device__ Local1D(const DevProblem &P, unsigned crank, unsigned ncta, void *base) {
+        const int lc = (P.nx + (int)ncta - 1) / (int)ncta;
+        cb = min(P.nx, (int)crank * lc);
+        ce = min(P.nx, cb + lc);
+        cmap = reinterpret_cast<double *>(base);
+        fx = cmap + (long long)P.nd * RB_LMAP;
+        kmat = fx + (long long)P.nd * RB_SCAN_NF;
+        scsd = kmat + (long long)P.nmat * P.np;
+        dx = scsd + (long long)P.nmat * P.nm5 * P.nm5;
+        mat = reinterpret_cast<int *>(dx + lc);
+        psi = reinterpret_cast<unsigned char *>(mat) + ((lc * 4 + 15) & ~15);
+        ldp = P.nd + 1;
+    }
+};
+
+// per-group copy of the tables the local pass reads per cell (after the group's constants are set)
+__device__ __forceinline__ void local1d_group_setup(const DevProblem &P, Local1D &L) {
+    const int nl = L.ce - L.cb;
+    const int nk = P.nmat * P.np, ns = P.csd ? P.nmat * P.nm5 * P.nm5 : 0;
+    for (int o = threadIdx.x; o < nk; o += blockDim.x) L.kmat[o] = P.kmat[o];
+    for (int o = threadIdx.x; o < ns; o += blockDim.x) L.scsd[o] = P.scsd[o];
+    for (int c = threadIdx.x; c < nl; c += blockDim.x) {
+        L.dx[c] = P.dx[L.cb + c];
+        L.mat[c] = P.mat[L.cb + c];
+    }
+    __syncthreads();
+}
+
+// compose (A,b) ← (A2,b2)∘(A,b): F ↦ A2·(A·F + b) + b2
+template <typename R, int NF>
+__device__ __forceinline__ void compose_map(const R (&A2)[NF * NF], const R (&b2)[NF], R (&A)[NF * NF], R (&b)[NF]) {
+    R An[NF * NF], bn[NF];
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        R s = b2[f];
+#pragma unroll
+        for (int g = 0; g < NF; g++) s += A2[f + NF * g] * b[g];
+        bn[f] = s;
+#pragma unroll
+        for (int g = 0; g < NF; g++) {
+            R a = R(0);
+#pragma unroll
+            for (int h = 0; h < NF; h++) a += A2[f + NF * h] * A[h + NF * g];
+            An[f + NF * g] = a;
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        b[f] = bn[f];
+#pragma unroll
+        for (int g = 0; g < NF; g++) A[f + NF * g] = An[f + NF * g];
+    }
+}
+
+// F ← A·F + b for a map stored as [A column-major | b]
+template <typename R, int NF>
+__device__ __forceinline__ void apply_map(const double *M, R (&F)[NF]) {
+    R Fn[NF];
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+        R s = (R)M[NF * NF + f];
+#pragma unroll
+        for (int g = 0; g < NF; g++) s += (R)M[f + NF * g] * F[g];
+        Fn[f] = s;
+    }
+#pragma unroll
+    for (int f = 0; f < NF; f++) F[f] = Fn[f];
+}
+
+// The sweep over the local cells. Threads: direction n = tid / chunks, chunk = tid % chunks
+// (nd ≤ blockDim.x is required). Ends with ψ of the local cells holding the angular flux and,
+// in CTA 0, the outgoing boundary moments written to zout.
+template <typename R, int NM, int NF, int NE, bool CSD, typename PS>
+__device__ void sweep1d_local(ClusterTeam &t, const DevProblem &P, GroupShared &gs, Local1D &L,
+                              const double *zin, double *zout, int matvec, int np_source, const double *phiE_in,
+                              double *phiE_out, int ig) {
+    const int nd = P.nd;
+    const int nl = L.ce - L.cb;
+    PS *psi = reinterpret_cast<PS *>(L.psi);
+    int chunks = (int)blockDim.x / nd;
+    if (chunks > nl) chunks = nl;
+    if (chunks < 1) chunks = 1;
+    const int dl = threadIdx.x / chunks, ch = threadIdx.x % chunks;
+    const bool active = dl < nd && nl > 0;
+    const int n = dl;
+    const int lk = (nl + chunks - 1) / chunks;
+    const int kb = min(nl, ch * lk), ke = min(nl, kb + lk);
+    const bool fwd = active ? (P.cosv[n] >= 0.0) : true;
+    const int cb = L.cb, ce = L.ce;
+    // 1. chunk maps
+    if (active) {
+        Cell1D<R, NM, NF, NE, CSD, PS> cell(P, gs, n, phiE_in, phiE_out, L.ldp, cb, L.mat, L.dx, L.scsd);
+        R Ac[NF * NF], bc[NF];
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+            bc[f] = R(0);
+#pragma unroll
+            for (int g = 0; g < NF; g++) Ac[f + NF * g] = (f == g) ? R(1) : R(0);
+        }
+        for (int k = kb; k < ke; k++) {
+            R A[NF * NF], b[NF];
+            cell.map(fwd ? cb + k : ce - 1 - k, psi, A, b);
+            compose_map<R, NF>(A, b, Ac, bc);
+        }
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+            gs.chb[threadIdx.x][f] = (double)bc[f];
+#pragma unroll
+            for (int g = 0; g < NF; g++) gs.chA[threadIdx.x][f + NF * g] = (double)Ac[f + NF * g];
+        }
+    }
+    __syncthreads();
+    // 2. the CTA's map of each direction (identity for a CTA without cells)
+    if (dl < nd && ch == 0) {
+        R A[NF * NF], b[NF];
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+            b[f] = R(0);
+#pragma unroll
+            for (int g = 0; g < NF; g++) A[f + NF * g] = (f == g) ? R(1) : R(0);
+        }
+        if (nl > 0)
+            for (int c2 = 0; c2 < chunks; c2++) {
+                R A2[NF * NF], b2[NF];
+                const int tid = dl * chunks + c2;
+#pragma unroll
+                for (int f = 0; f < NF; f++) {
+                    b2[f] = (R)gs.chb[tid][f];
+#pragma unroll
+                    for (int g = 0; g < NF; g++) A2[f + NF * g] = (R)gs.chA[tid][f + NF * g];
+                }
+                compose_map<R, NF>(A2, b2, A, b);
+            }
+        double *M = L.cmap + (long long)n * RB_LMAP;
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+            M[NF * NF + f] = (double)b[f];
+#pragma unroll
+            for (int g = 0; g < NF; g++) M[f + NF * g] = (double)A[f + NF * g];
+        }
+    }
+    t.sync();  // every CTA's maps visible to the cluster
+    // 3. incoming flux of this CTA: the boundary flux through the maps of the CTAs upstream;
+    //    CTA 0 goes on through every map for the exit flux
+    const int C = (int)t.ncta, r = (int)t.crank;
+    if (dl < nd && ch == 0 && (nl > 0 || r == 0)) {
+        cg::cluster_group cl = cg::this_cluster();
+        const bool fw = P.cosv[n] >= 0.0;
+        double F0[RB_MAXFACE];
+        boundary_in_1d(P, n, zin + P.off_b[0], np_source, ig, F0);
+        R F[NF], Fin[NF];
+#pragma unroll
+        for (int f = 0; f < NF; f++) { F[f] = (R)F0[f]; Fin[f] = F[f]; }
+        for (int s = 0; s < C; s++) {
+            const int q = fw ? s : C - 1 - s;
+            if (q == r) {
+#pragma unroll
+                for (int f = 0; f < NF; f++) Fin[f] = F[f];
+                if (r != 0) break;
+            }
+            const double *M = cl.map_shared_rank(L.cmap, q) + (long long)n * RB_LMAP;
+            apply_map<R, NF>(M, F);
+        }
+        if (r == 0)
+#pragma unroll
+            for (int f = 0; f < NF; f++) L.fx[(long long)n * RB_SCAN_NF + f] = (double)F[f];
+        if (nl > 0)  // incoming flux of each chunk
+            for (int c2 = 0; c2 < chunks; c2++) {
+                const int tid = dl * chunks + c2;
+                R Fn[NF];
+#pragma unroll
+                for (int f = 0; f < NF; f++) {
+                    gs.chF[tid][f] = (double)Fin[f];
+                    R s = (R)gs.chb[tid][f];
+#pragma unroll
+                    for (int g = 0; g < NF; g++) s += (R)gs.chA[tid][f + NF * g] * Fin[g];
+                    Fn[f] = s;
+                }
+#pragma unroll
+                for (int f = 0; f < NF; f++) Fin[f] = Fn[f];
+            }
+    }
+    __syncthreads();
+    // 4. re-sweep each chunk from its incoming flux; ψ becomes the angular flux
+    if (active) {
+        Cell1D<R, NM, NF, NE, CSD, PS> cell(P, gs, n, phiE_in, phiE_out, L.ldp, cb, L.mat, L.dx, L.scsd);
+        R F[NF];
+#pragma unroll
+        for (int f = 0; f < NF; f++) F[f] = (R)gs.chF[threadIdx.x][f];
+        for (int k = kb; k < ke; k++) cell.step(fwd ? cb + k : ce - 1 - k, psi, F);
+    }
+    // 5. CTA 0: outgoing boundary moments, side 1 (X+) collects μ ≥ 0, side 0 (X-) μ < 0
+    if (r == 0) {
+        __syncthreads();
+        const int nps = P.npsurf;
+        const long long nb = P.nb[0];
+        for (long long o = threadIdx.x; o < nb; o += blockDim.x) {
+            const int p = (int)(o % nps);
+            const int is = (int)((o / nps) % NF);
+            const int side = (int)(o / ((long long)nps * NF));
+            double s = 0.0;
+            for (int m = 0; m < nd; m++) {
+                const bool fw = P.cosv[m] >= 0.0;
+                if ((side == 1) == fw) s += P.frow_d[(long long)nps * m + p] * L.fx[(long long)m * RB_SCAN_NF + is];
+            }
+            const long long k = P.off_b[0] + o;
+            zout[k] = matvec ? zin[k] - s : s;
+        }
+    }
+    __syncthreads();
+}
+
+template <typename R, typename PS>
+__device__ bool sweep1d_local_fixed(ClusterTeam &t, const DevProblem &P, GroupShared &gs, Local1D &L,
+                                    const double *zin, double *zout, int matvec, int np_source, const double *pE,
+                                    double *phiE_out, int ig) {
+    const int nm = P.nm5, nf = P.nmf[0], ne = P.nm4;
+#define RB_LOCAL(NM_, NF_, NE_, CSD_) \
+    sweep1d_local<R, NM_, NF_, NE_, CSD_, PS>(t, P, gs, L, zin, zout, matvec, np_source, pE, phiE_out, ig)
+    if (!P.csd) {
+        if (nm == 1 && nf == 1) { RB_LOCAL(1, 1, 1, false); return true; }
+        if (nm == 2 && nf == 1) { RB_LOCAL(2, 1, 1, false); return true; }
+        if (nm == 3 && nf == 1) { RB_LOCAL(3, 1, 1, false); return true; }
+    } else {
+        if (nm == 1 && nf == 1 && ne == 1) { RB_LOCAL(1, 1, 1, true); return true; }
+        if (nm == 2 && nf == 1 && ne == 2) { RB_LOCAL(2, 1, 2, true); return true; }
+        if (nm == 2 && nf == 2 && ne == 1) { RB_LOCAL(2, 2, 1, true); return true; }
+        if (nm == 4 && nf == 2 && ne == 2) { RB_LOCAL(4, 2, 2, true); return true; }
+    }
+#undef RB_LOCAL
+    return false;
+}
+
+// One pass T(z) = A·z + c (matvec: z − A·z) of a 1D problem whose local region fits. T is the
+// arithmetic type of the products and the sweep, PS the storage type of ψ.
+template <typename T, typename PS>
+__device__ void pass1d_local_t(ClusterTeam &t, const DevProblem &P, GroupShared &gs, Local1D &L, const double *zin,
+                               double *zout, int homog, int matvec, int ig, const double *phiE_in,
+                               double *phiE_out) {
+    const int nd = P.nd, np = P.np, nm = P.nm5;
+    const int nl = L.ce - L.cb;
+    const long long col0 = (long long)nm * L.cb, ncl = (long long)nm * (nl > 0 ? nl : 0);
+    PS *psi = reinterpret_cast<PS *>(L.psi);
+    const long long ldp = L.ldp;
+    CtaTeam ct;
+    // M2D: ψ[n, col] = Mn·Qlout + Mn·(ys∘𝚽) + T·(Mn·ℳ)·𝚽 for the local columns
+    if (ncl > 0) {
+        const int *mat = L.mat;
+        const double *ys = L.kmat;
+        const double *add = homog ? nullptr : P.qnout;
+        ProductArgs<double> a{P.mn, P.mnfp, nd, nd, np, zin + (long long)np * col0, np, ncl};
+        auto sc = [=, &gs] __device__(int k, long long lc) {
+            const int m = mat[lc / nm];
+            return k < np ? ys[(long long)m * np + k] : gs.tg[m];
+        };
+        auto pre = [=] __device__(int i, long long lc) { return add ? add[(col0 + lc) * nd + i] : 0.0; };
+        team_product<T>(ct, gs, a, sc, pre, [=] __device__(int i, long long lc, double v, double ad) {
+            psi[i + ldp * lc] = (PS)(ad + v);
+        });
+    }
+    const int np_source = homog ? 0 : P.np_source;
+    const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
+    sweep1d_local_fixed<T, PS>(t, P, gs, L, zin, zout, matvec, np_source, pE, phiE_out, ig);
+    // D2M: 𝚽[p, col] = Σ_n Dn[p,n]·ψ[n, col], direction order kept per output
+    if (ncl > 0) {
+        ProductArgs<PS> a{P.dn, nullptr, np, np, nd, psi, (int)ldp, ncl};
+        auto one = [] __device__(int, long long) { return 1.0; };
+        auto pre = [=] __device__(int i, long long lc) { return matvec ? zin[(col0 + lc) * np + i] : 0.0; };
+        team_product<T>(ct, gs, a, one, pre, [=] __device__(int i, long long lc, double v, double z) {
+            zout[(col0 + lc) * np + i] = matvec ? z - v : v;
+        });
+    }
+    t.sync();
+}
+
+__device__ __forceinline__ void pass1d_local(ClusterTeam &t, const DevProblem &P, GroupShared &gs, void *base,
+                                             const double *zin, double *zout, int homog, int matvec, int ig,
+                                             const double *phiE_in, double *phiE_out, int mixed) {
+    Local1D L(P, t.crank, t.ncta, base);
+    if (mixed) pass1d_local_t<float, float>(t, P, gs, L, zin, zout, homog, matvec, ig, phiE_in, phiE_out);
+    else pass1d_local_t<double, double>(t, P, gs, L, zin, zout, homog, matvec, ig, phiE_in, phiE_out);
+}
+
+}  // namespace rb

@@ -11,6 +11,7 @@
 #include <math_constants.h>
 
 #include "rb_kernels.cuh"
+#include "rb_local1d.cuh"
 #include "rb_sweep_md.cuh"
 
 namespace rb {
@@ -36,8 +37,10 @@ struct Solver {
     const double *phiE_in;
     double *phiE_out;
     long long npass;
+    void *local = nullptr;  // shared-memory region of the local 1D pass
+    int local_ok = 0;       // this problem takes the local 1D pass
 
-    __device__ double *vec(int k) const { return P.vecs + (long long)k * P.nstate; }
+    __device__ double *vec(int k) const { return P.vecs + (long long)k * P.vstride; }
 
     // load_and_pass! (sn_one_speed.jl:138-143): out <- T(zin)
     // The mixed form runs every pass with FP32 angular arithmetic except the reconstruction
@@ -45,9 +48,15 @@ struct Solver {
     // the energy-face flux carried into the next group (the outer defect-correction update).
     __device__ void pass(const double *zin, double *out, int homog, int mv, int final = 0) {
         const int mixed = (P.precision == 1 && !final) ? 1 : 0;
+        npass++;
+        if constexpr (std::is_same<Team, ClusterTeam>::value) {
+            if (local_ok) {
+                pass1d_local(t, P, gs, local, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
+                return;
+            }
+        }
         if (P.ndims == 1) pass1d(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
         else pass_md(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out);
-        npass++;
     }
     __device__ void fixedpoint(double *out, const double *zin) { pass(zin, out, 0, 0); }
     // matvec! (sn_one_speed.jl:147): out <- zin − A·zin
@@ -189,10 +198,10 @@ struct Solver {
 
     // ---------------------------------------------------------------- gmres(m)
     __device__ SolveStat gmres(double *z, const double *rhs, int restart, int maxit, double tol) {
-        const long long N = P.nstate;
+        const long long N = P.nstate, N2 = P.vstride / 2;  // elements, pairs
         const int m = restart > 1 ? restart : 1;
         SolveStat st = {0, 0.0, 1, CUDART_NAN};
-        const double bnorm = norm(rhs);
+        const double bnorm = sqrt(vdot2(t, rhs, rhs, N2));
         if (bnorm == 0.0) { vzero(t, z, N); return st; }
         double *r = vec(2), *w = vec(3);
         double *H = gs.H;
@@ -202,10 +211,18 @@ struct Solver {
         while (iter < maxit && !conv) {
             matvec(r, z); iter++;
             double v1[1] = {0.0};
-            for (long long i = t.rank(); i < N; i += t.size()) {  // r = c − M z
-                const double ri = rhs[i] - r[i];
-                r[i] = ri;
-                v1[0] += ri * ri;
+            {  // r = c − M z
+                double2 xc[RB_VU2], xr[RB_VU2];
+                const double2 *c2 = RB_CD2(rhs);
+                double2 *r2 = RB_D2(r);
+                RB_VPAIRS(t, N2, { xc[u_] = c2[q]; xr[u_] = r2[q]; }, {
+                    double2 ri;
+                    ri.x = xc[u_].x - xr[u_].x;
+                    ri.y = xc[u_].y - xr[u_].y;
+                    r2[q] = ri;
+                    v1[0] += ri.x * ri.x;
+                    v1[0] += ri.y * ri.y;
+                })
             }
             t.template sumk<1>(v1);
             const double beta = sqrt(v1[0]);
@@ -214,8 +231,10 @@ struct Solver {
             if (resid < tol) { conv = 1; break; }
             {
                 const double inv = 1.0 / beta;
-                double *V0 = vec(4);
-                for (long long i = t.rank(); i < N; i += t.size()) V0[i] = r[i] * inv;
+                double2 *V02 = RB_D2(vec(4));
+                const double2 *r2 = RB_CD2(r);
+                double2 xr[RB_VU2];
+                RB_VPAIRS(t, N2, { xr[u_] = r2[q]; }, { V02[q] = make_double2(xr[u_].x * inv, xr[u_].y * inv); })
             }
             if (t.leader()) {
                 for (int i = 0; i <= m; i++) gs.g[i] = 0.0;
@@ -228,19 +247,32 @@ struct Solver {
                 matvec(w, vec(4 + j)); iter++;
                 // modified Gram-Schmidt, one sweep per basis vector: w ← w − h_i V_i fused with
                 // the dot product of the updated w against V_{i+1} (or against itself at the end)
-                double h = vdot(t, w, vec(4), N);
+                double h = vdot2(t, w, vec(4), N2);
+                double2 *w2 = RB_D2(w);
                 for (int i = 0; i <= j; i++) {
                     if (t.leader()) HH(i, j) = h;
-                    const double *Vi = vec(4 + i);
-                    const double *Vn = (i < j) ? vec(4 + i + 1) : nullptr;
+                    const double2 *Vi2 = RB_CD2(vec(4 + i));
+                    const double2 *Vn2 = (i < j) ? RB_CD2(vec(4 + i + 1)) : nullptr;
                     double acc[1] = {0.0};
-                    double xw[4], xv[4], xn[4];
-                    if (Vn) {
-                        RB_VLOOP4(t, N, { xw[u_] = w[q]; xv[u_] = Vi[q]; xn[u_] = Vn[q]; },
-                                  { const double wq = xw[u_] + (-h) * xv[u_]; w[q] = wq; acc[0] += wq * xn[u_]; })
+                    double2 xw[RB_VU2], xv[RB_VU2], xn[RB_VU2];
+                    if (Vn2) {
+                        RB_VPAIRS(t, N2, { xw[u_] = w2[q]; xv[u_] = Vi2[q]; xn[u_] = Vn2[q]; }, {
+                            double2 wq;
+                            wq.x = xw[u_].x + (-h) * xv[u_].x;
+                            wq.y = xw[u_].y + (-h) * xv[u_].y;
+                            w2[q] = wq;
+                            acc[0] += wq.x * xn[u_].x;
+                            acc[0] += wq.y * xn[u_].y;
+                        })
                     } else {
-                        RB_VLOOP4(t, N, { xw[u_] = w[q]; xv[u_] = Vi[q]; },
-                                  { const double wq = xw[u_] + (-h) * xv[u_]; w[q] = wq; acc[0] += wq * wq; })
+                        RB_VPAIRS(t, N2, { xw[u_] = w2[q]; xv[u_] = Vi2[q]; }, {
+                            double2 wq;
+                            wq.x = xw[u_].x + (-h) * xv[u_].x;
+                            wq.y = xw[u_].y + (-h) * xv[u_].y;
+                            w2[q] = wq;
+                            acc[0] += wq.x * wq.x;
+                            acc[0] += wq.y * wq.y;
+                        })
                     }
                     t.template sumk<1>(acc);
                     h = acc[0];
@@ -248,8 +280,9 @@ struct Solver {
                 const double hjp1 = sqrt(h);
                 if (hjp1 > 0.0) {
                     const double inv = 1.0 / hjp1;
-                    double *Vn = vec(4 + j + 1);
-                    for (long long q = t.rank(); q < N; q += t.size()) Vn[q] = w[q] * inv;
+                    double2 *Vn2 = RB_D2(vec(4 + j + 1));
+                    double2 xw[RB_VU2];
+                    RB_VPAIRS(t, N2, { xw[u_] = w2[q]; }, { Vn2[q] = make_double2(xw[u_].x * inv, xw[u_].y * inv); })
                 }
                 if (t.leader()) {
                     HH(j + 1, j) = hjp1;
@@ -282,11 +315,16 @@ struct Solver {
             __syncthreads();
             // z += Σ y_i V_i, in basis order per element
             {
-                double xz[4];
-                RB_VLOOP4(t, N, { xz[u_] = z[q]; }, {
-                    double zq = xz[u_];
-                    for (int i = 0; i < k; i++) zq += gs.y[i] * vec(4 + i)[q];
-                    z[q] = zq;
+                double2 xz[RB_VU2];
+                double2 *z2 = RB_D2(z);
+                RB_VPAIRS(t, N2, { xz[u_] = z2[q]; }, {
+                    double2 zq = xz[u_];
+                    for (int i = 0; i < k; i++) {
+                        const double2 v = RB_CD2(vec(4 + i))[q];
+                        zq.x += gs.y[i] * v.x;
+                        zq.y += gs.y[i] * v.y;
+                    }
+                    z2[q] = zq;
                 })
             }
             t.sync();
@@ -306,10 +344,13 @@ struct Solver {
         double *r = vec(2), *rh = vec(3), *p = vec(4), *v = vec(5), *s = vec(6), *tt = vec(7);
         matvec(r, z);
         double a1[1] = {0.0};
-        for (long long i = t.rank(); i < N; i += t.size()) {
-            const double ri = rhs[i] - r[i];
-            r[i] = ri; rh[i] = ri; p[i] = 0.0; v[i] = 0.0;
-            a1[0] += ri * ri;
+        {
+            double xc[RB_VU], xr[RB_VU];
+            RB_VLOOP(t, N, { xc[u_] = rhs[q]; xr[u_] = r[q]; }, {
+                const double ri = xc[u_] - xr[u_];
+                r[q] = ri; rh[q] = ri; p[q] = 0.0; v[q] = 0.0;
+                a1[0] += ri * ri;
+            })
         }
         t.template sumk<1>(a1);
         int iter = 1, conv = 0;
@@ -321,17 +362,24 @@ struct Solver {
             const double rho_new = vdot(t, rh, r, N);
             if (fabs(rho_new) < tiny) break;
             const double beta = (rho_new / rho_old) * (alpha / omega);
-            for (long long i = t.rank(); i < N; i += t.size()) p[i] = r[i] + 1.0 * (beta * (p[i] + (-omega) * v[i]));
+            {
+                double xr[RB_VU], xp[RB_VU], xv[RB_VU];
+                RB_VLOOP(t, N, { xr[u_] = r[q]; xp[u_] = p[q]; xv[u_] = v[q]; },
+                         { p[q] = xr[u_] + 1.0 * (beta * (xp[u_] + (-omega) * xv[u_])); })
+            }
             t.sync();
             matvec(v, p); iter++;
             const double denom = vdot(t, rh, v, N);
             if (fabs(denom) < tiny) break;
             alpha = rho_new / denom;
             double a2[1] = {0.0};
-            for (long long i = t.rank(); i < N; i += t.size()) {
-                const double si = r[i] + (-alpha) * v[i];
-                s[i] = si;
-                a2[0] += si * si;
+            {
+                double xr[RB_VU], xv[RB_VU];
+                RB_VLOOP(t, N, { xr[u_] = r[q]; xv[u_] = v[q]; }, {
+                    const double si = xr[u_] + (-alpha) * xv[u_];
+                    s[q] = si;
+                    a2[0] += si * si;
+                })
             }
             t.template sumk<1>(a2);
             const double sn_ = sqrt(a2[0]);
@@ -343,16 +391,25 @@ struct Solver {
             }
             matvec(tt, s); iter++;
             double a3[2] = {0.0, 0.0};
-            for (long long i = t.rank(); i < N; i += t.size()) { a3[0] += tt[i] * tt[i]; a3[1] += tt[i] * s[i]; }
+            {
+                double xt[RB_VU], xs[RB_VU];
+                RB_VLOOP(t, N, { xt[u_] = tt[q]; xs[u_] = s[q]; }, {
+                    a3[0] += xt[u_] * xt[u_];
+                    a3[1] += xt[u_] * xs[u_];
+                })
+            }
             t.template sumk<2>(a3);
             if (a3[0] < tiny) break;
             omega = a3[1] / a3[0];
             double a4[1] = {0.0};
-            for (long long i = t.rank(); i < N; i += t.size()) {
-                z[i] = (z[i] + alpha * p[i]) + omega * s[i];
-                const double ri = s[i] + (-omega) * tt[i];
-                r[i] = ri;
-                a4[0] += ri * ri;
+            {
+                double xz[RB_VU], xp[RB_VU], xs[RB_VU], xt[RB_VU];
+                RB_VLOOP(t, N, { xz[u_] = z[q]; xp[u_] = p[q]; xs[u_] = s[q]; xt[u_] = tt[q]; }, {
+                    z[q] = (xz[u_] + alpha * xp[u_]) + omega * xs[u_];
+                    const double ri = xs[u_] + (-omega) * xt[u_];
+                    r[q] = ri;
+                    a4[0] += ri * ri;
+                })
             }
             t.template sumk<1>(a4);
             resid = sqrt(a4[0]) / bnorm;
@@ -411,13 +468,19 @@ struct Solver {
 // the group loop of compute_flux(::SN) for one problem (sn_flux.jl:146-224)
 // ------------------------------------------------------------------------------------------
 template <class Team>
-__device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs) {
+__device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, void *local = nullptr,
+                              long long local_bytes = 0) {
+    const int local_ok = (local && local1d_ok(P, (int)t.ncta, local_bytes)) ? 1 : 0;
     const int ng = P.ng, nmat = P.nmat, np = P.np, nd = P.nd, nm = P.nm5;
     const long long nphi = P.nphi, ncell = P.ncell;
     const long long nE = (long long)nd * P.nm4 * ncell;
     const int st_ = P.solver_type;
     double *phiE_in = P.phiE_a, *phiE_out = P.phiE_b;
+    // the pad element of each Krylov vector (odd nstate) starts and stays zero
+    if (P.vstride > P.nstate)
+        for (int k = t.rank(); k < P.nvec; k += t.size()) P.vecs[(long long)k * P.vstride + P.nstate] = 0.0;
     if (P.csd) { vzero(t, phiE_in, nE); vzero(t, phiE_out, nE); }
+    t.sync();
     long long npass = 0;
     for (int ig = 0; ig < ng; ig++) {
         // per-group constants, one copy per CTA
@@ -471,11 +534,17 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs) {
             for (long long i = t.rank(); i < nE; i += t.size()) phiE_in[i] = phiE_in[i] * r1 / r0;
         }
         t.sync();
+        if (local_ok) {
+            Local1D L(P, t.crank, t.ncta, local);
+            local1d_group_setup(P, L);
+        }
         // Mn·Qlout into ψ, then kept as Qnout for the passes of this group
         m2d_tiles(t, P, gs, P.qlout, nullptr, 0);
         t.sync();
         vcopy(t, P.qnout, P.psi, (long long)nd * nm * ncell);
         Solver<Team> S{t, P, gs, ig, phiE_in, phiE_out, 0};
+        S.local = local;
+        S.local_ok = local_ok;
         SolveStat s = S.one_speed(P.flux + (long long)ig * nphi);
         npass += S.npass;
         if (t.rank() == 0) {
@@ -505,10 +574,12 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs) {
 // ------------------------------------------------------------------------------------------
 // persistent batch kernel: clusters pull problems from a device work queue
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(RB_THREADS, 2) solve_batch_kernel(DevProblem *const *probs, int nprob,
-                                                                 int *queue) {
+// Dynamic shared memory: GroupShared, then `local_bytes` for the local 1D pass.
+__global__ void __launch_bounds__(RB_THREADS, 1) solve_batch_kernel(DevProblem *const *probs, int nprob,
+                                                                 int *queue, int local_bytes) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
+    void *local = local_bytes > 0 ? (void *)(smem_raw + sizeof(GroupShared)) : nullptr;
     ClusterTeam t;
     t.init(&gs.team);
     while (true) {
@@ -516,7 +587,7 @@ __global__ void __launch_bounds__(RB_THREADS, 2) solve_batch_kernel(DevProblem *
         if (t.crank == 0 && threadIdx.x == 0) idx = atomicAdd(queue, 1);
         idx = t.broadcast_from_leader(idx);
         if (idx >= nprob) break;
-        solve_problem(t, *probs[idx], gs);
+        solve_problem(t, *probs[idx], gs, local, local_bytes);
     }
 }
 

@@ -4,9 +4,10 @@
 // spread over all threads of the cluster; team barriers are hardware cluster barriers.
 // Reductions are deterministic and give the same bits in every thread of every CTA: each warp
 // reduces by xor butterfly (commutative pairs, identical in all lanes), each CTA sums its warps
-// in a fixed order into a shared slot, and after one cluster barrier every thread adds the CTAs'
-// slots in rank order through distributed shared memory. Slots alternate between two buffers,
-// so a reduction costs one cluster barrier. All threads run the same control flow, which the
+// in a fixed order and stores that partial into its own slot in every CTA of the cluster
+// (distributed shared memory), and after one cluster barrier every thread adds the slots in
+// rank order from its own shared memory. Slot sets alternate between two buffers, so a
+// reduction costs one cluster barrier. All threads run the same control flow, which the
 // identical reduction bits guarantee, so no CTA can leave a barrier sequence early.
 #pragma once
 #include <cooperative_groups.h>
@@ -16,7 +17,7 @@ namespace rb {
 namespace cg = cooperative_groups;
 
 struct TeamShared {
-    double part[2][4];  // per-CTA partial sums, double-buffered, up to 4 values per reduction
+    double part[2][16][4];  // partial sums of each CTA, double-buffered, up to 4 values per reduction
     double warp[32][4];
     int idx;            // problem index broadcast by the cluster leader
 };
@@ -52,23 +53,24 @@ struct ClusterTeam {
         __syncthreads();
         const int slot = phase & 1;
         phase++;
-        if (threadIdx.x == 0) {
+        cg::cluster_group cl = cg::this_cluster();
+        if (threadIdx.x < ncta) {  // thread q stores this CTA's partial into CTA q
+            double s[K];
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                double s = 0.0;
-                for (int i = 0; i < nw; i++) s += sh->warp[i][k];
-                sh->part[slot][k] = s;
+                s[k] = 0.0;
+                for (int i = 0; i < nw; i++) s[k] += sh->warp[i][k];
             }
+            double *dst = cl.map_shared_rank(&sh->part[slot][crank][0], threadIdx.x);
+#pragma unroll
+            for (int k = 0; k < K; k++) dst[k] = s[k];
         }
-        cg::cluster_group cl = cg::this_cluster();
         cl.sync();
 #pragma unroll
         for (int k = 0; k < K; k++) v[k] = 0.0;
-        for (unsigned r = 0; r < ncta; r++) {
-            const double *p = cl.map_shared_rank(&sh->part[slot][0], r);
+        for (unsigned r = 0; r < ncta; r++)
 #pragma unroll
-            for (int k = 0; k < K; k++) v[k] += p[k];
-        }
+            for (int k = 0; k < K; k++) v[k] += sh->part[slot][r][k];
     }
     __device__ double sum(double v) {
         double a[1] = {v};
@@ -137,12 +139,12 @@ struct GridTeam {
             for (int k = 0; k < K; k++) {
                 double s = 0.0;
                 for (unsigned r = 0; r < ncta; r++) s += gpart[((long long)slot * ncta + r) * 4 + k];
-                sh->part[slot][k] = s;
+                sh->part[slot][0][k] = s;
             }
         }
         __syncthreads();
 #pragma unroll
-        for (int k = 0; k < K; k++) v[k] = sh->part[slot][k];
+        for (int k = 0; k < K; k++) v[k] = sh->part[slot][0][k];
     }
     __device__ double sum(double v) {
         double a[1] = {v};
