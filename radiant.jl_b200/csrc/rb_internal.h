@@ -11,6 +11,11 @@
 #define RB_MAXORD 8   // largest closure order per axis
 #define RB_MAXMAT 64  // materials per problem held in shared memory
 
+// mixed form: in-group tolerance floor of a solve with the FP32 operator (its noise floor is near
+// 1e-7), and the tolerance of the first Krylov solve before the FP64 defect correction
+#define RB_MIXED_TOL 1e-7
+#define RB_MIXED_TOL1 1e-5
+
 // status bits written by the device into DevProblem::status
 #define RB_DEV_OK 0
 #define RB_DEV_NOT_CONVERGED 1   // informational: some group hit max_iter (reference prints only)

@@ -37,13 +37,22 @@ __host__ __device__ __forceinline__ bool local1d_shape(const DevProblem &P) {
            (nm == 4 && nf == 2 && ne == 2);
 }
 
+// Krylov-vector slice of a CTA: the moments of its cells, and in the last CTA the boundary
+// in-moments too; its largest length over the cluster
+__host__ __device__ __forceinline__ long long local1d_slice(const DevProblem &P, int ncta) {
+    const long long lc = (P.nx + ncta - 1) / ncta;
+    return (long long)P.np * P.nm5 * lc + (P.nstate - P.nphi);
+}
+
 // bytes of the local region a problem needs on a cluster of `ncta` CTAs: face maps, exit
 // fluxes, the group's in-group Σs per material and moment, the CSD cell blocks per material,
-// the width and material of each owned cell, then ψ of the owned cells
+// the width and material of each owned cell, then ψ of the owned cells (which the
+// Gram-Schmidt loop reuses for the basis vector in use) and the slice of w
 __host__ __device__ __forceinline__ long long local1d_bytes(const DevProblem &P, int ncta) {
     const long long lc = (P.nx + ncta - 1) / ncta, nd = P.nd, nm = P.nm5;
+    const long long psi = (nd + 1) * nm * lc, sl = local1d_slice(P, ncta);
     return nd * (RB_LMAP + RB_SCAN_NF) * 8 + (long long)P.nmat * P.np * 8 + (long long)P.nmat * nm * nm * 8 +
-           lc * 8 + ((lc * 4 + 15) & ~15LL) + (nd + 1) * nm * lc * 8;
+           lc * 8 + ((lc * 4 + 15) & ~15LL) + (psi > sl ? psi : sl) * 8 + sl * 8;
 }
 
 // whether a problem takes the local pass on a cluster of `ncta` CTAs with `local_bytes` of
@@ -59,9 +68,13 @@ struct Local1D {
     double *scsd;   // [nmat][nm·nm] CSD block of the cell matrix (this group)
     double *dx;     // [lc] widths of the owned cells
     int *mat;       // [lc] materials of the owned cells
-    void *psi;      // [ncl][ldp] ψ of the local columns (double or float)
+    void *psi;      // [ncl][ldp] ψ of the local columns (double or float); in the Gram-Schmidt
+                    // loop, the slice of the basis vector in use
+    double *ws;     // the slice of w in the Gram-Schmidt loop
     long long ldp;  // leading dimension of ψ (nd + 1: odd, so column accesses spread over banks)
     int cb, ce;     // owned cells [cb, ce)
+    long long e0, eb;  // slice element j < l1 is state element e0 + j, the rest eb + (j − l1)
+    int l1, ls;        // length of the cell part and of the whole slice
 
     __device__ Local1D(const DevProblem &P, unsigned crank, unsigned ncta, void *base) {
         const int lc = (P.nx + (int)ncta - 1) / (int)ncta;
@@ -75,8 +88,36 @@ struct Local1D {
         mat = reinterpret_cast<int *>(dx + lc);
         psi = reinterpret_cast<unsigned char *>(mat) + ((lc * 4 + 15) & ~15);
         ldp = P.nd + 1;
+        const long long np_ = (long long)(P.nd + 1) * P.nm5 * lc, sl = local1d_slice(P, (int)ncta);
+        ws = reinterpret_cast<double *>(psi) + (np_ > sl ? np_ : sl);
+        e0 = (long long)P.np * P.nm5 * cb;
+        eb = P.nphi;
+        l1 = (int)((long long)P.np * P.nm5 * (ce - cb));
+        ls = l1 + (crank + 1 == ncta ? (int)(P.nstate - P.nphi) : 0);
     }
 };
+
+// Loop over the CTA's slice of a Krylov vector: element j of the slice is state element g,
+// RB_VU elements per thread in flight.
+#define RB_SLICE_LOOP(L, LOAD, USE)                                                         \
+    {                                                                                      \
+        const int l1_ = (L).l1, ls_ = (L).ls;                                              \
+        const long long e0_ = (L).e0, eb_ = (L).eb;                                        \
+        for (int j0_ = threadIdx.x; j0_ < ls_; j0_ += RB_VU * blockDim.x) {               \
+            _Pragma("unroll") for (int u_ = 0; u_ < RB_VU; u_++) {                         \
+                const int j = j0_ + u_ * blockDim.x;                                       \
+                const long long g = j < l1_ ? e0_ + j : eb_ + (j - l1_);                   \
+                if (j < ls_) { LOAD }                                                      \
+                (void)g;                                                                   \
+            }                                                                              \
+            _Pragma("unroll") for (int u_ = 0; u_ < RB_VU; u_++) {                         \
+                const int j = j0_ + u_ * blockDim.x;                                       \
+                const long long g = j < l1_ ? e0_ + j : eb_ + (j - l1_);                   \
+                if (j < ls_) { USE }                                                       \
+                (void)g;                                                                   \
+            }                                                                              \
+        }                                                                                  \
+    }
 
 // per-group copy of the tables the local pass reads per cell (after the group's constants are set)
 __device__ __forceinline__ void local1d_group_setup(const DevProblem &P, Local1D &L) {

@@ -43,9 +43,10 @@ struct Solver {
     __device__ double *vec(int k) const { return P.vecs + (long long)k * P.vstride; }
 
     // load_and_pass! (sn_one_speed.jl:138-143): out <- T(zin)
-    // The mixed form runs every pass with FP32 angular arithmetic except the reconstruction
-    // pass of each group (final = 1), which is FP64: it produces the returned flux moments and
-    // the energy-face flux carried into the next group (the outer defect-correction update).
+    // The mixed form runs every pass with FP32 angular arithmetic except two per group
+    // (final = 1), which are FP64: the Krylov right-hand side c = T(0) and the reconstruction
+    // pass, which produces the returned flux moments and the energy-face flux carried into the
+    // next group (the outer defect-correction update).
     __device__ void pass(const double *zin, double *out, int homog, int mv, int final = 0) {
         const int mixed = (P.precision == 1 && !final) ? 1 : 0;
         npass++;
@@ -196,6 +197,61 @@ struct Solver {
         return s;
     }
 
+    // Modified Gram-Schmidt of w against V_0..V_j for a problem on the local 1D pass: each CTA
+    // keeps its slice of w, and of the basis vector in use, in shared memory, so a step reads
+    // only the next basis vector from memory. Same steps and fused dot products as the
+    // team-wide loop in gmres; writes H[0..j, j] and V_{j+1}, returns false when not local.
+    __device__ bool mgs_local(const double *w, int jb, int m, double &hjp1) {
+        if constexpr (std::is_same<Team, ClusterTeam>::value) {
+            if (!local_ok) return false;
+            Local1D L(P, t.crank, t.ncta, local);
+            double *ws = L.ws, *vs = reinterpret_cast<double *>(L.psi);
+            double *H = gs.H;
+            {
+                const double *V0 = vec(4);
+                double acc[1] = {0.0};
+                double xw[RB_VU], xv[RB_VU];
+                RB_SLICE_LOOP(L, { xw[u_] = w[g]; xv[u_] = V0[g]; }, {
+                    ws[j] = xw[u_];
+                    vs[j] = xv[u_];
+                    acc[0] += xw[u_] * xv[u_];
+                })
+                t.template sumk<1>(acc);
+                double h = acc[0];
+                for (int i = 0; i <= jb; i++) {
+                    if (t.leader()) H[i + (m + 1) * jb] = h;
+                    double a1[1] = {0.0};
+                    if (i < jb) {
+                        const double *Vn = vec(4 + i + 1);
+                        double xn[RB_VU];
+                        RB_SLICE_LOOP(L, { xn[u_] = Vn[g]; }, {
+                            const double wq = ws[j] + (-h) * vs[j];
+                            ws[j] = wq;
+                            vs[j] = xn[u_];
+                            a1[0] += wq * xn[u_];
+                        })
+                    } else {
+                        RB_SLICE_LOOP(L, {}, {
+                            const double wq = ws[j] + (-h) * vs[j];
+                            ws[j] = wq;
+                            a1[0] += wq * wq;
+                        })
+                    }
+                    t.template sumk<1>(a1);
+                    h = a1[0];
+                }
+                hjp1 = sqrt(h);
+                if (hjp1 > 0.0) {
+                    const double inv = 1.0 / hjp1;
+                    double *Vn = vec(4 + jb + 1);
+                    RB_SLICE_LOOP(L, {}, { Vn[g] = ws[j] * inv; })
+                }
+            }
+            return true;
+        }
+        return false;
+    }
+
     // ---------------------------------------------------------------- gmres(m)
     __device__ SolveStat gmres(double *z, const double *rhs, int restart, int maxit, double tol) {
         const long long N = P.nstate, N2 = P.vstride / 2;  // elements, pairs
@@ -245,6 +301,8 @@ struct Solver {
             for (int j = 0; j < m; j++) {
                 if (iter >= maxit) break;
                 matvec(w, vec(4 + j)); iter++;
+                double hjp1;
+                if (!mgs_local(w, j, m, hjp1)) {
                 // modified Gram-Schmidt, one sweep per basis vector: w ← w − h_i V_i fused with
                 // the dot product of the updated w against V_{i+1} (or against itself at the end)
                 double h = vdot2(t, w, vec(4), N2);
@@ -277,12 +335,13 @@ struct Solver {
                     t.template sumk<1>(acc);
                     h = acc[0];
                 }
-                const double hjp1 = sqrt(h);
+                hjp1 = sqrt(h);
                 if (hjp1 > 0.0) {
                     const double inv = 1.0 / hjp1;
                     double2 *Vn2 = RB_D2(vec(4 + j + 1));
                     double2 xw[RB_VU2];
                     RB_VPAIRS(t, N2, { xw[u_] = w2[q]; }, { Vn2[q] = make_double2(xw[u_].x * inv, xw[u_].y * inv); })
+                }
                 }
                 if (t.leader()) {
                     HH(j + 1, j) = hjp1;
@@ -446,15 +505,49 @@ struct Solver {
         double *z = vec(0);
         vzero(t, z, N);  // initial state: 𝚽l of the group = 0, boundary in-moments = 0
         SolveStat st;
+        const bool mixed = P.precision == 1;
         if (P.accel == 0 || P.accel == 1) {
-            st = livolant(z, P.maxit, P.tol, P.accel == 0 ? 0 : 3);
+            st = livolant(z, P.maxit, mixed ? fmax(P.tol, RB_MIXED_TOL) : P.tol, P.accel == 0 ? 0 : 3);
         } else if (P.accel == 2) {
-            st = anderson(z, P.depth, P.maxit, P.tol);
+            st = anderson(z, P.depth, P.maxit, mixed ? fmax(P.tol, RB_MIXED_TOL) : P.tol);
         } else {
             double *rhs = vec(1);
-            fixedpoint(rhs, z);  // c = T(0)
-            if (P.accel == 3) st = gmres(z, rhs, P.restart, P.maxit, P.tol);
-            else st = bicgstab(z, rhs, P.maxit, P.tol);
+            pass(z, rhs, 0, 0, 1);  // c = T(0), FP64 in both forms
+            // The mixed form solves with the FP32 operator to RB_MIXED_TOL1, then takes one outer
+            // defect-correction step: the residual r = c − (I − A)·z with the FP64 operator, the
+            // correction δ from the FP32-operator solve of (I − A)·δ = r to the tolerance that
+            // brings the whole residual to `tol`, z ← z + δ.
+            const double tol1 = mixed ? fmax(P.tol, RB_MIXED_TOL1) : P.tol;
+            if (P.accel == 3) st = gmres(z, rhs, P.restart, P.maxit, tol1);
+            else st = bicgstab(z, rhs, P.maxit, tol1);
+            if (mixed) {
+                double *dz = vec(P.nvec - 2), *res = vec(P.nvec - 1);
+                pass(z, res, 1, 1, 1);  // res = z − A·z, FP64
+                double v[2] = {0.0, 0.0};
+                for (long long i = t.rank(); i < N; i += t.size()) {
+                    const double ri = rhs[i] - res[i];
+                    res[i] = ri;
+                    v[0] += ri * ri;
+                    v[1] += rhs[i] * rhs[i];
+                }
+                t.template sumk<2>(v);
+                const double rel = v[1] > 0.0 ? sqrt(v[0] / v[1]) : 0.0;
+                if (rel >= P.tol) {
+                    vzero(t, dz, N);
+                    const double tol2 = fmax(P.tol / rel, RB_MIXED_TOL);
+                    SolveStat s2;
+                    if (P.accel == 3) s2 = gmres(dz, res, P.restart, P.maxit, tol2);
+                    else s2 = bicgstab(dz, res, P.maxit, tol2);
+                    vaxpy(t, 1.0, dz, z, N);
+                    st.iter += s2.iter + 1;
+                    st.resid = s2.resid * rel;
+                    st.conv = s2.conv;
+                } else {
+                    st.iter += 1;
+                    st.resid = rel;
+                    st.conv = 1;
+                }
+            }
         }
         // reconstruction pass (sn_one_speed.jl:184-187)
         double *out = vec(1);
