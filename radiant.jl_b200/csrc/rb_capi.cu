@@ -481,8 +481,12 @@ int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm,
     cluster = sh.cluster;
     const size_t smem = sh.smem;
     const int local_bytes = (int)sh.local_bytes;
-    CK(cudaFuncSetAttribute(rb::solve_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (cluster > 8) CK(cudaFuncSetAttribute(rb::solve_batch_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    // a batch whose every problem takes the local 1D pass runs on the kernel carrying only it
+    bool all_local = !hs.empty() && local_bytes > 0;
+    for (const DevProblem *h : hs) all_local = all_local && rb::local1d_ok(*h, cluster, local_bytes);
+    void (*kern)(DevProblem *const *, int, int *, int) = all_local ? rb::solve_local1d_kernel : rb::solve_batch_kernel;
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (cluster > 8) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -496,11 +500,11 @@ int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm,
     cfg.numAttrs = 1;
     int max_clusters = 0;
     cfg.gridDim = dim3(cluster * (nsm / cluster > 0 ? nsm / cluster : 1), 1, 1);
-    CK(cudaOccupancyMaxActiveClusters(&max_clusters, rb::solve_batch_kernel, &cfg));
+    CK(cudaOccupancyMaxActiveClusters(&max_clusters, kern, &cfg));
     if (max_clusters < 1) return fail(ctx, RB_ERR_CUDA, "no cluster of %d CTAs fits on the device", cluster);
     int nclusters = max_clusters < n ? max_clusters : n;
     cfg.gridDim = dim3(cluster * nclusters, 1, 1);
-    CK(cudaLaunchKernelEx(&cfg, rb::solve_batch_kernel, (DevProblem *const *)list, n, queue, local_bytes));
+    CK(cudaLaunchKernelEx(&cfg, kern, (DevProblem *const *)list, n, queue, local_bytes));
     return RB_OK;
 }
 

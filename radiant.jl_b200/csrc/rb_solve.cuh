@@ -28,7 +28,8 @@ __device__ __forceinline__ double rho_estimate(double r0, double r, int it) {  /
     return CUDART_NAN;
 }
 
-template <class Team>
+// LO: the team runs only 1D problems on the local pass (the kernel that carries no other pass)
+template <class Team, bool LO = false>
 struct Solver {
     Team &t;
     const DevProblem &P;
@@ -51,13 +52,15 @@ struct Solver {
         const int mixed = (P.precision == 1 && !final) ? 1 : 0;
         npass++;
         if constexpr (std::is_same<Team, ClusterTeam>::value) {
-            if (local_ok) {
+            if (LO || local_ok) {
                 pass1d_local(t, P, gs, local, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
                 return;
             }
         }
-        if (P.ndims == 1) pass1d(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
-        else pass_md(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out);
+        if constexpr (!LO) {
+            if (P.ndims == 1) pass1d(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
+            else pass_md(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out);
+        }
     }
     __device__ void fixedpoint(double *out, const double *zin) { pass(zin, out, 0, 0); }
     // matvec! (sn_one_speed.jl:147): out <- zin − A·zin
@@ -560,7 +563,7 @@ struct Solver {
 // ------------------------------------------------------------------------------------------
 // the group loop of compute_flux(::SN) for one problem (sn_flux.jl:146-224)
 // ------------------------------------------------------------------------------------------
-template <class Team>
+template <class Team, bool LO = false>
 __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, void *local = nullptr,
                               long long local_bytes = 0) {
     const int local_ok = (local && local1d_ok(P, (int)t.ncta, local_bytes)) ? 1 : 0;
@@ -635,7 +638,7 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, voi
         m2d_tiles(t, P, gs, P.qlout, nullptr, 0);
         t.sync();
         vcopy(t, P.qnout, P.psi, (long long)nd * nm * ncell);
-        Solver<Team> S{t, P, gs, ig, phiE_in, phiE_out, 0};
+        Solver<Team, LO> S{t, P, gs, ig, phiE_in, phiE_out, 0};
         S.local = local;
         S.local_ok = local_ok;
         SolveStat s = S.one_speed(P.flux + (long long)ig * nphi);
@@ -681,6 +684,24 @@ __global__ void __launch_bounds__(RB_THREADS, 1) solve_batch_kernel(DevProblem *
         idx = t.broadcast_from_leader(idx);
         if (idx >= nprob) break;
         solve_problem(t, *probs[idx], gs, local, local_bytes);
+    }
+}
+
+// The same persistent loop for batches whose every problem takes the local 1D pass: the kernel
+// carries no other pass, so its registers go to that path alone.
+__global__ void __launch_bounds__(RB_THREADS, 1) solve_local1d_kernel(DevProblem *const *probs, int nprob,
+                                                                   int *queue, int local_bytes) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
+    void *local = (void *)(smem_raw + sizeof(GroupShared));
+    ClusterTeam t;
+    t.init(&gs.team);
+    while (true) {
+        int idx = 0;
+        if (t.crank == 0 && threadIdx.x == 0) idx = atomicAdd(queue, 1);
+        idx = t.broadcast_from_leader(idx);
+        if (idx >= nprob) break;
+        solve_problem<ClusterTeam, true>(t, *probs[idx], gs, local, local_bytes);
     }
 }
 
