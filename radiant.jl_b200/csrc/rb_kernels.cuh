@@ -25,7 +25,7 @@
 #define RB_THREADS 256
 #define RB_SCAN_NF 2      // scan path for face-moment counts up to this (every fixed 1D shape)
 #define RB_MAXCLUSTER 16
-#define RB_TILE_DOUBLES 5120  // largest staging of team_product (16-deep panels, 32x128 tile)
+#define RB_TILE_DOUBLES 2688  // largest staging of team_product (16-deep panels, 32x128 tile, padded)
 
 namespace rb {
 

@@ -23,6 +23,7 @@
 namespace rb {
 
 #define RB_LMAP (RB_SCAN_NF * RB_SCAN_NF + RB_SCAN_NF)  // doubles of one face map
+#define RB_LKEYS 2  // distinct (material, width) cell kinds per CTA with factored cell operators
 
 // a CTA-local team: team_product over this CTA's columns only
 struct CtaTeam {
@@ -48,11 +49,16 @@ __host__ __device__ __forceinline__ long long local1d_slice(const DevProblem &P,
 // fluxes, the group's in-group Σs per material and moment, the CSD cell blocks per material,
 // the width and material of each owned cell, then ψ of the owned cells (which the
 // Gram-Schmidt loop reuses for the basis vector in use) and the slice of w
+__host__ __device__ __forceinline__ int local1d_kent(const DevProblem &P) {  // doubles per cell operator
+    const int nm = P.nm5, nf = P.nmf[0];
+    return nm * nm + nm * nf + nf * nf;
+}
 __host__ __device__ __forceinline__ long long local1d_bytes(const DevProblem &P, int ncta) {
     const long long lc = (P.nx + ncta - 1) / ncta, nd = P.nd, nm = P.nm5;
     const long long psi = (nd + 1) * nm * lc, sl = local1d_slice(P, ncta);
-    return nd * (RB_LMAP + RB_SCAN_NF) * 8 + (long long)P.nmat * P.np * 8 + (long long)P.nmat * nm * nm * 8 +
-           lc * 8 + ((lc * 4 + 15) & ~15LL) + (psi > sl ? psi : sl) * 8 + sl * 8;
+    return 16 + nd * (RB_LMAP + RB_SCAN_NF) * 8 + (long long)P.nmat * P.np * 8 + (long long)P.nmat * nm * nm * 8 +
+           (long long)RB_LKEYS * nd * local1d_kent(P) * 8 + lc * 8 + 2 * ((lc * 4 + 15) & ~15LL) +
+           (psi > sl ? psi : sl) * 8 + sl * 8;
 }
 
 // whether a problem takes the local pass on a cluster of `ncta` CTAs with `local_bytes` of
@@ -68,6 +74,10 @@ struct Local1D {
     double *scsd;   // [nmat][nm·nm] CSD block of the cell matrix (this group)
     double *dx;     // [lc] widths of the owned cells
     int *mat;       // [lc] materials of the owned cells
+    int *key;       // [lc] cell kind (index of its (material, width) pair) of the owned cells
+    int *nkey;      // kinds among the owned cells; 0 when more than RB_LKEYS (per-cell solves)
+    double *ktab;   // [RB_LKEYS][nd][kent] factored cell operators: S⁻¹, S⁻¹·h·Gsrc, the face map
+    int kent;
     void *psi;      // [ncl][ldp] ψ of the local columns (double or float); in the Gram-Schmidt
                     // loop, the slice of the basis vector in use
     double *ws;     // the slice of w in the Gram-Schmidt loop
@@ -80,13 +90,17 @@ struct Local1D {
         const int lc = (P.nx + (int)ncta - 1) / (int)ncta;
         cb = min(P.nx, (int)crank * lc);
         ce = min(P.nx, cb + lc);
-        cmap = reinterpret_cast<double *>(base);
+        nkey = reinterpret_cast<int *>(base);
+        cmap = reinterpret_cast<double *>(reinterpret_cast<unsigned char *>(base) + 16);
         fx = cmap + (long long)P.nd * RB_LMAP;
         kmat = fx + (long long)P.nd * RB_SCAN_NF;
         scsd = kmat + (long long)P.nmat * P.np;
-        dx = scsd + (long long)P.nmat * P.nm5 * P.nm5;
+        kent = local1d_kent(P);
+        ktab = scsd + (long long)P.nmat * P.nm5 * P.nm5;
+        dx = ktab + (long long)RB_LKEYS * P.nd * kent;
         mat = reinterpret_cast<int *>(dx + lc);
-        psi = reinterpret_cast<unsigned char *>(mat) + ((lc * 4 + 15) & ~15);
+        key = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(mat) + ((lc * 4 + 15) & ~15));
+        psi = reinterpret_cast<unsigned char *>(key) + ((lc * 4 + 15) & ~15);
         ldp = P.nd + 1;
         const long long np_ = (long long)(P.nd + 1) * P.nm5 * lc, sl = local1d_slice(P, (int)ncta);
         ws = reinterpret_cast<double *>(psi) + (np_ > sl ? np_ : sl);
@@ -130,7 +144,193 @@ __device__ __forceinline__ void local1d_group_setup(const DevProblem &P, Local1D
         L.mat[c] = P.mat[L.cb + c];
     }
     __syncthreads();
+    if (threadIdx.x == 0) {  // the (material, width) kinds of the owned cells, in first-seen order
+        int nk2 = 0, km[RB_LKEYS];
+        double kd[RB_LKEYS];
+        for (int c = 0; c < nl && nk2 >= 0; c++) {
+            int k = 0;
+            while (k < nk2 && !(km[k] == L.mat[c] && kd[k] == L.dx[c])) k++;
+            if (k == nk2) {
+                if (nk2 == RB_LKEYS) { nk2 = -1; break; }
+                km[k] = L.mat[c];
+                kd[k] = L.dx[c];
+                nk2++;
+            }
+            L.key[c] = k;
+        }
+        *L.nkey = nk2 < 0 ? 0 : nk2;
+    }
+    __syncthreads();
 }
+
+// Factored cell operators of each (kind, direction): S = Σt·I + h·G + Scsd of flux_1D_BTE /
+// flux_1D_BFP (sn_1D_bte.jl:42-46, sn_1D_bfp.jl:77-82) is the same for every cell of a kind,
+// so it is solved once per group for the identity and h·Gsrc, giving S⁻¹, Y = S⁻¹·h·Gsrc and
+// the face map A = ω₁·I + Gout·Y (the identity for a tangential direction).
+template <int NM, int NF>
+__device__ void local1d_factor(const DevProblem &P, const GroupShared &gs, Local1D &L) {
+    const int nk = *L.nkey, nd = P.nd;
+    for (int o = threadIdx.x; o < nk * nd; o += blockDim.x) {
+        const int k = o / nd, n = o % nd;
+        int c = 0;
+        while (L.key[c] != k) c++;
+        const int m = L.mat[c];
+        const bool tang = P.tang[n] != 0;
+        const double h = tang ? 0.0 : fabs(P.cosv[n]) / L.dx[c];
+        const long long tb = (long long)n * 3;
+        double S[NM * NM], q[NM + NF][NM];
+#pragma unroll
+        for (int i = 0; i < NM; i++)
+#pragma unroll
+            for (int j = 0; j < NM; j++)
+                S[i + NM * j] = (i == j ? gs.sigt[m] : 0.0) + h * P.G[tb * NM * NM + i + NM * j] +
+                                (P.csd ? L.scsd[(long long)m * NM * NM + i + NM * j] : 0.0);
+#pragma unroll
+        for (int r = 0; r < NM + NF; r++)
+#pragma unroll
+            for (int i = 0; i < NM; i++)
+                q[r][i] = r < NM ? (r == i ? 1.0 : 0.0) : h * P.Gsrc[tb * NM * P.nfmax + i + NM * (r - NM)];
+        lu_solve<double, NM, NM + NF>(S, q);
+        double *T = L.ktab + (long long)o * L.kent;
+#pragma unroll
+        for (int j = 0; j < NM; j++)
+#pragma unroll
+            for (int i = 0; i < NM; i++) T[i + NM * j] = q[j][i];
+#pragma unroll
+        for (int f = 0; f < NF; f++)
+#pragma unroll
+            for (int i = 0; i < NM; i++) T[NM * NM + i + NM * f] = q[NM + f][i];
+#pragma unroll
+        for (int f = 0; f < NF; f++)
+#pragma unroll
+            for (int g = 0; g < NF; g++) {
+                double a = (f == g) ? (tang ? 1.0 : P.w1[0]) : 0.0;
+                if (!tang)
+#pragma unroll
+                    for (int j = 0; j < NM; j++) a += P.Gout[tb * NM * P.nfmax + f + NF * j] * q[NM + g][j];
+                T[NM * NM + NM * NF + f + NF * g] = a;
+            }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void local1d_factor_fixed(const DevProblem &P, const GroupShared &gs, Local1D &L) {
+    const int nm = P.nm5, nf = P.nmf[0];
+    if (nm == 1 && nf == 1) local1d_factor<1, 1>(P, gs, L);
+    else if (nm == 2 && nf == 1) local1d_factor<2, 1>(P, gs, L);
+    else if (nm == 3 && nf == 1) local1d_factor<3, 1>(P, gs, L);
+    else if (nm == 2 && nf == 2) local1d_factor<2, 2>(P, gs, L);
+    else if (nm == 4 && nf == 2) local1d_factor<4, 2>(P, gs, L);
+}
+
+// One cell with the factored operator of its kind: the right-hand side q0 = Qn − E·F_E, then
+// y = S⁻¹·q0; the face map is F_out = A·F_in + Gout·y and the cell moments are y + Y·F_in.
+template <typename R, int NM, int NF, int NE, bool CSD, typename PS>
+struct CellKey1D {
+    const DevProblem &P;
+    const GroupShared &gs;
+    const Local1D &L;
+    int n, nd;
+    bool tang;
+    R Go[NF * NM];
+    R w1x, w1E;
+    const double *phiE_in;
+    double *phiE_out;
+
+    __device__ CellKey1D(const DevProblem &P_, const GroupShared &gs_, const Local1D &L_, int n_, const double *pEi,
+                         double *pEo)
+        : P(P_), gs(gs_), L(L_), n(n_), nd(P_.nd), phiE_in(pEi), phiE_out(pEo) {
+        tang = P.tang[n] != 0;
+#pragma unroll
+        for (int k = 0; k < NF * NM; k++) Go[k] = (R)P.Gout[(long long)n * 3 * NM * P.nfmax + k];
+        w1x = (R)P.w1[0];
+        w1E = (R)P.w1[3];
+    }
+    __device__ __forceinline__ const double *op(int lc) const {
+        return L.ktab + ((long long)L.key[lc] * nd + n) * L.kent;
+    }
+    // y = S⁻¹·q0 of local cell lc; FE returns the incoming energy-face flux
+    __device__ __forceinline__ void solve0(int lc, const PS *psi, R (&y)[NM], R (&FE)[NE]) const {
+        R q0[NM];
+        const PS *pc = psi + n + L.ldp * NM * lc;
+#pragma unroll
+        for (int j = 0; j < NM; j++) q0[j] = (R)pc[L.ldp * j];
+        if (CSD) {
+            const int m = L.mat[lc];
+            const long long c = L.cb + lc;
+#pragma unroll
+            for (int e = 0; e < NE; e++) FE[e] = phiE_in ? (R)phiE_in[n + (long long)nd * (e + (long long)NE * c)] : R(0);
+            const R spl = (R)gs.sp[m], smn = (R)gs.sm[m];
+#pragma unroll
+            for (int j = 0; j < NM; j++) {
+                R a = R(0);
+#pragma unroll
+                for (int e = 0; e < NE; e++) a += ((R)P.EsA[j + NM * e] * spl - (R)P.EsB[j + NM * e] * smn) * FE[e];
+                q0[j] -= a;
+            }
+        }
+        const double *T = op(lc);
+#pragma unroll
+        for (int i = 0; i < NM; i++) {
+            R a = R(0);
+#pragma unroll
+            for (int j = 0; j < NM; j++) a += (R)T[i + NM * j] * q0[j];
+            y[i] = a;
+        }
+    }
+    __device__ __forceinline__ void map(int lc, const PS *psi, R (&A)[NF * NF], R (&b)[NF]) const {
+        R y[NM], FE[NE];
+        solve0(lc, psi, y, FE);
+        const double *T = op(lc) + NM * NM + NM * NF;
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+            R bb = R(0);
+            if (!tang)
+#pragma unroll
+                for (int j = 0; j < NM; j++) bb += Go[f + NF * j] * y[j];
+            b[f] = bb;
+#pragma unroll
+            for (int g = 0; g < NF; g++) A[f + NF * g] = (R)T[f + NF * g];
+        }
+    }
+    __device__ __forceinline__ void step(int lc, PS *psi, R (&F)[NF]) const {
+        R y[NM], FE[NE];
+        solve0(lc, psi, y, FE);
+        const double *Y = op(lc) + NM * NM;
+#pragma unroll
+        for (int i = 0; i < NM; i++) {
+            R a = y[i];
+#pragma unroll
+            for (int f = 0; f < NF; f++) a += (R)Y[i + NM * f] * F[f];
+            y[i] = a;
+        }
+        if (!tang) {
+            R Fo[NF];
+#pragma unroll
+            for (int f = 0; f < NF; f++) {
+                R a = w1x * F[f];
+#pragma unroll
+                for (int j = 0; j < NM; j++) a += Go[f + NF * j] * y[j];
+                Fo[f] = a;
+            }
+#pragma unroll
+            for (int f = 0; f < NF; f++) F[f] = Fo[f];
+        }
+        if (CSD) {
+            const long long c = L.cb + lc;
+#pragma unroll
+            for (int e = 0; e < NE; e++) {
+                R a = w1E * FE[e];
+#pragma unroll
+                for (int j = 0; j < NM; j++) a += (R)P.Eout[e + NE * j] * y[j];
+                phiE_out[n + (long long)nd * (e + (long long)NE * c)] = (double)a;
+            }
+        }
+        PS *pc = psi + n + L.ldp * NM * lc;
+#pragma unroll
+        for (int j = 0; j < NM; j++) pc[L.ldp * j] = (PS)y[j];
+    }
+};
 
 // compose (A,b) ← (A2,b2)∘(A,b): F ↦ A2·(A·F + b) + b2
 template <typename R, int NF>
@@ -193,9 +393,9 @@ __device__ void sweep1d_local(ClusterTeam &t, const DevProblem &P, GroupShared &
     const int kb = min(nl, ch * lk), ke = min(nl, kb + lk);
     const bool fwd = active ? (P.cosv[n] >= 0.0) : true;
     const int cb = L.cb, ce = L.ce;
+    const bool keyed = *L.nkey > 0;  // factored operators of the cell kinds (else per-cell solves)
     // 1. chunk maps
     if (active) {
-        Cell1D<R, NM, NF, NE, CSD, PS> cell(P, gs, n, phiE_in, phiE_out, L.ldp, cb, L.mat, L.dx, L.scsd);
         R Ac[NF * NF], bc[NF];
 #pragma unroll
         for (int f = 0; f < NF; f++) {
@@ -203,10 +403,20 @@ __device__ void sweep1d_local(ClusterTeam &t, const DevProblem &P, GroupShared &
 #pragma unroll
             for (int g = 0; g < NF; g++) Ac[f + NF * g] = (f == g) ? R(1) : R(0);
         }
-        for (int k = kb; k < ke; k++) {
-            R A[NF * NF], b[NF];
-            cell.map(fwd ? cb + k : ce - 1 - k, psi, A, b);
-            compose_map<R, NF>(A, b, Ac, bc);
+        if (keyed) {
+            CellKey1D<R, NM, NF, NE, CSD, PS> cell(P, gs, L, n, phiE_in, phiE_out);
+            for (int k = kb; k < ke; k++) {
+                R A[NF * NF], b[NF];
+                cell.map(fwd ? k : nl - 1 - k, psi, A, b);
+                compose_map<R, NF>(A, b, Ac, bc);
+            }
+        } else {
+            Cell1D<R, NM, NF, NE, CSD, PS> cell(P, gs, n, phiE_in, phiE_out, L.ldp, cb, L.mat, L.dx, L.scsd);
+            for (int k = kb; k < ke; k++) {
+                R A[NF * NF], b[NF];
+                cell.map(fwd ? cb + k : ce - 1 - k, psi, A, b);
+                compose_map<R, NF>(A, b, Ac, bc);
+            }
         }
 #pragma unroll
         for (int f = 0; f < NF; f++) {
@@ -289,11 +499,16 @@ __device__ void sweep1d_local(ClusterTeam &t, const DevProblem &P, GroupShared &
     __syncthreads();
     // 4. re-sweep each chunk from its incoming flux; ψ becomes the angular flux
     if (active) {
-        Cell1D<R, NM, NF, NE, CSD, PS> cell(P, gs, n, phiE_in, phiE_out, L.ldp, cb, L.mat, L.dx, L.scsd);
         R F[NF];
 #pragma unroll
         for (int f = 0; f < NF; f++) F[f] = (R)gs.chF[threadIdx.x][f];
-        for (int k = kb; k < ke; k++) cell.step(fwd ? cb + k : ce - 1 - k, psi, F);
+        if (keyed) {
+            CellKey1D<R, NM, NF, NE, CSD, PS> cell(P, gs, L, n, phiE_in, phiE_out);
+            for (int k = kb; k < ke; k++) cell.step(fwd ? k : nl - 1 - k, psi, F);
+        } else {
+            Cell1D<R, NM, NF, NE, CSD, PS> cell(P, gs, n, phiE_in, phiE_out, L.ldp, cb, L.mat, L.dx, L.scsd);
+            for (int k = kb; k < ke; k++) cell.step(fwd ? cb + k : ce - 1 - k, psi, F);
+        }
     }
     // 5. CTA 0: outgoing boundary moments, side 1 (X+) collects μ ≥ 0, side 0 (X-) μ < 0
     if (r == 0) {

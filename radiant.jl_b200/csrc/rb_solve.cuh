@@ -206,7 +206,7 @@ struct Solver {
     // team-wide loop in gmres; writes H[0..j, j] and V_{j+1}, returns false when not local.
     __device__ bool mgs_local(const double *w, int jb, int m, double &hjp1) {
         if constexpr (std::is_same<Team, ClusterTeam>::value) {
-            if (!local_ok) return false;
+            if (!LO && !local_ok) return false;
             Local1D L(P, t.crank, t.ncta, local);
             double *ws = L.ws, *vs = reinterpret_cast<double *>(L.psi);
             double *H = gs.H;
@@ -630,9 +630,10 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, voi
             for (long long i = t.rank(); i < nE; i += t.size()) phiE_in[i] = phiE_in[i] * r1 / r0;
         }
         t.sync();
-        if (local_ok) {
+        if (LO || local_ok) {
             Local1D L(P, t.crank, t.ncta, local);
             local1d_group_setup(P, L);
+            local1d_factor_fixed(P, gs, L);
         }
         // Mn·Qlout into ψ, then kept as Qnout for the passes of this group
         m2d_tiles(t, P, gs, P.qlout, nullptr, 0);
