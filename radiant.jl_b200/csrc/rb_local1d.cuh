@@ -377,7 +377,7 @@ __device__ __forceinline__ void apply_map(const double *M, R (&F)[NF]) {
 // (nd ≤ blockDim.x is required). Ends with ψ of the local cells holding the angular flux and,
 // in CTA 0, the outgoing boundary moments written to zout.
 template <typename R, int NM, int NF, int NE, bool CSD, typename PS>
-__device__ void sweep1d_local(ClusterTeam &t, const DevProblem &P, GroupShared &gs, Local1D &L,
+__device__ __noinline__ void sweep1d_local(ClusterTeam &t, const DevProblem &P, GroupShared &gs, Local1D &L,
                               const double *zin, double *zout, int matvec, int np_source, const double *phiE_in,
                               double *phiE_out, int ig) {
     const int nd = P.nd;
@@ -552,12 +552,11 @@ __device__ bool sweep1d_local_fixed(ClusterTeam &t, const DevProblem &P, GroupSh
     return false;
 }
 
-// One pass T(z) = A·z + c (matvec: z − A·z) of a 1D problem whose local region fits. T is the
-// arithmetic type of the products and the sweep, PS the storage type of ψ.
+// the products of the local pass, compiled as functions of their own so that their registers
+// are allocated apart from the rest of the solve
 template <typename T, typename PS>
-__device__ void pass1d_local_t(ClusterTeam &t, const DevProblem &P, GroupShared &gs, Local1D &L, const double *zin,
-                               double *zout, int homog, int matvec, int ig, const double *phiE_in,
-                               double *phiE_out) {
+__device__ __noinline__ void m2d_local(const DevProblem &P, GroupShared &gs, Local1D &L, const double *zin,
+                                       int homog) {
     const int nd = P.nd, np = P.np, nm = P.nm5;
     const int nl = L.ce - L.cb;
     const long long col0 = (long long)nm * L.cb, ncl = (long long)nm * (nl > 0 ? nl : 0);
@@ -579,9 +578,17 @@ __device__ void pass1d_local_t(ClusterTeam &t, const DevProblem &P, GroupShared 
             psi[i + ldp * lc] = (PS)(ad + v);
         });
     }
-    const int np_source = homog ? 0 : P.np_source;
-    const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
-    sweep1d_local_fixed<T, PS>(t, P, gs, L, zin, zout, matvec, np_source, pE, phiE_out, ig);
+}
+
+template <typename T, typename PS>
+__device__ __noinline__ void d2m_local(const DevProblem &P, GroupShared &gs, Local1D &L, const double *zin,
+                                       double *zout, int matvec) {
+    const int nd = P.nd, np = P.np, nm = P.nm5;
+    const int nl = L.ce - L.cb;
+    const long long col0 = (long long)nm * L.cb, ncl = (long long)nm * (nl > 0 ? nl : 0);
+    PS *psi = reinterpret_cast<PS *>(L.psi);
+    const long long ldp = L.ldp;
+    CtaTeam ct;
     // D2M: 𝚽[p, col] = Σ_n Dn[p,n]·ψ[n, col], direction order kept per output
     if (ncl > 0) {
         ProductArgs<PS> a{P.dn, nullptr, np, np, nd, psi, (int)ldp, ncl};
@@ -591,6 +598,19 @@ __device__ void pass1d_local_t(ClusterTeam &t, const DevProblem &P, GroupShared 
             zout[(col0 + lc) * np + i] = matvec ? z - v : v;
         });
     }
+}
+
+// One pass T(z) = A·z + c (matvec: z − A·z) of a 1D problem whose local region fits. T is the
+// arithmetic type of the products and the sweep, PS the storage type of ψ.
+template <typename T, typename PS>
+__device__ void pass1d_local_t(ClusterTeam &t, const DevProblem &P, GroupShared &gs, Local1D &L, const double *zin,
+                               double *zout, int homog, int matvec, int ig, const double *phiE_in,
+                               double *phiE_out) {
+    m2d_local<T, PS>(P, gs, L, zin, homog);
+    const int np_source = homog ? 0 : P.np_source;
+    const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
+    sweep1d_local_fixed<T, PS>(t, P, gs, L, zin, zout, matvec, np_source, pE, phiE_out, ig);
+    d2m_local<T, PS>(P, gs, L, zin, zout, matvec);
     t.sync();
 }
 

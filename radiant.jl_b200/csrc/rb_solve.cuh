@@ -204,7 +204,7 @@ struct Solver {
     // keeps its slice of w, and of the basis vector in use, in shared memory, so a step reads
     // only the next basis vector from memory. Same steps and fused dot products as the
     // team-wide loop in gmres; writes H[0..j, j] and V_{j+1}, returns false when not local.
-    __device__ bool mgs_local(const double *w, int jb, int m, double &hjp1) {
+    __device__ __noinline__ bool mgs_local(const double *w, int jb, int m, double &hjp1) {
         if constexpr (std::is_same<Team, ClusterTeam>::value) {
             if (!LO && !local_ok) return false;
             Local1D L(P, t.crank, t.ncta, local);
