@@ -436,37 +436,61 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     return k;
 }
 
-// Shared memory of the batch kernel (one CTA per SM): GroupShared plus the local region of the
-// 1D local pass, sized for the largest 1D problem of the launch that qualifies. When `widen` is
-// set the cluster may grow (up to 4×, at most RB_MAXCLUSTER CTAs) until that region fits.
-// Problems whose region does not fit take the team-wide pass.
+// Cluster size and shared memory of a launch (one CTA per SM): GroupShared plus, when some 1D
+// problem can take the local pass, a local region of all the shared memory left. The cluster:
+//   LAUNCH_FIXED   the caller's size;
+//   LAUNCH_SERVE   the caller's size, doubled (up to 4×) until the local pass fits;
+//   LAUNCH_BATCH   from 4 CTAs up, the smallest size that still gives no more teams than
+//                  problems (a large batch runs many small teams, a small one a few large
+//                  teams), among the sizes at which every 1D problem fits the local pass with its
+//                  Gram-Schmidt slice in shared memory (else, fits it at all). Below 4 CTAs a team
+//                  is slower per pass than the extra teams gain, measured on B200.
+// Problems that do not fit take the team-wide pass.
+enum { LAUNCH_FIXED = 0, LAUNCH_SERVE = 1, LAUNCH_BATCH = 2 };
 struct LaunchShape {
     int cluster;
     long long local_bytes;
     size_t smem;
 };
 
-static LaunchShape choose_shape(const std::vector<const DevProblem *> &hs, int cluster, bool widen) {
+static LaunchShape choose_shape(const std::vector<const DevProblem *> &hs, int cluster, int mode, int nsm) {
     int dev = 0, per_sm = 0, reserved = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const long long gsz = (long long)sizeof(rb::GroupShared);
-    const long long b1 = std::min<long long>(optin, (long long)per_sm - reserved) - gsz;
-    auto need = [&](int C) {
-        long long m = 0;
-        for (const DevProblem *h : hs)
-            if (rb::local1d_ok(*h, C, 1LL << 40)) m = std::max(m, rb::local1d_bytes(*h, C));
-        return m;
-    };
+    const long long b1 = (std::min<long long>(optin, (long long)per_sm - reserved) - gsz) & ~15LL;
     LaunchShape sh{cluster, 0, (size_t)gsz};
-    if (need(cluster) == 0 || b1 <= 0) return sh;
-    sh.local_bytes = b1;  // problems larger than the whole region take the team-wide pass
-    for (int C = cluster; C <= (widen ? std::min(RB_MAXCLUSTER, 4 * cluster) : cluster); C *= 2)
-        if (need(C) <= b1) { sh.cluster = C; sh.local_bytes = need(C); break; }
-    sh.local_bytes = (sh.local_bytes + 15) & ~15LL;
-    sh.smem = (size_t)(gsz + sh.local_bytes);
+    bool any = false;
+    for (const DevProblem *h : hs) any = any || rb::local1d_ok(*h, 1 << 4, 1LL << 40);
+    if (!any || b1 <= 0) return sh;
+    auto fits = [&](int C, bool w) {  // every local-shaped 1D problem fits the local pass at cluster C
+        for (const DevProblem *h : hs)
+            if (rb::local1d_ok(*h, C, 1LL << 40) && !(w ? rb::local1d_w(*h, C, b1) : rb::local1d_ok(*h, C, b1)))
+                return false;
+        return true;
+    };
+    int C = cluster;
+    if (mode == LAUNCH_SERVE) {
+        for (int c = cluster; c <= std::min(RB_MAXCLUSTER, 4 * cluster); c *= 2)
+            if (fits(c, false)) { C = c; break; }
+    } else if (mode == LAUNCH_BATCH) {
+        const int n = (int)hs.size();
+        for (int w = 1; w >= 0 && C == cluster; w--) {
+            int best = -1, largest = -1;
+            for (int c = 4; c <= RB_MAXCLUSTER; c *= 2) {
+                if (!fits(c, w != 0)) continue;
+                largest = c;
+                if (best < 0 && nsm / c <= n + n / 20) best = c;
+            }
+            if (best < 0) best = largest;
+            if (best > 0) { C = best; break; }
+        }
+    }
+    sh.cluster = C;
+    sh.local_bytes = b1;
+    sh.smem = (size_t)(gsz + b1);
     return sh;
 }
 
@@ -474,10 +498,11 @@ static LaunchShape choose_shape(const std::vector<const DevProblem *> &hs, int c
 // as many clusters as fit on the device at once, capped by the number of problems. `hs` holds
 // host copies of the problems' records (sizes only) for the shared-memory plan.
 int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm, int cluster, cudaStream_t s,
-                 const std::vector<const DevProblem *> &hs, bool widen) {
+                 const std::vector<const DevProblem *> &hs, int mode) {
     if (cluster < 1) cluster = 1;
     if (cluster > RB_MAXCLUSTER) cluster = RB_MAXCLUSTER;
-    const LaunchShape sh = choose_shape((ctx && !ctx->local1d) ? std::vector<const DevProblem *>() : hs, cluster, widen);
+    const LaunchShape sh =
+        choose_shape((ctx && !ctx->local1d) ? std::vector<const DevProblem *>() : hs, cluster, mode, nsm);
     cluster = sh.cluster;
     const size_t smem = sh.smem;
     const int local_bytes = (int)sh.local_bytes;
@@ -562,7 +587,7 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
             cluster = h0.nd >= 32 ? 4 : (h0.nd >= 16 ? 4 : (h0.nd >= 8 ? 2 : 1));
         }
         int st2 = launch_solve(ctx, ctx->d_list, (int)small.size(), ctx->d_queue, ctx->nsm, cluster, s, small_h,
-                               ctx->cluster <= 0);
+                               ctx->cluster > 0 ? LAUNCH_FIXED : LAUNCH_BATCH);
         if (st2) return st2;
     }
     for (auto *r : large) {
@@ -875,7 +900,8 @@ int32_t rb_submit(rb_context *ctx, const rb_sn_problem *prob, rb_handle *out) {
     CK(cudaMemsetAsync(r->own_queue, 0, sizeof(int), s));
     CK(cudaMemsetAsync(r->h.status, 0, sizeof(int), s));
     int cluster = ctx->cluster > 0 ? ctx->cluster : (r->h.ndims > 1 ? 16 : (r->h.nd >= 16 ? 4 : 2));
-    st = launch_solve(ctx, r->own_list, 1, r->own_queue, ctx->nsm, cluster, s, {&r->h}, ctx->cluster <= 0);
+    st = launch_solve(ctx, r->own_list, 1, r->own_queue, ctx->nsm, cluster, s, {&r->h},
+                      ctx->cluster > 0 ? LAUNCH_FIXED : LAUNCH_SERVE);
     if (st) return st;
     CK(cudaEventCreateWithFlags(&r->done, cudaEventDisableTiming));
     CK(cudaEventRecord(r->done, s));
@@ -984,7 +1010,7 @@ extern "C" int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_resul
     CK(cudaMemcpyAsync(d_list, &d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(d_queue, 0, sizeof(int), s));
     CK(cudaMemsetAsync(h.status, 0, sizeof(int), s));
-    st = launch_solve(nullptr, d_list, 1, d_queue, 1, 1, s, {&h}, false);
+    st = launch_solve(nullptr, d_list, 1, d_queue, 1, 1, s, {&h}, LAUNCH_FIXED);
     if (st) return st;
     const int ng = prob->ng;
     if (res->flux) {

@@ -53,18 +53,23 @@ __host__ __device__ __forceinline__ int local1d_kent(const DevProblem &P) {  // 
     const int nm = P.nm5, nf = P.nmf[0];
     return nm * nm + nm * nf + nf * nf;
 }
-__host__ __device__ __forceinline__ long long local1d_bytes(const DevProblem &P, int ncta) {
+// (with_w: also the slice of w, for the Gram-Schmidt loop in shared memory)
+__host__ __device__ __forceinline__ long long local1d_bytes(const DevProblem &P, int ncta, bool with_w = true) {
     const long long lc = (P.nx + ncta - 1) / ncta, nd = P.nd, nm = P.nm5;
     const long long psi = (nd + 1) * nm * lc, sl = local1d_slice(P, ncta);
     return 16 + nd * (RB_LMAP + RB_SCAN_NF) * 8 + (long long)P.nmat * P.np * 8 + (long long)P.nmat * nm * nm * 8 +
            (long long)RB_LKEYS * nd * local1d_kent(P) * 8 + lc * 8 + 2 * ((lc * 4 + 15) & ~15LL) +
-           (psi > sl ? psi : sl) * 8 + sl * 8;
+           (with_w ? ((psi > sl ? psi : sl) + sl) * 8 : psi * 8);
 }
 
 // whether a problem takes the local pass on a cluster of `ncta` CTAs with `local_bytes` of
 // shared memory beyond the per-CTA state
 __host__ __device__ __forceinline__ bool local1d_ok(const DevProblem &P, int ncta, long long local_bytes) {
-    return P.ndims == 1 && local1d_shape(P) && P.nd <= RB_THREADS && local1d_bytes(P, ncta) <= local_bytes;
+    return P.ndims == 1 && local1d_shape(P) && P.nd <= RB_THREADS && local1d_bytes(P, ncta, false) <= local_bytes;
+}
+// whether its Gram-Schmidt loop also keeps the slice of w in shared memory
+__host__ __device__ __forceinline__ bool local1d_w(const DevProblem &P, int ncta, long long local_bytes) {
+    return local1d_ok(P, ncta, local_bytes) && local1d_bytes(P, ncta, true) <= local_bytes;
 }
 
 struct Local1D {

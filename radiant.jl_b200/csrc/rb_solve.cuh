@@ -40,6 +40,7 @@ struct Solver {
     long long npass;
     void *local = nullptr;  // shared-memory region of the local 1D pass
     int local_ok = 0;       // this problem takes the local 1D pass
+    int local_w = 0;        // and keeps the slice of w in shared memory in the Gram-Schmidt loop
 
     __device__ double *vec(int k) const { return P.vecs + (long long)k * P.vstride; }
 
@@ -206,7 +207,7 @@ struct Solver {
     // team-wide loop in gmres; writes H[0..j, j] and V_{j+1}, returns false when not local.
     __device__ __noinline__ bool mgs_local(const double *w, int jb, int m, double &hjp1) {
         if constexpr (std::is_same<Team, ClusterTeam>::value) {
-            if (!LO && !local_ok) return false;
+            if (!local_w) return false;
             Local1D L(P, t.crank, t.ncta, local);
             double *ws = L.ws, *vs = reinterpret_cast<double *>(L.psi);
             double *H = gs.H;
@@ -567,6 +568,7 @@ template <class Team, bool LO = false>
 __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, void *local = nullptr,
                               long long local_bytes = 0) {
     const int local_ok = (local && local1d_ok(P, (int)t.ncta, local_bytes)) ? 1 : 0;
+    const int local_w = (local && local1d_w(P, (int)t.ncta, local_bytes)) ? 1 : 0;
     const int ng = P.ng, nmat = P.nmat, np = P.np, nd = P.nd, nm = P.nm5;
     const long long nphi = P.nphi, ncell = P.ncell;
     const long long nE = (long long)nd * P.nm4 * ncell;
@@ -642,6 +644,7 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, voi
         Solver<Team, LO> S{t, P, gs, ig, phiE_in, phiE_out, 0};
         S.local = local;
         S.local_ok = local_ok;
+        S.local_w = local_w;
         SolveStat s = S.one_speed(P.flux + (long long)ig * nphi);
         npass += S.npass;
         if (t.rank() == 0) {
