@@ -36,10 +36,10 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "cell-dir-group updates/s"
-# DRAM bytes per update of solve_batch_kernel, from one ncu capture (dram__bytes_read.sum +
+# DRAM bytes per update of solve_local1d_kernel, from one ncu capture (dram__bytes_read.sum +
 # dram__bytes_write.sum) of 18 electron solves of this workload reduced to 8 groups, FP64;
 # traffic grows in proportion to the updates, so a launch's traffic is this times its updates.
-TRAFFIC_BYTES_PER_UPDATE = 418.3
+TRAFFIC_BYTES_PER_UPDATE = 399.8
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
