@@ -564,9 +564,6 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
     if (n == 0) return RB_OK;
     int st = ensure_launch_scratch(ctx, n);
     if (st) return st;
-    std::vector<DevProblem *> ptrs(n);
-    for (int i = 0; i < n; i++) ptrs[i] = recs[i]->d;
-    CK(cudaMemcpyAsync(ctx->d_list, ptrs.data(), sizeof(DevProblem *) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int), s));
     for (auto *r : recs) CK(cudaMemsetAsync(r->h.status, 0, sizeof(int), s));
     // 1D problems (and 2D/3D ones when RB_MD_TEAM=cluster) share one persistent cluster launch;
@@ -574,13 +571,21 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
     std::vector<DevProblem *> small;
     std::vector<const DevProblem *> small_h;
     std::vector<ProblemRec *> large;
+    std::vector<ProblemRec *> qs;
     for (auto *r : recs) {
-        if (r->h.ndims == 1 || ctx->md_cluster) { small.push_back(r->d); small_h.push_back(&r->h); }
+        if (r->h.ndims == 1 || ctx->md_cluster) qs.push_back(r);
         else large.push_back(r);
     }
+    // the work queue hands problems out heaviest first (longest-processing-time order), so the
+    // light ones fill the teams' last slots; the estimate is groups × directions × cells × cell
+    // moments, doubled for the CSD solvers
+    auto work = [](const DevProblem &h) {
+        return (double)h.ng * h.nd * (double)h.ncell * h.nm5 * (h.csd ? 2.0 : 1.0);
+    };
+    std::stable_sort(qs.begin(), qs.end(), [&](const ProblemRec *a, const ProblemRec *b) { return work(a->h) > work(b->h); });
+    for (auto *r : qs) { small.push_back(r->d); small_h.push_back(&r->h); }
     if (!small.empty()) {
-        if ((int)small.size() != n)
-            CK(cudaMemcpyAsync(ctx->d_list, small.data(), sizeof(DevProblem *) * small.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(ctx->d_list, small.data(), sizeof(DevProblem *) * small.size(), cudaMemcpyHostToDevice, s));
         int cluster = ctx->cluster;
         if (cluster <= 0) {  // one cluster per problem, sized to the problem's directions
             const DevProblem &h0 = recs[0]->h;
