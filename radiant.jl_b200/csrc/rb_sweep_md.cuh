@@ -208,6 +208,14 @@ __device__ void sweep_3d_tiles(Team &t, const DevProblem &P, GroupShared &gs, co
     if (D < 1) D = 1;
     const long long sstride = md_scratch_stride(P);
     const int nfx = AF == 1 ? 1 : P.nmf[0], nfy = AF == 1 ? 1 : P.nmf[1], nfz = AF == 1 ? 1 : P.nmf[2];
+    // one-moment cells and faces: inside a tile the y and z faces pass between neighbouring
+    // pencils through shared memory, double-buffered by step parity (the pencil (jy, jz) reads at
+    // step s what (jy−1, jz) and (jy, jz−1) wrote at step s − 1; tile edges use the global face
+    // planes), and each pencil loads the source, material and width of its next cell while it
+    // solves the current one
+    constexpr bool PF = AM == 1 && AF == 1;
+    const bool smf = PF && 4 * D * pen <= RB_TILE_DOUBLES;
+    double *sfy = gs.tile, *sfz = gs.tile + 2 * D * pen;  // [2][D·pen] each
     for (int k0 = 0; k0 < my_dirs; k0 += D) {
         const int dl = threadIdx.x / pen, pl = threadIdx.x % pen;
         const int jy = pl % TY, jz = pl / TY;
@@ -225,8 +233,12 @@ __device__ void sweep_3d_tiles(Team &t, const DevProblem &P, GroupShared &gs, co
                 const bool pcl = active && iyy < ny && izz < nz;
                 const int iy = fy ? iyy : ny - 1 - iyy, iz = fz ? izz : nz - 1 - izz;
                 double F[3][AF], FE[AE], Qn[AM];
+                double qpre = 0.0, dxpre = 1.0;
+                int mpre = 0;
+                const int me = dl * pen + pl;  // this pencil's slot in the shared face buffers
                 for (int s = 0; s < nx + TY + TZ - 2; s++) {
                     const int ixx = s - jy - jz;
+                    const int rd = ((s + 1) & 1) * D * pen, wr = (s & 1) * D * pen;
                     if (pcl && ixx >= 0 && ixx < nx) {
                         const int ix = fx ? ixx : nx - 1 - ixx;
                         const long long c = ix + (long long)nx * (iy + (long long)ny * iz);
@@ -235,16 +247,36 @@ __device__ void sweep_3d_tiles(Team &t, const DevProblem &P, GroupShared &gs, co
                             boundary_in_md(P, n, 0, fx, iy + (long long)ny * iz, zin, np_source, ig, F[0], nfx);
                         if (iyy == 0)
                             boundary_in_md(P, n, 1, fy, ix + (long long)nx * iz, zin, np_source, ig, F[1], nfy);
+                        else if (smf && jy > 0)
+                            F[1][0] = sfy[rd + me - 1];
                         else
                             for (int f = 0; f < nfy; f++) F[1][f] = yfc[yk + f];
                         if (izz == 0)
                             boundary_in_md(P, n, 2, fz, ix + (long long)nx * iy, zin, np_source, ig, F[2], nfz);
+                        else if (smf && jz > 0)
+                            F[2][0] = sfz[rd + me - TY];
                         else
                             for (int f = 0; f < nfz; f++) F[2][f] = zfc[zk + f];
-                        const int m = P.mat[c];
-                        double h[3] = {fabs(mu) / P.dx[ix], fabs(eta) / P.dy[iy], fabs(xi) / P.dz[iz]};
                         double *pc = P.psi + n + (long long)nd * nm * c;
-                        for (int j = 0; j < nm; j++) Qn[j] = pc[(long long)nd * j];
+                        int m;
+                        double dxc;
+                        if (PF && ixx > 0) {
+                            m = mpre;
+                            dxc = dxpre;
+                            Qn[0] = qpre;
+                        } else {
+                            m = P.mat[c];
+                            dxc = P.dx[ix];
+                            for (int j = 0; j < nm; j++) Qn[j] = pc[(long long)nd * j];
+                        }
+                        if (PF && ixx + 1 < nx) {  // the next cell of this pencil
+                            const int ixn = fx ? ix + 1 : ix - 1;
+                            const long long cn = fx ? c + 1 : c - 1;
+                            qpre = P.psi[n + (long long)nd * cn];
+                            mpre = P.mat[cn];
+                            dxpre = P.dx[ixn];
+                        }
+                        double h[3] = {fabs(mu) / dxc, fabs(eta) / P.dy[iy], fabs(xi) / P.dz[iz]};
                         if (P.csd)
                             for (int e = 0; e < ne; e++)
                                 FE[e] = phiE_in ? phiE_in[n + (long long)nd * (e + (long long)ne * c)] : 0.0;
@@ -252,10 +284,20 @@ __device__ void sweep_3d_tiles(Team &t, const DevProblem &P, GroupShared &gs, co
                         for (int j = 0; j < nm; j++) pc[(long long)nd * j] = Qn[j];
                         if (P.csd)
                             for (int e = 0; e < ne; e++) phiE_out[n + (long long)nd * (e + (long long)ne * c)] = FE[e];
-                        if (iyy < ny - 1) for (int f = 0; f < nfy; f++) yfc[yk + f] = F[1][f];
-                        else for (int f = 0; f < nfy; f++) exy[yk + f] = F[1][f];
-                        if (izz < nz - 1) for (int f = 0; f < nfz; f++) zfc[zk + f] = F[2][f];
-                        else for (int f = 0; f < nfz; f++) exz[zk + f] = F[2][f];
+                        if (smf) {
+                            sfy[wr + me] = F[1][0];
+                            sfz[wr + me] = F[2][0];
+                        }
+                        if (iyy < ny - 1) {
+                            if (!smf || jy == TY - 1) for (int f = 0; f < nfy; f++) yfc[yk + f] = F[1][f];
+                        } else {
+                            for (int f = 0; f < nfy; f++) exy[yk + f] = F[1][f];
+                        }
+                        if (izz < nz - 1) {
+                            if (!smf || jz == TZ - 1) for (int f = 0; f < nfz; f++) zfc[zk + f] = F[2][f];
+                        } else {
+                            for (int f = 0; f < nfz; f++) exz[zk + f] = F[2][f];
+                        }
                         if (ixx == nx - 1) for (int f = 0; f < nfx; f++) exx[(iy + (long long)ny * iz) * nfm + f] = F[0][f];
                     }
                     __syncthreads();
