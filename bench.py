@@ -43,9 +43,12 @@ TRAFFIC_BYTES_PER_UPDATE = 399.8
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
-def kernel_name():
+def kernel_name(workload="c2"):
     """The persistent kernel the workload runs on: every 1D problem of the benchmark's workloads
-    takes the local (cell-split) pass, whose batches run on their own kernel."""
+    takes the local (cell-split) pass, whose batches run on their own kernel; a 3D problem runs on
+    the whole GPU as one cooperative launch."""
+    if workload == "c4g1":
+        return "solve_grid_kernel"
     return "solve_batch_kernel" if os.environ.get("RB_LOCAL1D", "1") == "0" else "solve_local1d_kernel"
 
 
@@ -66,6 +69,8 @@ def workload_tables(seeds, precision, workload="c2"):
         return [W.c1_tables(seed=s, precision=precision) for s in seeds]
     if workload == "c2e8":  # small case (profiling): the electron BFP solve of the workload, 8 groups
         return [W.c2_tables(seed=s, precision=precision, ng=8) for s in seeds]
+    if workload == "c4g1":  # small case (profiling): the C4-shaped 3D photon solve, one group
+        return [W.c4_tables(seed=s, ng=1) for s in seeds]
     for s in seeds:
         for part in ("photon", "electron", "positron"):
             t = W.c2_tables(seed=s * 3 + {"photon": 0, "electron": 1, "positron": 2}[part], precision=precision,
@@ -261,7 +266,7 @@ def run_ours(args, rank, world):
                      "frac": achieved / peak,
                      "traffic": TRAFFIC_BYTES_PER_UPDATE * updates if args.workload == "c2" and args.precision == "fp64" else None,
                      "traffic_note": "bytes per launch, scaled from an ncu capture of the reduced workload",
-                     "algorithmic_bytes": abytes, "peak_source": pk, "kernel": kernel_name()},
+                     "algorithmic_bytes": abytes, "peak_source": pk, "kernel": kernel_name(args.workload)},
         "e2e": {"value": updates * world / (e2e_ms / 1e3), "unit": "updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": args.steps,
@@ -393,8 +398,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--seeds", type=int, default=50)
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2e8"],
-                    help="c2: the benchmark workload; c1 / c2e8: small cases for profiling captures")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2e8", "c4g1"],
+                    help="c2: the benchmark workload; c1 / c2e8 / c4g1: small cases for profiling captures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per problem team (0: library default)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
