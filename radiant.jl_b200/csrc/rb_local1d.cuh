@@ -117,19 +117,20 @@ struct Local1D {
 };
 
 // Loop over the CTA's slice of a Krylov vector: element j of the slice is state element g,
-// RB_VU elements per thread in flight.
+// RB_SVU elements per thread in flight (a 4-CTA team's whole slice of a C2-sized state).
+#define RB_SVU 40
 #define RB_SLICE_LOOP(L, LOAD, USE)                                                         \
     {                                                                                      \
         const int l1_ = (L).l1, ls_ = (L).ls;                                              \
         const long long e0_ = (L).e0, eb_ = (L).eb;                                        \
-        for (int j0_ = threadIdx.x; j0_ < ls_; j0_ += RB_VU * blockDim.x) {               \
-            _Pragma("unroll") for (int u_ = 0; u_ < RB_VU; u_++) {                         \
+        for (int j0_ = threadIdx.x; j0_ < ls_; j0_ += RB_SVU * blockDim.x) {               \
+            _Pragma("unroll") for (int u_ = 0; u_ < RB_SVU; u_++) {                         \
                 const int j = j0_ + u_ * blockDim.x;                                       \
                 const long long g = j < l1_ ? e0_ + j : eb_ + (j - l1_);                   \
                 if (j < ls_) { LOAD }                                                      \
                 (void)g;                                                                   \
             }                                                                              \
-            _Pragma("unroll") for (int u_ = 0; u_ < RB_VU; u_++) {                         \
+            _Pragma("unroll") for (int u_ = 0; u_ < RB_SVU; u_++) {                         \
                 const int j = j0_ + u_ * blockDim.x;                                       \
                 const long long g = j < l1_ ? e0_ + j : eb_ + (j - l1_);                   \
                 if (j < ls_) { USE }                                                       \

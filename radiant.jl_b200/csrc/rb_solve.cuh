@@ -214,7 +214,7 @@ struct Solver {
             {
                 const double *V0 = vec(4);
                 double acc[1] = {0.0};
-                double xw[RB_VU], xv[RB_VU];
+                double xw[RB_SVU], xv[RB_SVU];
                 RB_SLICE_LOOP(L, { xw[u_] = w[g]; xv[u_] = V0[g]; }, {
                     ws[j] = xw[u_];
                     vs[j] = xv[u_];
@@ -227,7 +227,7 @@ struct Solver {
                     double a1[1] = {0.0};
                     if (i < jb) {
                         const double *Vn = vec(4 + i + 1);
-                        double xn[RB_VU];
+                        double xn[RB_SVU];
                         RB_SLICE_LOOP(L, { xn[u_] = Vn[g]; }, {
                             const double wq = ws[j] + (-h) * vs[j];
                             ws[j] = wq;
