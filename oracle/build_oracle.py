@@ -19,7 +19,7 @@ def build(force: bool = False) -> str:
             and os.path.getmtime(OUT) >= max(os.path.getmtime(src), os.path.getmtime(hdr))):
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    cmd = ["gcc", "-O2", "-std=c99", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math",
+    cmd = ["gcc", "-O2", "-std=gnu99", "-fPIC", "-shared", "-pthread", "-ffp-contract=off", "-fno-fast-math",
            "-Wall", "-Wno-unused-function", src, "-o", OUT, "-lm"]
     subprocess.check_call(cmd)
     return OUT

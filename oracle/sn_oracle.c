@@ -1,8 +1,8 @@
 /*
  * sn_oracle.c -- TEST INFRASTRUCTURE ONLY (the oracle). Never linked into the product.
  *
- * A plain-C, FP64, single-thread restatement of Radiant.jl's discrete-ordinates solve,
- * following the reference line by line so that the CUDA library can be checked against it:
+ * A plain-C, FP64 restatement of Radiant.jl's discrete-ordinates solve, following the
+ * reference line by line so that the CUDA library can be checked against it:
  *
  *   oracle_compute_flux   <- compute_flux(::SN)        src/particle_transport/sn_flux.jl:22-233
  *   one_speed             <- sn_one_speed               src/particle_transport/sn_one_speed.jl:81-195
@@ -22,13 +22,23 @@
  * known answers (pure absorber, infinite medium, particle balance) in tests/, and by the
  * reference's published in-group pass counts (docs/src/theory_sweeping_process.md:88-94).
  *
- * Build: oracle/build_oracle.py (gcc -O2 -fPIC -shared, no -ffast-math, -ffp-contract=off).
+ * Threads. The directions of one pass are swept concurrently (ORACLE_THREADS threads, default:
+ * every online core), each into its own angular-flux and exit-face buffers; the reference's
+ * accumulations over directions, 𝚽l[:,:,cell] += Dn[:,n]·𝚽n (sn_sweep_*D.jl) and the boundary
+ * out-moments (sn_inner_pass.jl:127-129), are then summed per element in direction order
+ * n = 1..Nd from zero, so every element sees the reference's exact sequence of roundings and
+ * the result does not depend on the thread count. Other per-element loops split over cells.
+ *
+ * Build: oracle/build_oracle.py (gcc -O2 -fPIC -shared -pthread, no -ffast-math,
+ * -ffp-contract=off).
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include "../include/radiant_b200.h"
 
@@ -172,6 +182,47 @@ typedef struct {
 } Ctx;
 
 static double *zalloc(int64_t n) { return (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }
+
+/* ------------------------------------------------------------------------------------ */
+/* parallel_for: [0, n) cut into one contiguous range per thread (plain pthreads)        */
+/* ------------------------------------------------------------------------------------ */
+typedef void (*range_fn)(void *arg, int64_t lo, int64_t hi);
+typedef struct { range_fn fn; void *arg; int64_t lo, hi; } RangeJob;
+
+static void *range_worker(void *p) {
+    RangeJob *j = (RangeJob *)p;
+    j->fn(j->arg, j->lo, j->hi);
+    return NULL;
+}
+
+static int oracle_threads(void) {
+    const char *e = getenv("ORACLE_THREADS");
+    long n = e ? atol(e) : sysconf(_SC_NPROCESSORS_ONLN);
+    if (n < 1) n = 1;
+    if (n > 256) n = 256;
+    return (int)n;
+}
+
+/* `work` ~ operations per item: small jobs stay on the calling thread (a thread start costs
+ * about as much as 1e5 operations). */
+static void parallel_for(int64_t n, range_fn fn, void *arg, double work) {
+    int nt = oracle_threads();
+    const double want = (double)n * work / 2e5;
+    if (want < nt) nt = want < 1.0 ? 1 : (int)want;
+    if (nt > n) nt = (int)(n > 0 ? n : 1);
+    if (nt <= 1) { fn(arg, 0, n); return; }
+    pthread_t th[256];
+    RangeJob job[256];
+    int started[256];
+    for (int t = 0; t < nt; t++) {
+        job[t].fn = fn; job[t].arg = arg;
+        job[t].lo = n * t / nt; job[t].hi = n * (t + 1) / nt;
+        started[t] = (t > 0) && pthread_create(&th[t], NULL, range_worker, &job[t]) == 0;
+        if (t > 0 && !started[t]) fn(arg, job[t].lo, job[t].hi); /* no thread: run it here */
+    }
+    fn(arg, job[0].lo, job[0].hi);
+    for (int t = 1; t < nt; t++) if (started[t]) pthread_join(th[t], NULL);
+}
 
 static int64_t face_cells(const Ctx *c, int axis) {
     if (c->ndims == 1) return 1;
@@ -335,7 +386,10 @@ static void boundary_out(Ctx *c, int face, const double *drow, int64_t bcell, co
             bt[p + (int64_t)c->npsurf * (is + (int64_t)nf * (side + 2 * bcell))] += drow[p] * F[is];
 }
 
-static void sweep_direction(Ctx *c, int n, int np_source, const double *phiE_eff) {
+/* Sweeps direction n. Its cell moments 𝚽n go to psi_n[is + nm5·cell] and its outgoing face
+ * fluxes on the exit faces to ex[axis][f + nf·bcell] (bcell the boundary cell of that face);
+ * inner_pass adds them into 𝚽l and the boundary out-moments in direction order. */
+static void sweep_direction(Ctx *c, int n, int np_source, const double *phiE_eff, double *psi_n, double *ex[3]) {
     const rb_sn_problem *P = c->P;
     int nd = c->nd, np = c->np, nm5 = c->nm5;
     int nx = c->ns[0], ny = c->ns[1], nz = c->ns[2];
@@ -343,7 +397,7 @@ static void sweep_direction(Ctx *c, int n, int np_source, const double *phiE_eff
     const double *mrow[3] = {0}, *drow[3] = {0};
     int sm[3] = {0};
     for (int d = 0; d < c->ndims; d++) face_rows(c, n, d, &mrow[d], &drow[d], &sm[d]);
-    const double *Mn = P->mn, *Dn = P->dn;
+    const double *Mn = P->mn;
     int nm4 = c->nm[3];
     /* face flux stores: x faces per (iy,iz), y faces per iz (2D: scalar), z per nothing */
     int nfx = c->nm[0], nfy = c->ndims >= 2 ? c->nm[1] : 1;
@@ -405,36 +459,72 @@ static void sweep_direction(Ctx *c, int n, int np_source, const double *phiE_eff
                 if (c->csd)
                     for (int k = 0; k < nm4; k++)
                         c->phiE_out[n + (int64_t)nd * (k + (int64_t)nm4 * cell)] = FE[k];
-                /* 𝚽l[p,is,cell] += Dn[p,n]·𝚽n[is] */
-                double *phi = c->work;
-                for (int is = 0; is < nm5; is++)
-                    for (int p = 0; p < np; p++)
-                        phi[p + (int64_t)np * (is + (int64_t)nm5 * cell)] += Dn[p + (int64_t)np * n] * phin[is];
-                /* boundary out-moments */
-                if (ixx == nx - 1) boundary_out(c, xs > 0 ? 1 : 0, drow[0], iy + (int64_t)ny * iz, fx);
-                if (c->ndims >= 2 && iyy == ny - 1)
-                    boundary_out(c, ys > 0 ? 3 : 2, drow[1], c->ndims == 2 ? ix : ix + (int64_t)nx * iz, fy);
+                /* 𝚽n of the cell (added into 𝚽l by inner_pass, sn_sweep_*D.jl D2M lines) */
+                for (int is = 0; is < nm5; is++) psi_n[is + (int64_t)nm5 * cell] = phin[is];
+                /* outgoing faces on the exit boundaries */
+                if (ixx == nx - 1)
+                    for (int f = 0; f < nfx; f++) ex[0][f + (int64_t)nfx * (iy + (int64_t)ny * iz)] = fx[f];
+                if (c->ndims >= 2 && iyy == ny - 1) {
+                    int64_t b = c->ndims == 2 ? ix : ix + (int64_t)nx * iz;
+                    for (int f = 0; f < nfy; f++) ex[1][f + (int64_t)nfy * b] = fy[f];
+                }
                 if (c->ndims >= 3 && izz == nz - 1)
-                    boundary_out(c, zs > 0 ? 5 : 4, drow[2], ix + (int64_t)nx * iy, Fz);
+                    for (int f = 0; f < c->nm[2]; f++) ex[2][f + (int64_t)c->nm[2] * (ix + (int64_t)nx * iy)] = Fz[f];
             }
         }
     }
     free(Fx); free(Fy);
 }
 
-/* ------------------------------------------------------------------------------------ */
-/* one source-iteration pass T(z) = A z + c  (sn_inner_pass.jl:17-137)                   */
-/* ------------------------------------------------------------------------------------ */
-static void inner_pass(Ctx *c, int homogeneous) {
+
+/* the directions of one pass, swept concurrently (see the header) */
+typedef struct {
+    Ctx *c;
+    int np_source;
+    const double *phiE_eff;
+    double *psi;       /* [nd][nm5·ncell] */
+    double *ex[3];     /* [nd][exn[axis]] */
+    int64_t exn[3];
+} SweepJob;
+
+static void sweep_range(void *arg, int64_t lo, int64_t hi) {
+    SweepJob *j = (SweepJob *)arg;
+    const int64_t nq = (int64_t)j->c->nm5 * j->c->ncell;
+    for (int64_t n = lo; n < hi; n++) {
+        double *ex[3] = {NULL, NULL, NULL};
+        for (int d = 0; d < j->c->ndims; d++) ex[d] = j->ex[d] + n * j->exn[d];
+        sweep_direction(j->c, (int)n, j->np_source, j->phiE_eff, j->psi + n * nq, ex);
+    }
+}
+
+static void d2m_range(void *arg, int64_t lo, int64_t hi) {
+    SweepJob *j = (SweepJob *)arg;
+    Ctx *c = j->c;
+    const int np = c->np, nm5 = c->nm5, nd = c->nd;
+    const int64_t nq = (int64_t)nm5 * c->ncell;
+    const double *Dn = c->P->dn;
+    for (int64_t cell = lo; cell < hi; cell++)
+        for (int is = 0; is < nm5; is++)
+            for (int p = 0; p < np; p++) {
+                double s = 0.0;
+                for (int n = 0; n < nd; n++) s += Dn[p + (int64_t)np * n] * j->psi[(int64_t)n * nq + is + (int64_t)nm5 * cell];
+                c->work[p + (int64_t)np * (is + (int64_t)nm5 * cell)] = s;
+            }
+}
+
+/* Ql of the cells [lo, hi): Qlout (or 0) + in-group Σs·𝚽 (scattering_source.jl:25-30)
+ * + T·ℳ·𝚽 (fokker_planck_source.jl:26-35), each element in the reference's order. */
+typedef struct { Ctx *c; int homogeneous; const double *phi; } SourceJob;
+
+static void source_range(void *arg, int64_t lo, int64_t hi) {
+    SourceJob *j = (SourceJob *)arg;
+    Ctx *c = j->c;
     const rb_sn_problem *P = c->P;
-    int np = c->np, nm5 = c->nm5;
-    int64_t nphi = c->nphi;
-    double *phi = c->work;
-    /* Ql = Qlout (or 0) + Σs·𝚽 (+ T·ℳ·𝚽) */
-    for (int64_t i = 0; i < nphi; i++) c->ql[i] = homogeneous ? 0.0 : c->qlout[i];
-    int st = P->solver_type;
+    const int np = c->np, nm5 = c->nm5, st = P->solver_type;
+    const double *phi = j->phi;
+    for (int64_t k = lo * np * nm5; k < hi * np * nm5; k++) c->ql[k] = j->homogeneous ? 0.0 : c->qlout[k];
     if (st != 4 && st != 5 && st != 6) {
-        for (int64_t cell = 0; cell < c->ncell; cell++) {
+        for (int64_t cell = lo; cell < hi; cell++) {
             int m = P->mat[cell] - 1;
             for (int p = 0; p < np; p++)
                 for (int is = 0; is < nm5; is++) {
@@ -443,8 +533,8 @@ static void inner_pass(Ctx *c, int homogeneous) {
                 }
         }
     }
-    if (st == 2 || st == 4) { /* fokker_planck_source.jl:26-35 */
-        for (int64_t cell = 0; cell < c->ncell; cell++) {
+    if (st == 2 || st == 4) {
+        for (int64_t cell = lo; cell < hi; cell++) {
             int m = P->mat[cell] - 1;
             for (int is = 0; is < nm5; is++)
                 for (int n = 0; n < np; n++)
@@ -453,13 +543,54 @@ static void inner_pass(Ctx *c, int homogeneous) {
                             c->tg[m] * P->fp[n + (int64_t)np * mm] * phi[mm + (int64_t)np * (is + (int64_t)nm5 * cell)];
         }
     }
+}
+
+/* ------------------------------------------------------------------------------------ */
+/* one source-iteration pass T(z) = A z + c  (sn_inner_pass.jl:17-137)                   */
+/* ------------------------------------------------------------------------------------ */
+static void inner_pass(Ctx *c, int homogeneous) {
+    const rb_sn_problem *P = c->P;
+    int nm5 = c->nm5;
+    int64_t nphi = c->nphi;
+    double *phi = c->work;
+    /* Ql = Qlout (or 0) + Σs·𝚽 (+ T·ℳ·𝚽), cell by cell (independent elements) */
+    SourceJob sj = {c, homogeneous, phi};
+    parallel_for(c->ncell, source_range, &sj, (double)c->np * c->nm5 * (P->solver_type == 2 || P->solver_type == 4 ? c->np : 1));
     int np_source = homogeneous ? 0 : P->np_source;
     int64_t nE = (int64_t)c->nd * c->nm[3] * c->ncell;
     double *phiE_eff = c->phiE_in;
     double *zeroE = NULL;
     if (c->csd && homogeneous) { zeroE = zalloc(nE); phiE_eff = zeroE; }
-    memset(phi, 0, sizeof(double) * nphi);
-    for (int n = 0; n < c->nd; n++) sweep_direction(c, n, np_source, phiE_eff);
+    /* every direction swept into its own buffers, concurrently */
+    SweepJob job = {c, np_source, phiE_eff, NULL, {NULL, NULL, NULL}, {0, 0, 0}};
+    const int64_t nq = (int64_t)nm5 * c->ncell;
+    job.psi = zalloc((int64_t)c->nd * nq);
+    for (int d = 0; d < c->ndims; d++) {
+        job.exn[d] = (int64_t)c->nm[d] * face_cells(c, d);
+        job.ex[d] = zalloc((int64_t)c->nd * job.exn[d]);
+    }
+    parallel_for(c->nd, sweep_range, &job, (double)c->ncell * c->nm5 * (2.0 * c->np + 4.0 * c->nm5 * c->nm5));
+    /* 𝚽l[p,is,cell] = Σ_n Dn[p,n]·𝚽n[is,cell], summed from zero in direction order */
+    parallel_for(c->ncell, d2m_range, &job, (double)c->np * c->nm5 * c->nd);
+    (void)phi;
+    /* boundary out-moments, direction by direction in order (each direction adds one term
+     * to each element it reaches, as the sweep's own calls did) */
+    const int nx = c->ns[0], ny = c->ns[1], nz = c->ns[2];
+    for (int n = 0; n < c->nd; n++) {
+        const double *mrow[3] = {0}, *drow[3] = {0};
+        int sm[3] = {0};
+        for (int d = 0; d < c->ndims; d++) face_rows(c, n, d, &mrow[d], &drow[d], &sm[d]);
+        double cosv[3] = {P->mu[n], c->ndims >= 2 ? P->eta[n] : 0.0, c->ndims >= 3 ? P->xi[n] : 0.0};
+        for (int d = 0; d < c->ndims; d++) {
+            const int face = d * 2 + (cosv[d] >= 0 ? 1 : 0);
+            const int64_t nb = face_cells(c, d);
+            const double *e = job.ex[d] + (int64_t)n * job.exn[d];
+            for (int64_t b = 0; b < nb; b++) boundary_out(c, face, drow[d], b, e + (int64_t)c->nm[d] * b);
+        }
+    }
+    (void)nx; (void)ny; (void)nz;
+    free(job.psi);
+    for (int d = 0; d < c->ndims; d++) free(job.ex[d]);
     /* lagged boundaries: 𝚽*12_in .= 𝚽*12_temp; 𝚽*12_temp .= 0 */
     for (int64_t i = nphi; i < c->nstate; i++) { c->work[i] = c->btemp[i]; c->btemp[i] = 0.0; }
     free(zeroE);
@@ -784,6 +915,33 @@ static SolveStat one_speed(Ctx *c, double *phi_g) {
     return st;
 }
 
+/* Out-of-group source of the cells [lo, hi) for group c->ig (scattering_source.jl:59-68),
+ * groups gi accumulated in increasing order as the reference does. */
+typedef struct { Ctx *c; const double *flux; } OutJob;
+
+static void outscatter_range(void *arg, int64_t lo, int64_t hi) {
+    OutJob *j = (OutJob *)arg;
+    Ctx *c = j->c;
+    const rb_sn_problem *P = c->P;
+    const int ng = c->ng, nmat = c->nmat, np = c->np, ig = c->ig, st = P->solver_type;
+    for (int64_t k = lo * np * c->nm5; k < hi * np * c->nm5; k++) c->qlout[k] = 0.0;
+    if (st == 4 || st == 5) return;
+    for (int gi = 0; gi < ng; gi++) {
+        if (gi == ig) continue;
+        const double *fg = j->flux + (int64_t)gi * c->nphi;
+        for (int64_t cell = lo; cell < hi; cell++) {
+            int m = P->mat[cell] - 1;
+            for (int p = 0; p < np; p++) {
+                double sv = P->sigma_s[m + (int64_t)nmat * (gi + (int64_t)ng * (ig + (int64_t)ng * P->pl[p]))];
+                for (int is = 0; is < c->nm5; is++) {
+                    int64_t k = p + (int64_t)np * (is + (int64_t)c->nm5 * cell);
+                    c->qlout[k] += sv * fg[k];
+                }
+            }
+        }
+    }
+}
+
 /* ------------------------------------------------------------------------------------ */
 /* compute_flux(::SN) group loop (sn_flux.jl:146-233)                                    */
 /* ------------------------------------------------------------------------------------ */
@@ -825,24 +983,9 @@ int oracle_compute_flux(const rb_sn_problem *P, rb_sn_result *R) {
     int st_ = P->solver_type;
     for (int ig = 0; ig < ng; ig++) {
         c->ig = ig;
-        /* Qlout = Σ_{gi≠ig} Σs[mat,gi,ig,l]·𝚽l[gi] (scattering_source.jl:59-68) */
-        memset(c->qlout, 0, sizeof(double) * c->nphi);
-        if (st_ != 4 && st_ != 5) {
-            for (int gi = 0; gi < ng; gi++) {
-                if (gi == ig) continue;
-                const double *fg = flux + (int64_t)gi * c->nphi;
-                for (int64_t cell = 0; cell < c->ncell; cell++) {
-                    int m = P->mat[cell] - 1;
-                    for (int p = 0; p < np; p++) {
-                        double sv = P->sigma_s[m + (int64_t)nmat * (gi + (int64_t)ng * (ig + (int64_t)ng * P->pl[p]))];
-                        for (int is = 0; is < c->nm5; is++) {
-                            int64_t k = p + (int64_t)np * (is + (int64_t)c->nm5 * cell);
-                            c->qlout[k] += sv * fg[k];
-                        }
-                    }
-                }
-            }
-        }
+        /* Qlout = Σ_{gi≠ig} Σs[mat,gi,ig,l]·𝚽l[gi] (scattering_source.jl:59-68), per cell */
+        OutJob oj = {c, flux};
+        parallel_for(c->ncell, outscatter_range, &oj, (double)c->np * c->nm5 * c->ig);
         /* Qlout .+= volume_sources[ig,...] */
         if (P->volume_sources)
             for (int64_t k = 0; k < c->nphi; k++) c->qlout[k] += P->volume_sources[ig + (int64_t)ng * k];
