@@ -2,12 +2,14 @@
 
     python radiant.jl_b200/build.py [--force] [--verbose]
 
-nvcc compiles csrc/rb_capi.cu (which includes the kernels) straight into a shared library
-with a C ABI; the output lands in radiant_b200/lib/ so it travels with the source tree.
+nvcc compiles every csrc/*.cu (the host ABI in rb_capi.cu and each persistent kernel in its own
+rb_kernel_*.cu) to an object in parallel, then links one shared library with a C ABI; the
+output lands in radiant_b200/lib/ so it travels with the source tree.
 """
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -26,12 +28,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
             and os.path.getmtime(OUT) >= max(os.path.getmtime(s) for s in sources())):
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr", "--extended-lambda",
-           os.path.join(CSRC, "rb_capi.cu"), "-o", OUT, "-lcudart"]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [*ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+             "--expt-relaxed-constexpr", "--extended-lambda", "-diag-suppress=128"]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.check_call(cmd)
+        flags.append("-Xptxas=-v")
+    units = sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+    objs = [os.path.join(objdir, u[:-3] + ".o") for u in units]
+
+    def compile_one(k):
+        subprocess.check_call([NVCC, *flags, "-c", os.path.join(CSRC, units[k]), "-o", objs[k]])
+
+    with ThreadPoolExecutor(max_workers=len(units)) as ex:
+        list(ex.map(compile_one, range(len(units))))
+    subprocess.check_call([NVCC, *ARCH, "-shared", *objs, "-o", OUT, "-lcudart"])
     return OUT
 
 

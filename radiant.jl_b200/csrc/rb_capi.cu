@@ -1,5 +1,7 @@
 // rb_capi.cu -- the C ABI of include/radiant_b200.h.
 //
+// The persistent solve kernels it launches are defined in rb_kernel_{batch,local1d,grid}.cu
+// (declared in rb_solve.cuh); this file holds the host side and the small layout kernels.
 // Host side of the library: validates a problem description, derives the per-direction
 // closure tables once per solve, lays every table and work buffer out in one device
 // allocation per problem, launches the persistent solve kernel on a stream and copies the
@@ -22,6 +24,27 @@
 #include "../../include/radiant_b200.h"
 #include "rb_solve.cuh"
 
+
+namespace rb {
+// [ng][nphi] (group-major) -> [ng, nphi] (group fastest, the reference's layout)
+__global__ void to_reference_layout(const double *__restrict__ src, double *__restrict__ dst, int ng,
+                                    long long nphi) {
+    __shared__ double tile[32][33];
+    const long long k0 = (long long)blockIdx.x * 32;
+    const int g0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int g = g0 + j;
+        const long long k = k0 + threadIdx.x;
+        if (g < ng && k < nphi) tile[j][threadIdx.x] = src[(long long)g * nphi + k];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const long long k = k0 + j;
+        const int g = g0 + threadIdx.x;
+        if (g < ng && k < nphi) dst[(long long)ng * k + g] = tile[threadIdx.x][j];
+    }
+}
+}  // namespace rb
 
 namespace {
 
@@ -174,6 +197,43 @@ int nvec_for(const rb_sn_problem *P) {
     return 8;
 }
 
+// TF32 rounding of the tensor cores' input conversion (cvt.rna.tf32.f32: to nearest, ties away
+// from zero, 10 mantissa bits kept).
+float tf32_round(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    u = (u + 0x1000u) & 0xFFFFE000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+
+// Packs operator parts A_p[i + lda·k] (ni rows, nk columns) for tc_product (rb_tc.cuh): blocks of
+// 128 rows × 32 K, block (p, m, kc) at ((p·mtiles + m)·kchunks + kc)·2·4096 floats, the TF32 high
+// part then the low part v − hi, each element (r, k) at byte (r%8)·16 + (r/8)·1024 + (k%4)·4 +
+// (k/4)·128 of its block (the K-major, no-swizzle canonical layout). Zero outside the operator.
+std::vector<float> pack_tc_operator(const std::vector<const double *> &parts, int lda, int ni, int nk) {
+    const int mtiles = (ni + 127) / 128, kch = (nk + 31) / 32;
+    std::vector<float> out((size_t)parts.size() * mtiles * kch * 2 * 4096, 0.0f);
+    for (size_t p = 0; p < parts.size(); p++)
+        for (int m = 0; m < mtiles; m++)
+            for (int kc = 0; kc < kch; kc++) {
+                const size_t base = ((((size_t)p * mtiles + m) * kch + kc) * 2) * 4096;
+                for (int r = 0; r < 128; r++)
+                    for (int kk = 0; kk < 32; kk++) {
+                        const int i = 128 * m + r, k = 32 * kc + kk;
+                        if (i >= ni || k >= nk) continue;
+                        const double v = parts[p][i + (size_t)lda * k];
+                        const float hi = tf32_round((float)v);
+                        const float lo = (float)(v - (double)hi);
+                        const size_t e = (size_t)((r % 8) * 16 + (r / 8) * 1024 + (kk % 4) * 4 + (kk / 4) * 128) / 4;
+                        out[base + e] = hi;
+                        out[base + 4096 + e] = lo;
+                    }
+            }
+    return out;
+}
+
 // Everything derived from the description before it goes to the device.
 struct Derived {
     Moments M;
@@ -181,8 +241,16 @@ struct Derived {
     long long ncell, nphi, nstate, off_b[3], nb[3], fcells[3];
     int csd;
     std::vector<int> mat0;
-    std::vector<double> cosv, mnfp, frow_m, frow_d, G, Gsrc, Gout, Kcsd, Bcsd, EsA, EsB, Eout, vol;
+    std::vector<double> cosv, mn, dn, mnfp, frow_m, frow_d, G, Gsrc, Gout, Kcsd, Bcsd, EsA, EsB, Eout, vol;
     std::vector<int> tang;
+    // 2D/3D: the device holds the directions grouped by octant (quadrant in 2D), each group in
+    // the reference's order; perm[k] is the reference index of device direction k, and
+    // oct_start[o] .. oct_start[o+1] the device directions of octant o (bit 0: μ < 0,
+    // bit 1: η < 0, bit 2: ξ < 0). 1D keeps the reference's order.
+    std::vector<int> perm;
+    int noct = 1, oct_start[9] = {0};
+    // mixed form, 2D/3D: Mn (and Mn·ℳ) and Dn packed for the tensor-core products (rb_tc.cuh)
+    std::vector<float> tc_m2d, tc_d2m;
     double w1[4];
     int nfmax = 1;
 };
@@ -204,8 +272,6 @@ int validate_and_derive(rb_context *ctx, const rb_sn_problem *P, Derived &D) {
         return fail(ctx, RB_ERR_INVALID, "a required table is NULL");
     if (P->max_iter < 1) return fail(ctx, RB_ERR_INVALID, "max_iter must be >= 1");
     if (P->precision != 0 && P->precision != 1) return fail(ctx, RB_ERR_INVALID, "precision %d", P->precision);
-    if (P->precision == 1 && P->ndims != 1)
-        return fail(ctx, RB_ERR_UNSUPPORTED, "the mixed-precision form is built for 1D problems only");
     if (!(P->tol > 0)) return fail(ctx, RB_ERR_INVALID, "tol must be > 0");
     D.csd = P->solver_type >= 2;
     if (D.csd && (!P->s_minus || !P->s_plus || !P->s_mom || !P->e_width || !P->ww))
@@ -257,12 +323,36 @@ int validate_and_derive(rb_context *ctx, const rb_sn_problem *P, Derived &D) {
             if (!(P->dz[c] > 0)) return fail(ctx, RB_ERR_INVALID, "dz[%lld] must be > 0", c);
     }
     for (int d = 0; d < 3; d++) D.fcells[d] = d < P->ndims ? face_cells(P->ndims, D.ns, d) : 0;
-    // directions
+    // directions, grouped by octant on 2D/3D problems (stable: the reference's order inside)
+    D.perm.resize(nd);
+    D.noct = P->ndims == 1 ? 1 : (P->ndims == 2 ? 4 : 8);
+    {
+        auto oct = [&](int n) {
+            if (P->ndims == 1) return 0;
+            int o = (P->mu[n] < 0.0 ? 1 : 0) + (P->eta[n] < 0.0 ? 2 : 0);
+            if (P->ndims == 3) o += P->xi[n] < 0.0 ? 4 : 0;
+            return o;
+        };
+        int k = 0;
+        for (int o = 0; o < D.noct; o++) {
+            D.oct_start[o] = k;
+            for (int n = 0; n < nd; n++)
+                if (oct(n) == o) D.perm[k++] = n;
+        }
+        for (int o = D.noct; o <= 8; o++) D.oct_start[o] = nd;
+    }
+    const std::vector<int> &pm = D.perm;
     D.cosv.assign(3 * (size_t)nd, 0.0);
+    D.mn.resize((size_t)nd * np);
+    D.dn.resize((size_t)np * nd);
     for (int n = 0; n < nd; n++) {
-        D.cosv[n] = P->mu[n];
-        D.cosv[nd + n] = P->eta ? P->eta[n] : 0.0;
-        D.cosv[2 * nd + n] = P->xi ? P->xi[n] : 0.0;
+        D.cosv[n] = P->mu[pm[n]];
+        D.cosv[nd + n] = P->eta ? P->eta[pm[n]] : 0.0;
+        D.cosv[2 * nd + n] = P->xi ? P->xi[pm[n]] : 0.0;
+        for (int p = 0; p < np; p++) {
+            D.mn[n + (size_t)nd * p] = P->mn[pm[n] + (long long)nd * p];
+            D.dn[p + (size_t)np * n] = P->dn[p + (long long)np * pm[n]];
+        }
     }
     // Mn·ℳ
     if (P->solver_type == 2 || P->solver_type == 4) {
@@ -270,9 +360,16 @@ int validate_and_derive(rb_context *ctx, const rb_sn_problem *P, Derived &D) {
         for (int n = 0; n < nd; n++)
             for (int p = 0; p < np; p++) {
                 double s = 0.0;
-                for (int q = 0; q < np; q++) s += P->mn[n + (long long)nd * q] * P->fp[q + (long long)np * p];
+                for (int q = 0; q < np; q++) s += D.mn[n + (size_t)nd * q] * P->fp[q + (long long)np * p];
                 D.mnfp[n + (size_t)nd * p] = s;
             }
+    }
+    // the mixed form's tensor-core operators (2D/3D, up to 256 rows)
+    if (P->precision == 1 && P->ndims >= 2 && nd <= 256 && np <= 256) {
+        std::vector<const double *> pm2d{D.mn.data()};
+        if (!D.mnfp.empty()) pm2d.push_back(D.mnfp.data());
+        D.tc_m2d = pack_tc_operator(pm2d, nd, nd, np);
+        D.tc_d2m = pack_tc_operator({D.dn.data()}, np, np, nd);
     }
     // half-range rows per direction and axis (sn_inner_pass.jl:47-58)
     D.frow_m.assign((size_t)3 * nd * (nps > 0 ? nps : 1), 0.0);
@@ -280,8 +377,8 @@ int validate_and_derive(rb_context *ctx, const rb_sn_problem *P, Derived &D) {
     for (int a = 0; a < P->ndims; a++) {
         int fm = 2 * a, fp = 2 * a + 1;
         for (int n = 0; n < nd; n++) {
-            int k1 = P->n_to_nplus[fm] ? P->n_to_nplus[fm][n] : 0;
-            int k2 = P->n_to_nplus[fp] ? P->n_to_nplus[fp][n] : 0;
+            int k1 = P->n_to_nplus[fm] ? P->n_to_nplus[fm][pm[n]] : 0;
+            int k2 = P->n_to_nplus[fp] ? P->n_to_nplus[fp][pm[n]] : 0;
             int f = -1, k = 0;
             if (k1 != 0) { f = fm; k = k1; } else if (k2 != 0) { f = fp; k = k2; }
             if (f < 0) continue;
@@ -416,8 +513,7 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     offs[k++] = L.take<double>((size_t)nmat * np);        // 37 kmat (in-group Σs per material and moment)
     offs[k++] = L.take<double>((size_t)nmat * nm5 * nm5); // 38 scsd
     {
-        const long long md = (long long)nd * (2LL * D.ns[1] * D.ns[2] + 2LL * D.ns[0] * D.ns[2] +
-                                              2LL * D.ns[0] * D.ns[1]) * D.nfmax;
+        const long long md = (long long)nd * rb::md_scratch_stride_n(D.ns[0], D.ns[1], D.ns[2], D.nfmax);
         const long long one = (long long)nd * RB_MAXFACE;
         offs[k++] = L.take<double>(P->ndims == 1 ? one : md);  // 39 fexit / multi-D face scratch
     }
@@ -433,6 +529,8 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     offs[k++] = L.take<float>(P->precision == 1 ? (size_t)nq : 0);  // 49 psi32 (mixed form)
     offs[k++] = L.take<DevProblem *>(1);                  // 50 own launch list (one entry)
     offs[k++] = L.take<int>(1);                           // 51 own work-queue counter
+    offs[k++] = L.take<float>(D.tc_m2d.size());           // 52 tensor-core M2D operator (mixed 2D/3D)
+    offs[k++] = L.take<float>(D.tc_d2m.size());           // 53 tensor-core D2M operator
     return k;
 }
 
@@ -462,8 +560,8 @@ static LaunchShape choose_shape(const std::vector<const DevProblem *> &hs, int c
     const long long gsz = (long long)sizeof(rb::GroupShared);
     const long long b1 = (std::min<long long>(optin, (long long)per_sm - reserved) - gsz) & ~15LL;
     LaunchShape sh{cluster, 0, (size_t)gsz};
-    bool any = false;
-    for (const DevProblem *h : hs) any = any || rb::local1d_ok(*h, 1 << 4, 1LL << 40);
+    bool any = false;  // some problem takes the local 1D pass or the 3D octant sweep
+    for (const DevProblem *h : hs) any = any || rb::local1d_ok(*h, 1 << 4, 1LL << 40) || h->ndims == 3;
     if (!any || b1 <= 0) return sh;
     auto fits = [&](int C, bool w) {  // every local-shaped 1D problem fits the local pass at cluster C
         for (const DevProblem *h : hs)
@@ -533,9 +631,17 @@ int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm,
     return RB_OK;
 }
 
-// One 2D/3D problem on every SM: a cooperative launch of two CTAs per SM (the team is the grid).
+// One 2D/3D problem on every SM: a cooperative launch of one CTA per SM (the team is the grid),
+// with the shared memory of the 3D octant sweep after GroupShared.
 int launch_grid(rb_context *ctx, DevProblem *prob, cudaStream_t s) {
-    const size_t smem = sizeof(rb::GroupShared);
+    // the region after GroupShared serves the 3D octant sweep and the tensor-core products: all
+    // the shared memory a CTA may have
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const int local_bytes = (int)((optin - (long long)sizeof(rb::GroupShared)) & ~1023LL);
+    if (local_bytes < (int)std::max(rb::oct3d_smem<double>(), rb::oct3d_smem<float>()))
+        return fail(ctx, RB_ERR_CUDA, "not enough shared memory per block (%d bytes)", optin);
+    const size_t smem = sizeof(rb::GroupShared) + local_bytes;
     CK(cudaFuncSetAttribute(rb::solve_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb::solve_grid_kernel, RB_THREADS, smem));
@@ -543,7 +649,7 @@ int launch_grid(rb_context *ctx, DevProblem *prob, cudaStream_t s) {
     if (per_sm > 1) per_sm = 1;
     const int grid = ctx->nsm * per_sm;
     if (!ctx->d_gpart) CK(cudaMalloc(&ctx->d_gpart, sizeof(double) * 2 * 4 * 4096));
-    void *args[] = {(void *)&prob, (void *)&ctx->d_gpart};
+    void *args[] = {(void *)&prob, (void *)&ctx->d_gpart, (void *)&local_bytes};
     CK(cudaLaunchCooperativeKernel((void *)rb::solve_grid_kernel, dim3(grid), dim3(RB_THREADS), args, smem, s));
     return RB_OK;
 }
@@ -627,6 +733,8 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     h.vstride = (D.nstate + 1) & ~1LL;
     for (int a = 0; a < 4; a++) h.w1[a] = D.w1[a];
     for (int f = 0; f < 6; f++) h.bc[f] = P->bc[f];
+    h.noct = D.noct;
+    for (int o = 0; o <= 8; o++) h.oct_start[o] = D.oct_start[o];
 #define DP(T, k) (reinterpret_cast<T *>(b + o[k]))
     h.dx = DP(double, 1); h.mat = DP(int, 2); h.cosv = DP(double, 3); h.mn = DP(double, 4); h.dn = DP(double, 5);
     h.pl = DP(int, 6); h.mnfp = D.mnfp.empty() ? nullptr : DP(double, 7); h.frow_m = DP(double, 8);
@@ -647,6 +755,8 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     h.passes = DP(long long, 45); h.status = DP(int, 46);
     h.dy = P->ndims >= 2 ? DP(double, 47) : nullptr; h.dz = P->ndims >= 3 ? DP(double, 48) : nullptr;
     h.psi32 = P->precision == 1 ? DP(float, 49) : nullptr;
+    h.tc_m2d = D.tc_m2d.empty() ? nullptr : DP(float, 52);
+    h.tc_d2m = D.tc_d2m.empty() ? nullptr : DP(float, 53);
     // mixed form: its contract is 1e-5 relative L2 against the FP64 solution; the FP32
     // operator's noise floor is near 1e-7, so its in-group criterion is held at 1e-7 or looser
     // (the energy-face chain of a CSD solve amplifies the in-group error about tenfold)
@@ -658,8 +768,8 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     if (P->ndims >= 3) PUT(double, 48, P->dz, D.ns[2]);
     PUT(int, 2, D.mat0.data(), D.mat0.size());
     PUT(double, 3, D.cosv.data(), D.cosv.size());
-    PUT(double, 4, P->mn, (size_t)nd * np);
-    PUT(double, 5, P->dn, (size_t)np * nd);
+    PUT(double, 4, D.mn.data(), (size_t)nd * np);
+    PUT(double, 5, D.dn.data(), (size_t)np * nd);
     PUT(int, 6, P->pl, np);
     PUT(double, 7, D.mnfp.data(), D.mnfp.size());
     PUT(double, 8, D.frow_m.data(), D.frow_m.size());
@@ -685,6 +795,8 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     }
     if (P->t_mom) PUT(double, 23, P->t_mom, (size_t)ng * nmat);
     PUT(double, 25, D.vol.data(), D.vol.size());
+    PUT(float, 52, D.tc_m2d.data(), D.tc_m2d.size());
+    PUT(float, 53, D.tc_d2m.data(), D.tc_d2m.size());
     for (int f = 0; f < 2 * P->ndims; f++)
         if (P->surface_sources[f])
             PUT(double, 26 + f, P->surface_sources[f], (size_t)ng * P->np_source * face_cells(P->ndims, D.ns, f / 2));

@@ -32,6 +32,10 @@ struct DevProblem {
     int np_source;
     long long nphi, nstate, off_b[3], nb[3];
     long long fcells[3];  // boundary face cells per axis
+    int noct;          // direction groups: 1 (1D), 4 quadrants (2D), 8 octants (3D)
+    int oct_start[9];  // device directions of group o: [oct_start[o], oct_start[o+1]); 2D/3D
+                       // problems hold their directions sorted by group (bit 0: μ < 0,
+                       // bit 1: η < 0, bit 2: ξ < 0), the reference's order inside a group
     int nvec;          // Krylov vectors allocated in `vecs`
     long long vstride; // distance between Krylov vectors: nstate rounded up to even (the pad stays 0)
     // ---- tables (device pointers) --------------------------------------------------------
@@ -44,6 +48,9 @@ struct DevProblem {
     const double *mnfp;   // [nd,np]  Mn·ℳ (Fokker-Planck solvers) or null
     const double *frow_m; // [3][nd][npsurf] half-range incoming row (zeros when none)
     const double *frow_d; // [3][nd][npsurf] half-range outgoing row
+    // mixed form, 2D/3D: the operators of the tensor-core products packed in split TF32
+    // (rb_tc.cuh): Mn (and Mn·ℳ) for M2D, Dn for D2M; null when not built
+    const float *tc_m2d, *tc_d2m;
     // Closure tables, per direction n and spatial axis a (a < 3), factored so that the cell
     // system of flux_xD_BTE/BFP is  S = Σt·I + Σ_a h_a·G_a + Scsd[mat],
     //   q = Qn + Σ_a h_a·Gsrc_a·F_a − (EsA·S⁺ − EsB·S⁻)·F_E,   F_a' = ω₁·F_a + Gout_a·𝚽n.

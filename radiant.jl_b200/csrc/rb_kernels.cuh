@@ -203,6 +203,15 @@ __device__ void lu_solve_rt(R *S, R *q, int n) {  // S is n×n, leading dimensio
 // ------------------------------------------------------------------------------------------
 // per-CTA shared state
 // ------------------------------------------------------------------------------------------
+// The tensor-core state of a CTA (rb_tc.cuh): TMEM base address, the MMA-completion mbarrier
+// and the parity of its next phase. ready = 0 in kernels that do not allocate TMEM.
+struct TcState {
+    uint64_t mbar;
+    unsigned tmem;
+    unsigned phase;
+    int ready;
+};
+
 struct alignas(16) GroupShared {
     double sigt[RB_MAXMAT];
     double sp[RB_MAXMAT];   // S⁺/ΔE
@@ -223,6 +232,7 @@ struct alignas(16) GroupShared {
         double tile[RB_TILE_DOUBLES];
     };
     TeamShared team;
+    TcState tc;
 };
 
 // Incoming x-face flux of a 1D direction: surface source into moment 1 plus the lagged
@@ -485,7 +495,7 @@ __device__ void sweep1d_scan(Team &t, const DevProblem &P, GroupShared &gs, cons
 }
 
 // Run-time shapes (nm up to RB_MAXNM): one thread per direction walks all cells.
-__device__ void sweep1d_dir_rt(const DevProblem &P, const GroupShared &gs, int n, const double *zin_b,
+static __device__ void sweep1d_dir_rt(const DevProblem &P, const GroupShared &gs, int n, const double *zin_b,
                                int np_source, const double *phiE_in, double *phiE_out, double *psi, int ig) {
     const int nx = P.nx, nd = P.nd, nm = P.nm5, nf = P.nmf[0], ne = P.nm4;
     const double mu = P.cosv[n];

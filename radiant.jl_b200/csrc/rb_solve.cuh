@@ -12,7 +12,7 @@
 
 #include "rb_kernels.cuh"
 #include "rb_local1d.cuh"
-#include "rb_sweep_md.cuh"
+#include "rb_sweep_oct.cuh"
 
 namespace rb {
 
@@ -38,7 +38,8 @@ struct Solver {
     const double *phiE_in;
     double *phiE_out;
     long long npass;
-    void *local = nullptr;  // shared-memory region of the local 1D pass
+    void *local = nullptr;  // shared-memory region of the local 1D pass (and of the 3D octant sweep)
+    long long local_bytes = 0;
     int local_ok = 0;       // this problem takes the local 1D pass
     int local_w = 0;        // and keeps the slice of w in shared memory in the Gram-Schmidt loop
 
@@ -49,7 +50,9 @@ struct Solver {
     // (final = 1), which are FP64: the Krylov right-hand side c = T(0) and the reconstruction
     // pass, which produces the returned flux moments and the energy-face flux carried into the
     // next group (the outer defect-correction update).
-    __device__ void pass(const double *zin, double *out, int homog, int mv, int final = 0) {
+    // One copy of the pass per kernel (it is called from every accelerator): its own register
+    // allocation, and a compile time that does not grow with the number of call sites.
+    __device__ __noinline__ void pass(const double *zin, double *out, int homog, int mv, int final = 0) {
         const int mixed = (P.precision == 1 && !final) ? 1 : 0;
         npass++;
         if constexpr (std::is_same<Team, ClusterTeam>::value) {
@@ -60,7 +63,7 @@ struct Solver {
         }
         if constexpr (!LO) {
             if (P.ndims == 1) pass1d(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
-            else pass_md(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out);
+            else pass_md(t, P, gs, local, local_bytes, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
         }
     }
     __device__ void fixedpoint(double *out, const double *zin) { pass(zin, out, 0, 0); }
@@ -643,6 +646,7 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, voi
         vcopy(t, P.qnout, P.psi, (long long)nd * nm * ncell);
         Solver<Team, LO> S{t, P, gs, ig, phiE_in, phiE_out, 0};
         S.local = local;
+        S.local_bytes = local ? local_bytes : 0;
         S.local_ok = local_ok;
         S.local_w = local_w;
         SolveStat s = S.one_speed(P.flux + (long long)ig * nphi);
@@ -672,69 +676,17 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, voi
 }
 
 // ------------------------------------------------------------------------------------------
-// persistent batch kernel: clusters pull problems from a device work queue
+// the persistent kernels (each defined in its own translation unit, rb_kernel_*.cu)
 // ------------------------------------------------------------------------------------------
-// Dynamic shared memory: GroupShared, then `local_bytes` for the local 1D pass.
-__global__ void __launch_bounds__(RB_THREADS, 1) solve_batch_kernel(DevProblem *const *probs, int nprob,
-                                                                 int *queue, int local_bytes) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
-    void *local = local_bytes > 0 ? (void *)(smem_raw + sizeof(GroupShared)) : nullptr;
-    ClusterTeam t;
-    t.init(&gs.team);
-    while (true) {
-        int idx = 0;
-        if (t.crank == 0 && threadIdx.x == 0) idx = atomicAdd(queue, 1);
-        idx = t.broadcast_from_leader(idx);
-        if (idx >= nprob) break;
-        solve_problem(t, *probs[idx], gs, local, local_bytes);
-    }
-}
-
-// The same persistent loop for batches whose every problem takes the local 1D pass: the kernel
-// carries no other pass, so its registers go to that path alone.
-__global__ void __launch_bounds__(RB_THREADS, 1) solve_local1d_kernel(DevProblem *const *probs, int nprob,
-                                                                   int *queue, int local_bytes) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
-    void *local = (void *)(smem_raw + sizeof(GroupShared));
-    ClusterTeam t;
-    t.init(&gs.team);
-    while (true) {
-        int idx = 0;
-        if (t.crank == 0 && threadIdx.x == 0) idx = atomicAdd(queue, 1);
-        idx = t.broadcast_from_leader(idx);
-        if (idx >= nprob) break;
-        solve_problem<ClusterTeam, true>(t, *probs[idx], gs, local, local_bytes);
-    }
-}
-
-// one large (2D/3D) problem on the whole GPU: a cooperative launch, one team of every CTA
-__global__ void __launch_bounds__(RB_THREADS, 1) solve_grid_kernel(DevProblem *prob, double *gpart) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    GroupShared &gs = *reinterpret_cast<GroupShared *>(smem_raw);
-    GridTeam t;
-    t.init(&gs.team, gpart);
-    solve_problem(t, *prob, gs);
-}
-
-// [ng][nphi] (group-major) -> [ng, nphi] (group fastest, the reference's layout)
-__global__ void to_reference_layout(const double *__restrict__ src, double *__restrict__ dst, int ng,
-                                    long long nphi) {
-    __shared__ double tile[32][33];
-    const long long k0 = (long long)blockIdx.x * 32;
-    const int g0 = blockIdx.y * 32;
-    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-        const int g = g0 + j;
-        const long long k = k0 + threadIdx.x;
-        if (g < ng && k < nphi) tile[j][threadIdx.x] = src[(long long)g * nphi + k];
-    }
-    __syncthreads();
-    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-        const long long k = k0 + j;
-        const int g = g0 + threadIdx.x;
-        if (g < ng && k < nphi) dst[(long long)ng * k + g] = tile[threadIdx.x][j];
-    }
-}
+// Dynamic shared memory: GroupShared, then `local_bytes` for the local 1D pass (and the 3D
+// octant sweep). Clusters pull problems from the work queue `queue`.
+__global__ void __launch_bounds__(RB_THREADS, 1) solve_batch_kernel(DevProblem *const *probs, int nprob, int *queue,
+                                                                 int local_bytes);
+// The same loop for batches whose every problem takes the local 1D pass: the kernel carries no
+// other pass, so its registers go to that path alone.
+__global__ void __launch_bounds__(RB_THREADS, 1) solve_local1d_kernel(DevProblem *const *probs, int nprob, int *queue,
+                                                                   int local_bytes);
+// One large (2D/3D) problem on the whole GPU: a cooperative launch, one team of every CTA.
+__global__ void __launch_bounds__(RB_THREADS, 1) solve_grid_kernel(DevProblem *prob, double *gpart, int local_bytes);
 
 }  // namespace rb

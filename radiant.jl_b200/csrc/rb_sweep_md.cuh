@@ -184,9 +184,44 @@ struct CellMDgen {
 };
 
 // Scratch layout per direction (global): x exits [ny·nz], y exits [nx·nz], z exits [nx·ny],
-// the z-face plane [nx·ny] and (3D) the y-face plane [nx·nz], each × nfmax doubles.
+// the z-face plane [nx·ny] and (3D) the y-face plane [nx·nz] handed between rows / tiles, then
+// the incoming boundary fluxes of the x, y and z faces [ny·nz], [nx·nz], [nx·ny]; each × nfmax
+// doubles. (rb_capi.cu allocates nd times this stride.)
+__host__ __device__ __forceinline__ long long md_scratch_stride_n(long long nx, long long ny, long long nz, int nfm) {
+    return (2 * ny * nz + 3 * nx * nz + 3 * nx * ny) * nfm;
+}
 __device__ __forceinline__ long long md_scratch_stride(const DevProblem &P) {
-    return (2LL * P.ny * P.nz + 2LL * P.nx * P.nz + 2LL * P.nx * P.ny) * P.nfmax;
+    return md_scratch_stride_n(P.nx, P.ny, P.nz, P.nfmax);
+}
+// offset of the incoming boundary fluxes of axis a inside a direction's scratch
+__device__ __forceinline__ long long md_in_offset(const DevProblem &P, int a) {
+    const long long nx = P.nx, ny = P.ny, nz = P.nz;
+    const long long base = ny * nz + 2 * nx * nz + 2 * nx * ny;
+    return (a == 0 ? base : (a == 1 ? base + ny * nz : base + ny * nz + nx * nz)) * P.nfmax;
+}
+
+// The incoming face flux of every direction on every boundary face cell it enters through
+// (boundary_in_md: surface source plus the lagged reflective / periodic in-moments), as one
+// team phase before the sweep, so that the sweep reads one value per face cell instead of a
+// half-range sum per cell and direction.
+template <class Team>
+__device__ void boundary_in_phase(Team &t, const DevProblem &P, const double *zin, int np_source, int ig) {
+    const long long sstride = md_scratch_stride(P);
+    const int nfm = P.nfmax;
+    for (int a = 0; a < P.ndims; a++) {
+        const long long nfc = P.fcells[a];
+        const int nf = P.nmf[a];
+        const long long off = md_in_offset(P, a);
+        for (long long o = t.rank(); o < (long long)P.nd * nfc; o += t.size()) {
+            const int n = (int)(o / nfc);
+            const long long fc = o % nfc;
+            const bool fwd = P.cosv[(long long)a * P.nd + n] >= 0.0;
+            double f0[RB_MAXFACE];
+            boundary_in_md(P, n, a, fwd, fc, zin, np_source, ig, f0, nf);
+            double *dst = P.fexit + (long long)n * sstride + off + fc * nfm;
+            for (int f = 0; f < nf; f++) dst[f] = f0[f];
+        }
+    }
 }
 
 // 3D: pencils along x in tiles of TY×TZ (one thread per pencil). Inside a tile the cells form a
@@ -418,30 +453,6 @@ __device__ void boundary_out_md(Team &t, const DevProblem &P, const double *zin,
         }
         (void)ncell;
     }
-}
-
-// the pass for 2D and 3D problems
-template <class Team>
-__device__ void pass_md(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, double *zout, int homog,
-                        int matvec, int ig, const double *phiE_in, double *phiE_out) {
-    m2d_tiles(t, P, gs, zin, homog ? nullptr : P.qnout, 1);
-    t.sync();
-    const int np_source = homog ? 0 : P.np_source;
-    const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
-    const bool one = P.nm5 == 1 && P.nmf[0] == 1 && P.nmf[1] == 1 && (P.ndims < 3 || P.nmf[2] == 1) && P.nm4 == 1;
-    if (P.ndims == 3) {
-        if (one && !P.csd) sweep_3d_tiles<CellMDfix<1, 1, 1, false, 3>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
-        else if (one) sweep_3d_tiles<CellMDfix<1, 1, 1, true, 3>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
-        else sweep_3d_tiles<CellMDgen, RB_MAXNM, RB_MAXFACE, RB_MAXFACE>(t, P, gs, zin, np_source, pE, phiE_out, ig);
-    } else {
-        if (one && !P.csd) sweep_md<CellMDfix<1, 1, 1, false, 2>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
-        else if (one) sweep_md<CellMDfix<1, 1, 1, true, 2>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
-        else sweep_md<CellMDgen, RB_MAXNM, RB_MAXFACE, RB_MAXFACE>(t, P, gs, zin, np_source, pE, phiE_out, ig);
-    }
-    t.sync();
-    d2m_tiles(t, P, gs, zin, zout, matvec);
-    boundary_out_md(t, P, zin, zout, matvec);
-    t.sync();
 }
 
 }  // namespace rb

@@ -1,0 +1,403 @@
+// rb_sweep_oct.cuh -- 2D and 3D sweeps of one-moment cells (order-1 closures in every axis and
+// in energy: the diamond-difference / DG0 cells of sn_2D_bte.jl:35-116, sn_2D_bfp.jl:45-154,
+// sn_3D_bte.jl:42-152, sn_3D_bfp.jl:52-191), in FP64 (plain form) or FP32 (mixed form).
+//
+// 3D: directions are held grouped by octant, and all directions of one octant share one sweep
+// order, so a thread owns one x-pencil (iy, iz) of a TY×TZ tile and solves up to DB directions
+// of one octant at each cell it visits. Inside a tile the pencils form a hyperplane wavefront:
+// at local step σ the pencil (jy, jz) solves column σ − jy − jz. The x face stays in registers;
+// the y face of the pencil below comes by warp shuffle (it is the neighbouring lane); the z face
+// of the pencil behind comes through shared memory, double-buffered by step parity. Tiles hand
+// their outgoing y/z faces to the downstream tiles through per-direction face planes in global
+// memory. Every (octant batch, tile) is one task on one CTA of the team; the team advances in
+// stages of K local steps separated by team barriers, and a tile runs H stages behind each
+// upwind tile (H·K ≥ the tile's depth), so every face it reads was written one barrier earlier.
+// The cell's inputs (angular source, material, width, incoming energy-face flux) are loaded one
+// step ahead. Each cell sees the same upwind faces as in the reference's lexicographic order
+// (sn_sweep_3D.jl:73-110), so the result equals it up to rounding.
+//
+// 2D: the KBA wavefront of sweep_md (rows of a direction skewed by one column per row, y faces
+// handed between rows through shared memory), one direction per thread, with the next cell's
+// inputs loaded one step ahead.
+#pragma once
+#include "rb_sweep_md.cuh"
+#include "rb_tc.cuh"
+
+#define RB_OCT_K 16      // wavefront steps per stage (3D)
+#define RB_OCT_TILE 16   // tile edge in pencils (3D): 16×16 pencils, one per thread
+
+namespace rb {
+
+// octant batches: octant o's directions cut into ceil(count/db) batches of at most db
+__device__ __forceinline__ int oct_groups(const DevProblem &P, int db) {
+    int ng = 0;
+    for (int o = 0; o < P.noct; o++) ng += (P.oct_start[o + 1] - P.oct_start[o] + db - 1) / db;
+    return ng;
+}
+__device__ __forceinline__ int oct_group(const DevProblem &P, int db, int g, int &first, int &cnt) {
+    for (int o = 0; o < P.noct; o++) {
+        const int c = P.oct_start[o + 1] - P.oct_start[o], nb = (c + db - 1) / db;
+        if (g < nb) {
+            first = P.oct_start[o] + g * db;
+            cnt = min(db, c - g * db);
+            return o;
+        }
+        g -= nb;
+    }
+    first = 0;
+    cnt = 0;
+    return 0;
+}
+
+// The problem is a one-moment 2D/3D problem (every closure of order 1).
+__device__ __forceinline__ bool one_moment_md(const DevProblem &P) {
+    return P.nm5 == 1 && P.nmf[0] == 1 && P.nmf[1] == 1 && (P.ndims < 3 || P.nmf[2] == 1) && P.nm4 == 1;
+}
+
+template <typename R> struct OctDB { static constexpr int value = 10; };  // FP64: registers
+template <> struct OctDB<float> { static constexpr int value = 12; };
+
+// Shared memory the 3D octant sweep needs (bytes): direction constants and z-face buffers.
+template <typename R>
+__host__ __device__ constexpr long long oct3d_smem() {
+    return (long long)sizeof(R) * (OctDB<R>::value * 9 + 2 * OctDB<R>::value * RB_OCT_TILE * RB_OCT_TILE);
+}
+
+// Tile height in y: a power of two up to RB_OCT_TILE, so that a pencil's lower neighbour is the
+// previous lane of the same warp.
+__device__ __forceinline__ int oct_ty(int ny) {
+    int ty = 1;
+    while (ty * 2 <= ny && ty * 2 <= RB_OCT_TILE) ty *= 2;
+    return ty;
+}
+
+// The 3D octant sweep applies: one-moment cells, and one octant batch's tiles fit in the team.
+__device__ __forceinline__ bool oct3d_ok(const DevProblem &P, int ncta, long long smem_bytes, int mixed) {
+    if (P.ndims != 3 || !one_moment_md(P)) return false;
+    const int TY = oct_ty(P.ny), TZ = min(P.nz, RB_OCT_TILE);
+    const int ntiles = ((P.ny + TY - 1) / TY) * ((P.nz + TZ - 1) / TZ);
+    return ntiles <= ncta && smem_bytes >= (mixed ? oct3d_smem<float>() : oct3d_smem<double>());
+}
+
+template <typename R, typename PS, bool CSD, class Team>
+__device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShared &gs, void *smem, const double *zin,
+                            int np_source, const double *phiE_in, double *phiE_out, int ig, PS *psi) {
+    constexpr int DB = OctDB<R>::value, K = RB_OCT_K, TP = RB_OCT_TILE * RB_OCT_TILE;
+    const int nd = P.nd, nx = P.nx, ny = P.ny, nz = P.nz, nfm = P.nfmax;
+    const int TY = oct_ty(ny), TZ = min(nz, RB_OCT_TILE);
+    const int nty = (ny + TY - 1) / TY, ntz = (nz + TZ - 1) / TZ, ntiles = nty * ntz;
+    const int ngrp = oct_groups(P, DB);
+    const int gpr = (int)t.ncta / ntiles;  // octant batches per round (≥ 1: oct3d_ok)
+    const int nround = (ngrp + gpr - 1) / gpr;
+    const int H = 1 + (max(TY, TZ) - 1 + K - 1) / K;  // stages per tile hop
+    const int nsteps = nx + TY + TZ - 2;
+    const int nstage = (nsteps + K - 1) / K + H * (nty - 1 + ntz - 1);
+    // per-direction scratch (md_scratch_stride): exits x [ny·nz], y [nx·nz], z [nx·ny], then the
+    // z-face plane [nx·ny] and the y-face plane [nx·nz] handed between tiles
+    const long long sstride = md_scratch_stride(P);
+    const long long eyo = (long long)ny * nz * nfm, ezo = eyo + (long long)nx * nz * nfm;
+    const long long zoff = ezo + (long long)nx * ny * nfm, yoff = zoff + (long long)nx * ny * nfm;
+    const long long xin = md_in_offset(P, 0), yin = md_in_offset(P, 1), zin_ = md_in_offset(P, 2);
+    R *dc = reinterpret_cast<R *>(smem);  // [DB][9]: |cos|·G (3), |cos|·Gsrc (3), Gout (3)
+    R *sfz = dc + DB * 9;                  // [2][DB][TP]
+    const int me = threadIdx.x, jy = me % TY, jz = me / TY;
+    const R w1x = (R)P.w1[0], w1y = (R)P.w1[1], w1z = (R)P.w1[2], w1e = (R)P.w1[3];
+    const R esa = CSD ? (R)P.EsA[0] : R(0), esb = CSD ? (R)P.EsB[0] : R(0), eout = CSD ? (R)P.Eout[0] : R(0);
+    for (int rnd = 0; rnd < nround; rnd++) {
+        const int g = rnd * gpr + (int)t.crank / ntiles;
+        const int tile = (int)t.crank % ntiles;
+        int first = 0, cnt = 0, oc = 0;
+        if ((int)t.crank < gpr * ntiles && g < ngrp) oc = oct_group(P, DB, g, first, cnt);
+        const bool fx = !(oc & 1), fy = !(oc & 2), fz = !(oc & 4);
+        const int tyq = tile % nty, tzq = tile / nty;  // tile coordinates in sweep order
+        const int dly = H * (tyq + tzq);
+        const int iyy = tyq * TY + jy, izz = tzq * TZ + jz;
+        const bool pok = cnt > 0 && me < TY * TZ && iyy < ny && izz < nz;
+        const int iy = fy ? iyy : ny - 1 - iyy, iz = fz ? izz : nz - 1 - izz;
+        __syncthreads();
+        if (me < cnt) {
+            const int n = first + me;
+            for (int a = 0; a < 3; a++) {
+                const double ac = fabs(P.cosv[(long long)a * nd + n]);
+                const long long blk = (long long)n * 3 + a;
+                dc[me * 9 + a] = (R)(ac * P.G[blk]);
+                dc[me * 9 + 3 + a] = (R)(ac * P.Gsrc[blk * nfm]);
+                dc[me * 9 + 6 + a] = (R)P.Gout[blk * nfm];
+            }
+        }
+        __syncthreads();
+        const R idy = pok ? (R)(1.0 / P.dy[iy]) : R(0), idz = pok ? (R)(1.0 / P.dz[iz]) : R(0);
+        R fxs[DB], fyl[DB], qp[DB], fep[DB];
+        int mp = 0;
+        R idxp = R(0);
+#pragma unroll
+        for (int k = 0; k < DB; k++) { fxs[k] = fyl[k] = qp[k] = fep[k] = R(0); }
+        if (pok) {  // the inputs of the pencil's first cell; the later ones are loaded a step ahead
+            const int ix0 = fx ? 0 : nx - 1;
+            const long long c0 = ix0 + (long long)nx * (iy + (long long)ny * iz);
+            const PS *pq = psi + first + (long long)nd * c0;
+#pragma unroll
+            for (int k = 0; k < DB; k++) qp[k] = k < cnt ? (R)pq[k] : R(0);
+            if (CSD && phiE_in) {
+#pragma unroll
+                for (int k = 0; k < DB; k++) fep[k] = k < cnt ? (R)phiE_in[first + k + (long long)nd * c0] : R(0);
+            }
+            mp = P.mat[c0];
+            idxp = (R)(1.0 / P.dx[ix0]);
+        }
+        for (int st = 0; st < nstage; st++) {
+            const int s0 = (st - dly) * K;
+            for (int u = 0; u < K; u++) {
+                const int sg = s0 + u;
+                if (cnt == 0 || sg < 0 || sg >= nsteps) continue;  // uniform over the CTA
+                const int ixx = sg - jy - jz;
+                const int rd = (sg + 1) & 1, wr = sg & 1;
+                R fyi[DB];
+#pragma unroll
+                for (int k = 0; k < DB; k++) fyi[k] = __shfl_up_sync(0xffffffffu, fyl[k], 1);
+                // the next cell's inputs, in flight while this cell is solved
+                R qn[DB], fen[DB];
+                int mn_ = 0;
+                R idxn = R(0);
+                const bool nxt = pok && ixx >= 0 && ixx + 1 < nx;
+                if (nxt) {
+                    const int ixn = fx ? ixx + 1 : nx - 2 - ixx;
+                    const long long cn = ixn + (long long)nx * (iy + (long long)ny * iz);
+                    const PS *pq = psi + first + (long long)nd * cn;
+#pragma unroll
+                    for (int k = 0; k < DB; k++) qn[k] = k < cnt ? (R)pq[k] : R(0);
+                    if (CSD) {
+                        const double *pe = phiE_in ? phiE_in + first + (long long)nd * cn : nullptr;
+#pragma unroll
+                        for (int k = 0; k < DB; k++) fen[k] = (pe && k < cnt) ? (R)pe[k] : R(0);
+                    }
+                    mn_ = P.mat[cn];
+                    idxn = (R)(1.0 / P.dx[ixn]);
+                }
+                if (pok && ixx >= 0 && ixx < nx) {
+                    const int ix = fx ? ixx : nx - 1 - ixx;
+                    const long long c = ix + (long long)nx * (iy + (long long)ny * iz);
+                    const long long yk = (ix + (long long)nx * iz) * nfm, zk = (ix + (long long)nx * iy) * nfm;
+                    R fzi[DB];
+                    // faces entering the pencil: the domain's incoming fluxes (boundary_in_phase),
+                    // the upwind tile's face planes, or the neighbouring pencils
+                    if (ixx == 0) {
+                        const long long o = xin + (iy + (long long)ny * iz) * nfm;
+#pragma unroll
+                        for (int k = 0; k < DB; k++) fxs[k] = k < cnt ? (R)P.fexit[(long long)(first + k) * sstride + o] : R(0);
+                    }
+                    if (jy == 0) {
+                        const long long o = (iyy == 0 ? yin : yoff) + yk;
+#pragma unroll
+                        for (int k = 0; k < DB; k++) fyi[k] = k < cnt ? (R)P.fexit[(long long)(first + k) * sstride + o] : R(0);
+                    }
+                    if (jz == 0) {
+                        const long long o = (izz == 0 ? zin_ : zoff) + zk;
+#pragma unroll
+                        for (int k = 0; k < DB; k++) fzi[k] = k < cnt ? (R)P.fexit[(long long)(first + k) * sstride + o] : R(0);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < DB; k++) fzi[k] = sfz[(rd * DB + k) * TP + me - TY];
+                    }
+                    const int m = mp;
+                    const R sigt = (R)gs.sigt[m];
+                    R scs = R(0), srcE = R(0);
+                    if (CSD) {
+                        scs = (R)P.scsd[m];
+                        srcE = esa * (R)gs.sp[m] - esb * (R)gs.sm[m];
+                    }
+                    const R idx = idxp;
+                    PS *pc = psi + first + (long long)nd * c;
+#pragma unroll
+                    for (int k = 0; k < DB; k++) {
+                        if (k >= cnt) break;
+                        const R *d = dc + k * 9;
+                        const R S = (scs + sigt) + d[0] * idx + d[1] * idy + d[2] * idz;
+                        R q = qp[k] + (d[3] * idx) * fxs[k] + (d[4] * idy) * fyi[k] + (d[5] * idz) * fzi[k];
+                        if (CSD) q -= srcE * fep[k];
+                        const R v = q / S;
+                        fxs[k] = w1x * fxs[k] + d[6] * v;
+                        fyi[k] = w1y * fyi[k] + d[7] * v;
+                        fzi[k] = w1z * fzi[k] + d[8] * v;
+                        pc[k] = (PS)v;
+                        if (CSD) phiE_out[first + k + (long long)nd * c] = (double)(w1e * fep[k] + eout * v);
+                        sfz[(wr * DB + k) * TP + me] = fzi[k];
+                    }
+                    // faces leaving the tile or the domain
+                    if (jy == TY - 1 || iyy == ny - 1) {
+                        const long long off = iyy < ny - 1 ? yoff : eyo;
+                        for (int k = 0; k < cnt; k++) P.fexit[(long long)(first + k) * sstride + off + yk] = (double)fyi[k];
+                    }
+                    if (jz == TZ - 1 || izz == nz - 1) {
+                        const long long off = izz < nz - 1 ? zoff : ezo;
+                        for (int k = 0; k < cnt; k++) P.fexit[(long long)(first + k) * sstride + off + zk] = (double)fzi[k];
+                    }
+                    if (ixx == nx - 1)
+                        for (int k = 0; k < cnt; k++)
+                            P.fexit[(long long)(first + k) * sstride + (iy + (long long)ny * iz) * nfm] = (double)fxs[k];
+                }
+#pragma unroll
+                for (int k = 0; k < DB; k++) fyl[k] = fyi[k];
+                if (nxt) {
+#pragma unroll
+                    for (int k = 0; k < DB; k++) {
+                        qp[k] = qn[k];
+                        if (CSD) fep[k] = fen[k];
+                    }
+                    mp = mn_;
+                    idxp = idxn;
+                }
+                __syncthreads();
+            }
+            t.sync();
+        }
+    }
+}
+
+// 2D, one-moment cells: sweep_md's wavefront with the next cell's inputs loaded one step ahead
+// and the arithmetic in R (FP64 or FP32) over an angular buffer of PS.
+template <typename R, typename PS, bool CSD, class Team>
+__device__ __noinline__ void sweep2d_pf(Team &t, const DevProblem &P, GroupShared &gs, const double *zin, int np_source,
+                           const double *phiE_in, double *phiE_out, int ig, PS *psi) {
+    const int nd = P.nd, nx = P.nx, ny = P.ny, nfm = P.nfmax;
+    const int ncta = (int)t.ncta, crank = (int)t.crank;
+    // directions dealt in contiguous blocks, so the directions of a CTA are neighbours in ψ
+    const int dlo = (int)((long long)nd * crank / ncta), dhi = (int)((long long)nd * (crank + 1) / ncta);
+    const int my_dirs = dhi - dlo;
+    const int Rr = ny < (int)blockDim.x ? ny : (int)blockDim.x;  // rows per direction
+    int D = (int)blockDim.x / Rr;
+    const int dmax = RB_TILE_DOUBLES * (int)(sizeof(double) / sizeof(R)) / nx;  // y-face slots
+    if (D > dmax) D = dmax;
+    const int nrb = (ny + Rr - 1) / Rr;
+    const long long sstride = md_scratch_stride(P);
+    const long long xin = md_in_offset(P, 0), yin = md_in_offset(P, 1);
+    R *yface = reinterpret_cast<R *>(gs.tile);  // [D][nx]
+    const R w1x = (R)P.w1[0], w1y = (R)P.w1[1], w1e = (R)P.w1[3];
+    const R esa = CSD ? (R)P.EsA[0] : R(0), esb = CSD ? (R)P.EsB[0] : R(0), eout = CSD ? (R)P.Eout[0] : R(0);
+    for (int k0 = 0; k0 < my_dirs; k0 += D) {
+        const int dl = threadIdx.x / Rr, r = threadIdx.x % Rr;
+        const bool active = dl < D && k0 + dl < my_dirs;
+        const int n = dlo + k0 + dl;
+        const double mu = active ? P.cosv[n] : 0.0, eta = active ? P.cosv[nd + n] : 0.0;
+        const bool fx = mu >= 0.0, fy = eta >= 0.0;
+        R gx = R(0), gy = R(0), sx = R(0), sy = R(0), ox = R(0), oy = R(0);
+        if (active) {
+            gx = (R)(fabs(mu) * P.G[(long long)n * 3]);
+            gy = (R)(fabs(eta) * P.G[(long long)n * 3 + 1]);
+            sx = (R)(fabs(mu) * P.Gsrc[((long long)n * 3) * nfm]);
+            sy = (R)(fabs(eta) * P.Gsrc[((long long)n * 3 + 1) * nfm]);
+            ox = (R)P.Gout[((long long)n * 3) * nfm];
+            oy = (R)P.Gout[((long long)n * 3 + 1) * nfm];
+        }
+        double *scr = P.fexit + (active ? (long long)n * sstride : 0);
+        double *exx = scr, *exy = exx + (long long)ny * nfm;
+        R *yf = yface + (long long)dl * nx;
+        for (int rb = 0; rb < nrb; rb++) {
+            const int iyy = rb * Rr + r;
+            const bool row = active && iyy < ny;
+            const int iy = fy ? iyy : ny - 1 - iyy;
+            const R idy = row ? (R)(1.0 / P.dy[iy]) : R(0);
+            R F0 = R(0), qp = R(0), fep = R(0), idxp = R(0);
+            int mp = 0;
+            if (row) {  // the inputs of the row's first cell; the later ones are loaded a step ahead
+                const int ix0 = fx ? 0 : nx - 1;
+                const long long c0 = ix0 + (long long)nx * iy;
+                qp = (R)psi[n + (long long)nd * c0];
+                if (CSD) fep = phiE_in ? (R)phiE_in[n + (long long)nd * c0] : R(0);
+                mp = P.mat[c0];
+                idxp = (R)(1.0 / P.dx[ix0]);
+            }
+            for (int s = 0; s < nx + Rr - 1; s++) {
+                const int ixx = s - r;
+                R qn = R(0), fen = R(0), idxn = R(0);
+                int mn_ = 0;
+                const bool nxt = row && ixx >= 0 && ixx + 1 < nx;
+                if (nxt) {
+                    const int ixn = fx ? ixx + 1 : nx - 2 - ixx;
+                    const long long cn = ixn + (long long)nx * iy;
+                    qn = (R)psi[n + (long long)nd * cn];
+                    if (CSD) fen = phiE_in ? (R)phiE_in[n + (long long)nd * cn] : R(0);
+                    mn_ = P.mat[cn];
+                    idxn = (R)(1.0 / P.dx[ixn]);
+                }
+                if (row && ixx >= 0 && ixx < nx) {
+                    const int ix = fx ? ixx : nx - 1 - ixx;
+                    const long long c = ix + (long long)nx * iy;
+                    // X face of the row and Y face of the column (sn_sweep_2D.jl:71-132): the
+                    // incoming fluxes of boundary_in_phase
+                    if (ixx == 0) F0 = (R)scr[xin + (long long)iy * nfm];
+                    const R F1 = iyy == 0 ? (R)scr[yin + (long long)ix * nfm] : yf[ixx];
+                    const int m = mp;
+                    R S = (R)gs.sigt[m], srcE = R(0);
+                    if (CSD) {
+                        S = (R)P.scsd[m] + S;
+                        srcE = esa * (R)gs.sp[m] - esb * (R)gs.sm[m];
+                    }
+                    const R idx = idxp;
+                    S = S + gx * idx + gy * idy;
+                    R q = qp + (sx * idx) * F0 + (sy * idy) * F1;
+                    if (CSD) q -= srcE * fep;
+                    const R v = q / S;
+                    F0 = w1x * F0 + ox * v;
+                    const R F1o = w1y * F1 + oy * v;
+                    psi[n + (long long)nd * c] = (PS)v;
+                    if (CSD) phiE_out[n + (long long)nd * c] = (double)(w1e * fep + eout * v);
+                    yf[ixx] = F1o;
+                    if (ixx == nx - 1) exx[(long long)iy * nfm] = (double)F0;
+                    if (iyy == ny - 1) exy[(long long)ix * nfm] = (double)F1o;
+                }
+                if (nxt) { qp = qn; fep = fen; mp = mn_; idxp = idxn; }
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// The pass for 2D and 3D problems. mixed: FP32 angular buffer, products and sweep where the
+// cells are one-moment and (3D) the octant sweep fits the team; every other 2D/3D pass runs in
+// FP64 (the result is then the plain form's).
+template <class Team>
+__device__ __noinline__ void pass_md(Team &t, const DevProblem &P, GroupShared &gs, void *smem, long long smem_bytes,
+                        const double *zin, double *zout, int homog, int matvec, int ig, const double *phiE_in,
+                        double *phiE_out, int mixed) {
+    const bool one = one_moment_md(P);
+    const bool oct = oct3d_ok(P, (int)t.ncta, smem_bytes, mixed);
+    const int mx = (mixed && one && (P.ndims == 2 || oct)) ? 1 : 0;
+    // the mixed form's products go to the tensor cores where the CTA holds TMEM and they fit
+    if (!mx || !m2d_tc(t, P, gs, gs.tc, smem, smem_bytes, zin, homog ? nullptr : P.qnout))
+        m2d_tiles(t, P, gs, zin, homog ? nullptr : P.qnout, 1, mx);
+    const int np_source = homog ? 0 : P.np_source;
+    const double *pE = (P.csd && !homog) ? phiE_in : nullptr;
+    const bool newsweep = (P.ndims == 3 && oct) || (P.ndims == 2 && one);
+    if (newsweep) boundary_in_phase(t, P, zin, np_source, ig);
+    t.sync();
+    if (P.ndims == 3 && oct) {
+        if (mx) {
+            if (P.csd) sweep3d_oct<float, float, true>(t, P, gs, smem, zin, np_source, pE, phiE_out, ig, P.psi32);
+            else sweep3d_oct<float, float, false>(t, P, gs, smem, zin, np_source, pE, phiE_out, ig, P.psi32);
+        } else {
+            if (P.csd) sweep3d_oct<double, double, true>(t, P, gs, smem, zin, np_source, pE, phiE_out, ig, P.psi);
+            else sweep3d_oct<double, double, false>(t, P, gs, smem, zin, np_source, pE, phiE_out, ig, P.psi);
+        }
+    } else if (P.ndims == 2 && one) {
+        if (mx) {
+            if (P.csd) sweep2d_pf<float, float, true>(t, P, gs, zin, np_source, pE, phiE_out, ig, P.psi32);
+            else sweep2d_pf<float, float, false>(t, P, gs, zin, np_source, pE, phiE_out, ig, P.psi32);
+        } else {
+            if (P.csd) sweep2d_pf<double, double, true>(t, P, gs, zin, np_source, pE, phiE_out, ig, P.psi);
+            else sweep2d_pf<double, double, false>(t, P, gs, zin, np_source, pE, phiE_out, ig, P.psi);
+        }
+    } else if (P.ndims == 3) {
+        if (one && !P.csd) sweep_3d_tiles<CellMDfix<1, 1, 1, false, 3>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+        else if (one) sweep_3d_tiles<CellMDfix<1, 1, 1, true, 3>, 1, 1, 1>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+        else sweep_3d_tiles<CellMDgen, RB_MAXNM, RB_MAXFACE, RB_MAXFACE>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+    } else {
+        sweep_md<CellMDgen, RB_MAXNM, RB_MAXFACE, RB_MAXFACE>(t, P, gs, zin, np_source, pE, phiE_out, ig);
+    }
+    t.sync();
+    if (!mx || !d2m_tc(t, P, gs.tc, smem, smem_bytes, zin, zout, matvec)) d2m_tiles(t, P, gs, zin, zout, matvec, mx);
+    boundary_out_md(t, P, zin, zout, matvec);
+    t.sync();
+}
+
+}  // namespace rb

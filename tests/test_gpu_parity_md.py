@@ -115,3 +115,85 @@ def test_3d_reflective_z(md_ctx, accel):
 
 def test_3d_bfp_periodic(md_ctx):
     check(md_ctx, grid3d(sn2(solver="BFP"), bc=(2, 2, 0, 0, 0, 0), csd=True))
+
+
+# ---- the configurations' own shapes -------------------------------------------------------
+# 128² with level-symmetric S12 and the Galerkin-d basis (168 directions, 168 moments), and 64³
+# with S8 (80 directions, 80 moments), BiCGStab and a reflective Z- face: the sizes at which the
+# product tiles, the octant tiles of the 3D sweep and the 2D wavefront run in the benchmark.
+# The grid team only (one problem on the whole GPU); fewer groups than the configurations.
+
+@pytest.fixture(scope="module")
+def grid_ctx():
+    ctx = Context(0, 0)
+    yield ctx
+    ctx.close()
+
+
+def test_c3_shape_fp64(grid_ctx):
+    tabs = W.c3_tables(1, "photon", ng=2)
+    assert tabs["nd"] == 168 and tabs["np"] == 168 and tabs["ns"][:2] == [128, 128]
+    check(grid_ctx, tabs)
+
+
+def test_c4_shape_fp64(grid_ctx):
+    tabs = W.c4_tables(1, "photon", ng=1)
+    assert tabs["nd"] == 80 and tabs["np"] == 80 and tabs["ns"] == [64, 64, 64] and tabs["bc"][4] == 1
+    assert tabs["accel"] == "bicgstab"
+    check(grid_ctx, tabs)
+
+
+# ---- the mixed form in 2D and 3D: FP32 sweeps and products, FP64 Krylov and defect correction;
+# contract 1e-5 relative L2 against the FP64 oracle
+MIXED_TOL = 1e-5
+
+
+def check_mixed(ctx, tabs, tol=MIXED_TOL):
+    ref = oracle_run.solve(tabs)
+    t2 = dict(tabs)
+    t2["precision"] = "mixed"
+    pp = PackedProblem(t2)
+    got = ResultBuffers(pp)
+    h = ctx.upload(pp)
+    ctx.solve(h)
+    ctx.download(h, got)
+    ctx.release(h)
+    e = rel_l2(got.flux, ref.flux)
+    assert e <= tol, f"mixed flux rel L2 {e:.3e}"
+    if ref.flux_cutoff is not None:
+        ec = rel_l2(got.flux_cutoff, ref.flux_cutoff)
+        assert ec <= tol, f"mixed cutoff rel L2 {ec:.3e}"
+    assert np.all(got.group_converged == 1)
+    return e
+
+
+@pytest.mark.parametrize("accel", ["gmres", "bicgstab"])
+def test_2d_mixed(md_ctx, accel):
+    check_mixed(md_ctx, grid2d(sn2(accel=accel, boltz="galerkin-d")))
+
+
+def test_2d_bfp_mixed(md_ctx):
+    check_mixed(md_ctx, grid2d(sn2(solver="BFP"), csd=True))
+
+
+@pytest.mark.parametrize("accel", ["gmres", "bicgstab"])
+def test_3d_mixed(md_ctx, accel):
+    check_mixed(md_ctx, grid3d(sn2(accel=accel)))
+
+
+def test_3d_bfp_mixed(md_ctx):
+    check_mixed(md_ctx, grid3d(sn2(solver="BFP"), bc=(2, 2, 0, 0, 0, 0), csd=True))
+
+
+def test_2d_high_order_mixed_runs_fp64(md_ctx):
+    """Order-2 cells have no FP32 sweep: their mixed-form passes run in FP64."""
+    check_mixed(md_ctx, grid2d(sn2(order=2)))
+
+
+def test_c3_shape_mixed(grid_ctx):
+    check_mixed(grid_ctx, W.c3_tables(1, "photon", ng=2))
+
+
+def test_c4_shape_mixed(grid_ctx):
+    check_mixed(grid_ctx, W.c4_tables(1, "photon", ng=1))
+

@@ -96,3 +96,153 @@ def test_accelerators_order_like_the_published_table():
         counts[accel] = int(r.group_iters[0])
     assert counts["none"] > counts["livolant"] > counts["anderson"] > counts["gmres"]
     assert counts["gmres"] <= 40 and counts["bicgstab"] <= 60 and counts["none"] > 10 * counts["gmres"]
+
+
+def _grid_xs_one_group(sig_t, sig_s, L=0):
+    return one_group_xs(sig_t, sig_s, L=L)
+
+
+@pytest.mark.parametrize("ndims,boltz", [(2, "standard"), (2, "galerkin-d"), (3, "standard"), (3, "galerkin-d")])
+def test_infinite_medium_multid(ndims, boltz):
+    """All-reflective 2D / 3D box, uniform isotropic source: the solution is uniform and
+    isotropic, so every cell holds 𝚽₀ = Q / Σa and every higher moment vanishes. Pins the
+    multi-D closures, the moment<->direction products and the lagged reflective faces. The
+    standard half-range basis (Mn = R_lm, Dn = w·R_lm, angular_polynomial_basis.jl:392-407) gives
+    back a constant exactly only at order 0 on an S4 set (its half-range harmonics of order 1 are
+    not orthonormal under that quadrature), so the standard case runs at L = 0."""
+    sig_t, c, Q = 1.1, 0.7, 3.0
+    ns = [4, 3] if ndims == 2 else [3, 3, 2]
+    L = 0 if boltz == "standard" else 1
+    sn = SNSettings(solver_type="BTE", quadrature_type="carlson", quadrature_order=4, legendre_order=L,
+                    scheme_type={a: "DD" for a in "xyz"[:ndims]}, scheme_order={a: 1 for a in "xyz"[:ndims]},
+                    acceleration="gmres", convergence_criterion=1e-12, maximum_iteration=500, angular_boltzmann=boltz)
+    full = ns + [1] * (3 - ndims)
+    vol = np.zeros((1, 1, 1, *full))
+    vol[0, 0, 0] = Q
+    t = prepare_sn_tables(one_group_xs(sig_t, c * sig_t, L=L), ndims, ns, [np.full(k, 0.7) for k in ns],
+                          np.ones(full, dtype=np.int32), [1] * (2 * ndims) + [0] * (6 - 2 * ndims), sn,
+                          volume_sources=vol)
+    r = orun.solve(t)
+    np.testing.assert_allclose(r.flux[0, 0, 0], Q / (sig_t * (1 - c)), rtol=1e-9)
+    if r.flux.shape[1] > 1:
+        assert np.max(np.abs(r.flux[0, 1:])) <= 1e-9 * Q / (sig_t * (1 - c))
+
+
+def _csd_xs(ng, sb, de, nmat=1):
+    st = np.zeros((ng, nmat))
+    return MultigroupXS(sigma_t=st, sigma_s=np.zeros((nmat, ng, ng, 1)), sigma_a=st.copy(),
+                        sb=np.repeat(np.asarray(sb, dtype=float)[:, None], nmat, axis=1),
+                        t_mom=np.zeros((ng, nmat)), sigma_e=np.ones((ng + 1, nmat)), e_width=np.asarray(de, dtype=float),
+                        density=np.ones(nmat))
+
+
+@pytest.mark.parametrize("ndims,schemeE", [(1, "DD"), (1, "DG"), (2, "DD"), (2, "DG")])
+def test_csd_slowing_down_balance(ndims, schemeE):
+    """Continuous slowing down alone (Σt = 0, no scattering, no Fokker-Planck) in an infinite
+    medium (reflective faces) with isotropic sources in some groups. Per direction the energy
+    closure of flux_1D_BFP (sn_1D_bfp.jl:79-121) with the x terms cancelling gives
+    S⁺_g·𝚽E_out = Q_g + S⁻_g·𝚽E_in, and the carry 𝚽E_in(g) = 𝚽E_out(g-1)·ΔE_g/ΔE_(g-1)
+    (sn_flux.jl:183). So the particle current through each group's lower energy face is the
+    source above it: Sb[g+1]·𝚽E_out(g)/ΔE_g = Σ_{g'≤g} Q_g', and the cutoff flux (sn_flux.jl:215-218)
+    carries all of it: Sb[G]·𝚽cutoff/ΔE_G = Σ Q (particle balance: source = cutoff, no leakage
+    and no absorption). The group fluxes follow from the same recurrence."""
+    ng = 5
+    rng = np.random.default_rng(3)
+    de = rng.uniform(0.5, 2.0, ng)
+    sb = rng.uniform(1.0, 3.0, ng + 1)
+    Qg = np.array([1.0, 0.0, 0.4, 0.0, 0.0])
+    ns = [4] if ndims == 1 else [3, 3]
+    axes = "xyz"[:ndims]
+    st = {a: "DD" for a in axes}
+    so = {a: 1 for a in axes}
+    st["E"] = schemeE
+    so["E"] = 1
+    quad = dict(quadrature_type="gauss-legendre", quadrature_order=8) if ndims == 1 else dict(
+        quadrature_type="carlson", quadrature_order=4)
+    sn = SNSettings(solver_type="BFP", legendre_order=0, scheme_type=st, scheme_order=so, acceleration="gmres",
+                    convergence_criterion=1e-12, maximum_iteration=500, angular_fokker_planck="galerkin",
+                    angular_boltzmann="standard", **quad)
+    full = ns + [1] * (3 - ndims)
+    vol = np.zeros((ng, 1, 1, *full))
+    for g in range(ng):
+        vol[g, 0, 0] = Qg[g]
+    t = prepare_sn_tables(_csd_xs(ng, sb, de), ndims, ns, [np.full(k, 0.5) for k in ns],
+                          np.ones(full, dtype=np.int32), [1] * (2 * ndims) + [0] * (6 - 2 * ndims), sn,
+                          volume_sources=vol)
+    wE = np.asarray(t["w_axis"][3], dtype=float).ravel()
+    w1, w2 = wE[0], wE[1]
+    r = orun.solve(t)
+    e_in = 0.0
+    for g in range(ng):
+        sm, sp = sb[g] / de[g], sb[g + 1] / de[g]
+        phi = (Qg[g] - (sp * w1 - sm) * e_in) / (sp * w2)
+        e_out = w1 * e_in + w2 * phi
+        np.testing.assert_allclose(r.flux[g, 0, 0], phi, rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(sb[g + 1] * e_out / de[g], Qg[: g + 1].sum(), rtol=1e-9)
+        e_in = e_out * de[g + 1] / de[g] if g + 1 < ng else e_out
+    np.testing.assert_allclose(r.flux_cutoff[0, 0], e_in, rtol=1e-9)
+    np.testing.assert_allclose(sb[ng] * r.flux_cutoff[0, 0] / de[ng - 1], Qg.sum(), rtol=1e-9)
+
+
+@pytest.mark.parametrize("ndims", [1, 2])
+def test_direction_reversal_symmetry(ndims):
+    """A problem symmetric under x -> L - x (materials, widths and a volume source mirrored,
+    void faces) has a mirrored solution: Legendre / harmonic moments even in μ are symmetric and
+    those odd in μ antisymmetric. Pins the forward and backward sweep orders against each other."""
+    nx = 9
+    ng = 3
+    rng = np.random.default_rng(5)
+    mats = np.array([1, 2, 2, 1, 3, 1, 2, 2, 1], dtype=np.int32)
+    dxs = np.array([0.3, 0.2, 0.5, 0.4, 0.6, 0.4, 0.5, 0.2, 0.3])
+    nmat = 3
+    L = 3
+    st = rng.uniform(0.5, 2.0, (ng, nmat))
+    ss = np.zeros((nmat, ng, ng, L + 1))
+    for m in range(nmat):
+        for gi in range(ng):
+            for gf in range(gi, ng):
+                ss[m, gi, gf, 0] = 0.3 * st[gi, m] / (1 + gf - gi)
+                for l in range(1, L + 1):
+                    ss[m, gi, gf, l] = ss[m, gi, gf, 0] * 0.5 ** l
+    xs = MultigroupXS(sigma_t=st, sigma_s=ss, sigma_a=st * 0.5, density=np.ones(nmat), e_width=np.ones(ng))
+    if ndims == 1:
+        ns = [nx]
+        full = [nx, 1, 1]
+        quad = dict(quadrature_type="gauss-legendre", quadrature_order=8)
+        ds = [dxs]
+        mat = mats.reshape(full)
+    else:
+        ny = 4
+        ns = [nx, ny]
+        full = [nx, ny, 1]
+        quad = dict(quadrature_type="carlson", quadrature_order=4)
+        ds = [dxs, np.full(ny, 0.5)]
+        mat = np.repeat(mats[:, None], ny, axis=1).reshape(full)
+    axes = "xyz"[:ndims]
+    sn = SNSettings(solver_type="BTE", legendre_order=L, scheme_type={a: "DD" for a in axes},
+                    scheme_order={a: 1 for a in axes}, acceleration="gmres", convergence_criterion=1e-12,
+                    maximum_iteration=500, angular_boltzmann="galerkin-d", **quad)
+    vol = np.zeros((ng, 1, 1, *full))
+    prof = np.array([0.0, 1.0, 0.0, 0.0, 2.0, 0.0, 0.0, 1.0, 0.0])
+    for g in range(ng):
+        vol[g, 0, 0] = (prof * (g + 1))[:, None, None]
+    t = prepare_sn_tables(xs, ndims, ns, ds, mat, [0] * 6, sn, volume_sources=vol)
+    r = orun.solve(t)
+    flux = r.flux  # [ng, np, nm5, nx, ny, nz]
+    mirrored = flux[:, :, :, ::-1]
+    # parity of each moment under μ -> -μ: Legendre P_l has (-1)^l; in multi-D the harmonic's
+    # x-parity, read off the basis itself: Mn row of the mirrored direction
+    mu = np.asarray(t["omega"][0])
+    Mn = np.asarray(t["mn"])
+    par = np.zeros(t["np"])
+    for p in range(t["np"]):
+        for n in range(t["nd"]):
+            # the direction with μ -> -μ, other cosines equal
+            m = [k for k in range(t["nd"]) if abs(mu[k] + mu[n]) < 1e-12 and all(
+                abs(t["omega"][a][k] - t["omega"][a][n]) < 1e-12 for a in (1, 2))][0]
+            if abs(Mn[n, p]) > 1e-12:
+                par[p] = np.sign(Mn[m, p] / Mn[n, p])
+                break
+    scale = np.max(np.abs(flux))
+    for p in range(t["np"]):
+        np.testing.assert_allclose(flux[:, p], par[p] * mirrored[:, p], rtol=0, atol=1e-9 * scale)
