@@ -633,14 +633,28 @@ int launch_solve(rb_context *ctx, DevProblem **list, int n, int *queue, int nsm,
 
 // One 2D/3D problem on every SM: a cooperative launch of one CTA per SM (the team is the grid),
 // with the shared memory of the 3D octant sweep after GroupShared.
-int launch_grid(rb_context *ctx, DevProblem *prob, cudaStream_t s) {
-    // the region after GroupShared serves the 3D octant sweep and the tensor-core products: all
-    // the shared memory a CTA may have
+int launch_grid(rb_context *ctx, DevProblem *prob, const DevProblem &hp, cudaStream_t s) {
+    // the region after GroupShared serves the 3D octant sweep and the tensor-core products; it is
+    // sized to what this problem uses, since the rest of the SM's 256 KB stays L1 cache
     int optin = 0;
     CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    const int local_bytes = (int)((optin - (long long)sizeof(rb::GroupShared)) & ~1023LL);
-    if (local_bytes < (int)std::max(rb::oct3d_smem<double>(), rb::oct3d_smem<float>()))
-        return fail(ctx, RB_ERR_CUDA, "not enough shared memory per block (%d bytes)", optin);
+    const long long avail = (optin - (long long)sizeof(rb::GroupShared)) & ~1023LL;
+    const DevProblem &h = hp;
+    const bool mixed = h.precision == 1;
+    long long need = 0;
+    if (h.ndims == 3 && h.nm5 == 1 && h.nm4 == 1 && h.nmf[0] == 1 && h.nmf[1] == 1 && h.nmf[2] == 1)
+        need = mixed ? (h.csd ? rb::oct3d_smem<float, true>() : rb::oct3d_smem<float, false>())
+                     : (h.csd ? rb::oct3d_smem<double, true>() : rb::oct3d_smem<double, false>());
+    if (mixed && h.tc_m2d) {
+        const int parts = h.mnfp ? 2 : 1;
+        const int mt_m = (h.nd + 127) / 128, mt_d = (h.np + 127) / 128;
+        long long tcn = std::max(rb::tc::stage_bytes(parts, mt_m, parts, 128), rb::tc::stage_bytes(1, mt_d, 1, 128));
+        if (tcn > avail)
+            tcn = std::max(rb::tc::stage_bytes(parts, mt_m, parts, 64), rb::tc::stage_bytes(1, mt_d, 1, 64));
+        need = std::max(need, tcn);
+    }
+    if (need > avail) need = 0;  // the problem then takes the paths that need no region
+    const int local_bytes = (int)((need + 1023) & ~1023LL);
     const size_t smem = sizeof(rb::GroupShared) + local_bytes;
     CK(cudaFuncSetAttribute(rb::solve_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -702,7 +716,7 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
         if (st2) return st2;
     }
     for (auto *r : large) {
-        int st3 = launch_grid(ctx, r->d, s);
+        int st3 = launch_grid(ctx, r->d, r->h, s);
         if (st3) return st3;
     }
     for (auto *r : recs) { r->stream = s; r->solved = true; }

@@ -34,7 +34,7 @@ namespace rb {
 // loads of RB_VU strided elements before using them, so each thread keeps that many memory
 // requests in flight instead of one.
 // ------------------------------------------------------------------------------------------
-#define RB_VU 16  // elements per thread whose loads are in flight together in a vector loop
+#define RB_VU 8  // elements per thread whose loads are in flight together in a vector loop
 #define RB_VLOOP(t, N, LOAD, USE)                                                          \
     {                                                                                      \
         const long long T_ = (t).size();                                                   \
@@ -65,6 +65,24 @@ namespace rb {
                 if (q < p1_) { LOAD }                                                      \
             }                                                                              \
             _Pragma("unroll") for (int u_ = 0; u_ < RB_VU2; u_++) {                        \
+                const long long q = b_ + u_ * blockDim.x;                                  \
+                if (q < p1_) { USE }                                                       \
+            }                                                                              \
+        }                                                                                  \
+    }
+// the same with D pairs in flight per thread (loops over three or four vectors use fewer, so that
+// their values and addresses stay in registers)
+#define RB_VPAIRS_D(t, NP, D, LOAD, USE)                                                    \
+    {                                                                                      \
+        const long long np_ = (NP);                                                        \
+        const long long p1_ = np_ * ((t).crank + 1) / (t).ncta;                            \
+        for (long long b_ = np_ * (t).crank / (t).ncta + threadIdx.x; b_ < p1_;           \
+             b_ += (D) * blockDim.x) {                                                     \
+            _Pragma("unroll") for (int u_ = 0; u_ < (D); u_++) {                           \
+                const long long q = b_ + u_ * blockDim.x;                                  \
+                if (q < p1_) { LOAD }                                                      \
+            }                                                                              \
+            _Pragma("unroll") for (int u_ = 0; u_ < (D); u_++) {                           \
                 const long long q = b_ + u_ * blockDim.x;                                  \
                 if (q < p1_) { USE }                                                       \
             }                                                                              \
@@ -639,12 +657,16 @@ template <> struct Vec4<float> {
 template <typename T, class TX, class Team, class Scale, class Pre, class Store>
 __device__ void team_product(Team &t, GroupShared &gs, const ProductArgs<TX> &a, Scale scale, Pre pre, Store store) {
     constexpr int KC = 16;
-    constexpr int EA = (KC * 64 + RB_THREADS - 1) / RB_THREADS;   // operator elements per thread
+    constexpr int EA = (KC * 128 + RB_THREADS - 1) / RB_THREADS;  // operator elements per thread
     constexpr int EX = (KC * 128 + RB_THREADS - 1) / RB_THREADS;  // column elements per thread
+    // row tiles: the operator's rows split evenly into tiles of at most 128 (a multiple of 4), so
+    // an 80-row operator is one tile of 80 rows, not 64 + 16
     const int ni4 = (a.ni + 3) & ~3;
-    const int TR = ni4 < 64 ? ni4 : 64;
-    int TC = (4096 / TR) & ~3;  // a multiple of 4: the 4-column blocks stay 16-byte aligned
+    const int nrb0 = (ni4 + 127) / 128;
+    const int TR = ((ni4 + nrb0 - 1) / nrb0 + 3) & ~3;
+    int TC = (RB_THREADS / (TR / 4)) * 4;  // every thread owns a 4×4 block
     if (TC > 128) TC = 128;
+    if ((TC + 4) * 16 + TR * 16 > (int)(RB_TILE_DOUBLES * sizeof(double) / sizeof(T))) TC = 64;
     const int nrb = (a.ni + TR - 1) / TR;
     const long long ncb = (a.ncol + TC - 1) / TC;
     const int nk = a.nk, nkt = a.B ? 2 * a.nk : a.nk;

@@ -61,7 +61,9 @@ struct Solver {
                 return;
             }
         }
-        if constexpr (!LO) {
+        if constexpr (std::is_same<Team, GridTeam>::value) {  // the grid team runs 2D/3D problems only
+            pass_md(t, P, gs, local, local_bytes, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
+        } else if constexpr (!LO) {
             if (P.ndims == 1) pass1d(t, P, gs, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
             else pass_md(t, P, gs, local, local_bytes, zin, out, homog, mv, ig, phiE_in, phiE_out, mixed);
         }
@@ -72,7 +74,7 @@ struct Solver {
     __device__ double norm(const double *a) { return sqrt(vdot(t, a, a, P.nstate)); }
 
     // ---------------------------------------------------------------- livolant (and "none")
-    __device__ SolveStat livolant(double *z, int maxit, double tol, int period) {
+    __device__ __noinline__ SolveStat livolant(double *z, int maxit, double tol, int period) {
         const long long N = P.nstate;
         double *g = vec(1), *z1 = vec(3), *z0 = vec(4);
         int nhist = 0, iter = 0, conv = 0;
@@ -118,7 +120,7 @@ struct Solver {
     }
 
     // ---------------------------------------------------------------- anderson (β = 1)
-    __device__ SolveStat anderson(double *z, int depth, int maxit, double tol) {
+    __device__ __noinline__ SolveStat anderson(double *z, int depth, int maxit, double tol) {
         const long long N = P.nstate;
         const int m = depth > 1 ? depth : 1;
         double *g = vec(1), *f = vec(2), *fo = vec(3), *go = vec(4);
@@ -260,7 +262,7 @@ struct Solver {
     }
 
     // ---------------------------------------------------------------- gmres(m)
-    __device__ SolveStat gmres(double *z, const double *rhs, int restart, int maxit, double tol) {
+    __device__ __noinline__ SolveStat gmres(double *z, const double *rhs, int restart, int maxit, double tol) {
         const long long N = P.nstate, N2 = P.vstride / 2;  // elements, pairs
         const int m = restart > 1 ? restart : 1;
         SolveStat st = {0, 0.0, 1, CUDART_NAN};
@@ -402,20 +404,27 @@ struct Solver {
     }
 
     // ---------------------------------------------------------------- bicgstab
-    __device__ SolveStat bicgstab(double *z, const double *rhs, int maxit, double tol) {
-        const long long N = P.nstate;
+    // Vector loops over 16-byte element pairs of CTA-contiguous slices (the pad element of an odd
+    // state stays zero in every vector): 8 pairs in flight per thread over two vectors, 4 over
+    // three or four.
+    __device__ __noinline__ SolveStat bicgstab(double *z, const double *rhs, int maxit, double tol) {
+        const long long N = P.nstate, N2 = P.vstride / 2;
         SolveStat st = {0, 0.0, 1, CUDART_NAN};
-        const double bnorm = norm(rhs);
+        const double bnorm = sqrt(vdot2(t, rhs, rhs, N2));
         if (bnorm == 0.0) { vzero(t, z, N); return st; }
         double *r = vec(2), *rh = vec(3), *p = vec(4), *v = vec(5), *s = vec(6), *tt = vec(7);
+        double2 *r2 = RB_D2(r), *rh2 = RB_D2(rh), *p2 = RB_D2(p), *v2 = RB_D2(v), *s2 = RB_D2(s), *z2 = RB_D2(z);
+        const double2 *c2 = RB_CD2(rhs), *t2 = RB_CD2(tt);
+        const double2 zero2 = make_double2(0.0, 0.0);
         matvec(r, z);
         double a1[1] = {0.0};
         {
-            double xc[RB_VU], xr[RB_VU];
-            RB_VLOOP(t, N, { xc[u_] = rhs[q]; xr[u_] = r[q]; }, {
-                const double ri = xc[u_] - xr[u_];
-                r[q] = ri; rh[q] = ri; p[q] = 0.0; v[q] = 0.0;
-                a1[0] += ri * ri;
+            double2 xc[RB_VU2], xr[RB_VU2];
+            RB_VPAIRS(t, N2, { xc[u_] = c2[q]; xr[u_] = r2[q]; }, {
+                const double2 ri = make_double2(xc[u_].x - xr[u_].x, xc[u_].y - xr[u_].y);
+                r2[q] = ri; rh2[q] = ri; p2[q] = zero2; v2[q] = zero2;
+                a1[0] += ri.x * ri.x;
+                a1[0] += ri.y * ri.y;
             })
         }
         t.template sumk<1>(a1);
@@ -425,26 +434,29 @@ struct Solver {
         double rho_old = 1.0, alpha = 1.0, omega = 1.0;
         const double tiny = 1e-300;
         while (iter < maxit) {
-            const double rho_new = vdot(t, rh, r, N);
+            const double rho_new = vdot2(t, rh, r, N2);
             if (fabs(rho_new) < tiny) break;
             const double beta = (rho_new / rho_old) * (alpha / omega);
             {
-                double xr[RB_VU], xp[RB_VU], xv[RB_VU];
-                RB_VLOOP(t, N, { xr[u_] = r[q]; xp[u_] = p[q]; xv[u_] = v[q]; },
-                         { p[q] = xr[u_] + 1.0 * (beta * (xp[u_] + (-omega) * xv[u_])); })
+                double2 xr[4], xp[4], xv[4];
+                RB_VPAIRS_D(t, N2, 4, { xr[u_] = r2[q]; xp[u_] = p2[q]; xv[u_] = v2[q]; }, {
+                    p2[q] = make_double2(xr[u_].x + 1.0 * (beta * (xp[u_].x + (-omega) * xv[u_].x)),
+                                         xr[u_].y + 1.0 * (beta * (xp[u_].y + (-omega) * xv[u_].y)));
+                })
             }
             t.sync();
             matvec(v, p); iter++;
-            const double denom = vdot(t, rh, v, N);
+            const double denom = vdot2(t, rh, v, N2);
             if (fabs(denom) < tiny) break;
             alpha = rho_new / denom;
             double a2[1] = {0.0};
             {
-                double xr[RB_VU], xv[RB_VU];
-                RB_VLOOP(t, N, { xr[u_] = r[q]; xv[u_] = v[q]; }, {
-                    const double si = xr[u_] + (-alpha) * xv[u_];
-                    s[q] = si;
-                    a2[0] += si * si;
+                double2 xr[RB_VU2], xv[RB_VU2];
+                RB_VPAIRS(t, N2, { xr[u_] = r2[q]; xv[u_] = v2[q]; }, {
+                    const double2 si = make_double2(xr[u_].x + (-alpha) * xv[u_].x, xr[u_].y + (-alpha) * xv[u_].y);
+                    s2[q] = si;
+                    a2[0] += si.x * si.x;
+                    a2[0] += si.y * si.y;
                 })
             }
             t.template sumk<1>(a2);
@@ -458,10 +470,12 @@ struct Solver {
             matvec(tt, s); iter++;
             double a3[2] = {0.0, 0.0};
             {
-                double xt[RB_VU], xs[RB_VU];
-                RB_VLOOP(t, N, { xt[u_] = tt[q]; xs[u_] = s[q]; }, {
-                    a3[0] += xt[u_] * xt[u_];
-                    a3[1] += xt[u_] * xs[u_];
+                double2 xt[RB_VU2], xs[RB_VU2];
+                RB_VPAIRS(t, N2, { xt[u_] = t2[q]; xs[u_] = s2[q]; }, {
+                    a3[0] += xt[u_].x * xt[u_].x;
+                    a3[0] += xt[u_].y * xt[u_].y;
+                    a3[1] += xt[u_].x * xs[u_].x;
+                    a3[1] += xt[u_].y * xs[u_].y;
                 })
             }
             t.template sumk<2>(a3);
@@ -469,12 +483,14 @@ struct Solver {
             omega = a3[1] / a3[0];
             double a4[1] = {0.0};
             {
-                double xz[RB_VU], xp[RB_VU], xs[RB_VU], xt[RB_VU];
-                RB_VLOOP(t, N, { xz[u_] = z[q]; xp[u_] = p[q]; xs[u_] = s[q]; xt[u_] = tt[q]; }, {
-                    z[q] = (xz[u_] + alpha * xp[u_]) + omega * xs[u_];
-                    const double ri = xs[u_] + (-omega) * xt[u_];
-                    r[q] = ri;
-                    a4[0] += ri * ri;
+                double2 xz[4], xp[4], xs[4], xt[4];
+                RB_VPAIRS_D(t, N2, 4, { xz[u_] = z2[q]; xp[u_] = p2[q]; xs[u_] = s2[q]; xt[u_] = t2[q]; }, {
+                    z2[q] = make_double2((xz[u_].x + alpha * xp[u_].x) + omega * xs[u_].x,
+                                         (xz[u_].y + alpha * xp[u_].y) + omega * xs[u_].y);
+                    const double2 ri = make_double2(xs[u_].x + (-omega) * xt[u_].x, xs[u_].y + (-omega) * xt[u_].y);
+                    r2[q] = ri;
+                    a4[0] += ri.x * ri.x;
+                    a4[0] += ri.y * ri.y;
                 })
             }
             t.template sumk<1>(a4);
@@ -488,7 +504,7 @@ struct Solver {
     }
 
     // ---------------------------------------------------------------- sn_one_speed
-    __device__ SolveStat one_speed(double *flux_g) {
+    __device__ __noinline__ SolveStat one_speed(double *flux_g) {
         const long long N = P.nstate, nphi = P.nphi;
         const long long nE = (long long)P.nd * P.nm4 * P.ncell;
         // zero-source short-circuit (sn_one_speed.jl:115-120)
@@ -635,10 +651,12 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, voi
             for (long long i = t.rank(); i < nE; i += t.size()) phiE_in[i] = phiE_in[i] * r1 / r0;
         }
         t.sync();
-        if (LO || local_ok) {
-            Local1D L(P, t.crank, t.ncta, local);
-            local1d_group_setup(P, L);
-            local1d_factor_fixed(P, gs, L);
+        if constexpr (std::is_same<Team, ClusterTeam>::value) {
+            if (LO || local_ok) {
+                Local1D L(P, t.crank, t.ncta, local);
+                local1d_group_setup(P, L);
+                local1d_factor_fixed(P, gs, L);
+            }
         }
         // Mn·Qlout into ψ, then kept as Qnout for the passes of this group
         m2d_tiles(t, P, gs, P.qlout, nullptr, 0);

@@ -57,10 +57,20 @@ __device__ __forceinline__ bool one_moment_md(const DevProblem &P) {
 template <typename R> struct OctDB { static constexpr int value = 10; };  // FP64: registers
 template <> struct OctDB<float> { static constexpr int value = 12; };
 
-// Shared memory the 3D octant sweep needs (bytes): direction constants and z-face buffers.
-template <typename R>
+#define RB_OCT_NB 2  // stages of the angular source (cp.async, one step ahead)
+
+// Shared memory the 3D octant sweep needs (bytes): direction constants, z-face buffers, RB_OCT_NB
+// stages of the angular flux of one step's cells (and of the energy-face flux, CSD), the cells'
+// materials, and each pencil's cell base and depth.
+template <typename R, bool CSD>
 __host__ __device__ constexpr long long oct3d_smem() {
-    return (long long)sizeof(R) * (OctDB<R>::value * 9 + 2 * OctDB<R>::value * RB_OCT_TILE * RB_OCT_TILE);
+    constexpr long long DB = OctDB<R>::value, TP = RB_OCT_TILE * RB_OCT_TILE, NB = RB_OCT_NB;
+    return (long long)sizeof(R) * (DB * 9 + 2 * DB * TP) + NB * TP * DB * (long long)sizeof(R) +
+           (CSD ? NB * TP * DB * 8 : 0) + TP * 8 + NB * TP * 4 + TP * 4;
+}
+__host__ __device__ constexpr long long oct3d_smem_max() {
+    return oct3d_smem<double, true>() > oct3d_smem<float, true>() ? oct3d_smem<double, true>()
+                                                                  : oct3d_smem<float, true>();
 }
 
 // Tile height in y: a power of two up to RB_OCT_TILE, so that a pencil's lower neighbour is the
@@ -76,13 +86,26 @@ __device__ __forceinline__ bool oct3d_ok(const DevProblem &P, int ncta, long lon
     if (P.ndims != 3 || !one_moment_md(P)) return false;
     const int TY = oct_ty(P.ny), TZ = min(P.nz, RB_OCT_TILE);
     const int ntiles = ((P.ny + TY - 1) / TY) * ((P.nz + TZ - 1) / TZ);
-    return ntiles <= ncta && smem_bytes >= (mixed ? oct3d_smem<float>() : oct3d_smem<double>());
+    const long long need = mixed ? (P.csd ? oct3d_smem<float, true>() : oct3d_smem<float, false>())
+                                 : (P.csd ? oct3d_smem<double, true>() : oct3d_smem<double, false>());
+    return ntiles <= ncta && smem_bytes >= need;
 }
+
+// asynchronous global -> shared copies (cp.async, L1-allocating), and their groups
+template <int B>
+__device__ __forceinline__ void cp_async(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src),
+                 "n"(B)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <typename R, typename PS, bool CSD, class Team>
 __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShared &gs, void *smem, const double *zin,
-                            int np_source, const double *phiE_in, double *phiE_out, int ig, PS *psi) {
-    constexpr int DB = OctDB<R>::value, K = RB_OCT_K, TP = RB_OCT_TILE * RB_OCT_TILE;
+                                         int np_source, const double *phiE_in, double *phiE_out, int ig, PS *psi) {
+    constexpr int DB = OctDB<R>::value, K = RB_OCT_K, TP = RB_OCT_TILE * RB_OCT_TILE, NB = RB_OCT_NB;
     const int nd = P.nd, nx = P.nx, ny = P.ny, nz = P.nz, nfm = P.nfmax;
     const int TY = oct_ty(ny), TZ = min(nz, RB_OCT_TILE);
     const int nty = (ny + TY - 1) / TY, ntz = (nz + TZ - 1) / TZ, ntiles = nty * ntz;
@@ -92,14 +115,21 @@ __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShar
     const int H = 1 + (max(TY, TZ) - 1 + K - 1) / K;  // stages per tile hop
     const int nsteps = nx + TY + TZ - 2;
     const int nstage = (nsteps + K - 1) / K + H * (nty - 1 + ntz - 1);
-    // per-direction scratch (md_scratch_stride): exits x [ny·nz], y [nx·nz], z [nx·ny], then the
-    // z-face plane [nx·ny] and the y-face plane [nx·nz] handed between tiles
+    // per-direction scratch (md_scratch_stride): exits x [ny·nz], y [nx·nz], z [nx·ny], the
+    // z-face plane [nx·ny] and the y-face plane [nx·nz] handed between tiles, then the incoming
+    // boundary fluxes (boundary_in_phase)
     const long long sstride = md_scratch_stride(P);
     const long long eyo = (long long)ny * nz * nfm, ezo = eyo + (long long)nx * nz * nfm;
     const long long zoff = ezo + (long long)nx * ny * nfm, yoff = zoff + (long long)nx * ny * nfm;
     const long long xin = md_in_offset(P, 0), yin = md_in_offset(P, 1), zin_ = md_in_offset(P, 2);
+    // shared memory (oct3d_smem)
     R *dc = reinterpret_cast<R *>(smem);  // [DB][9]: |cos|·G (3), |cos|·Gsrc (3), Gout (3)
     R *sfz = dc + DB * 9;                  // [2][DB][TP]
+    PS *qb = reinterpret_cast<PS *>(sfz + 2 * DB * TP);                  // [NB][TP][DB] angular source / flux
+    double *eb = reinterpret_cast<double *>(qb + NB * TP * DB);          // [NB][TP][DB] energy-face flux
+    long long *pcb = reinterpret_cast<long long *>(eb + (CSD ? NB * TP * DB : 0));  // [TP] cell base, −1: none
+    int *mb = reinterpret_cast<int *>(pcb + TP);  // [NB][TP] material of the pencil's cell
+    int *pjs = mb + NB * TP;                      // [TP] jy + jz
     const int me = threadIdx.x, jy = me % TY, jz = me / TY;
     const R w1x = (R)P.w1[0], w1y = (R)P.w1[1], w1z = (R)P.w1[2], w1e = (R)P.w1[3];
     const R esa = CSD ? (R)P.EsA[0] : R(0), esb = CSD ? (R)P.EsB[0] : R(0), eout = CSD ? (R)P.Eout[0] : R(0);
@@ -125,58 +155,65 @@ __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShar
                 dc[me * 9 + 6 + a] = (R)P.Gout[blk * nfm];
             }
         }
-        __syncthreads();
-        const R idy = pok ? (R)(1.0 / P.dy[iy]) : R(0), idz = pok ? (R)(1.0 / P.dz[iz]) : R(0);
-        R fxs[DB], fyl[DB], qp[DB], fep[DB];
-        int mp = 0;
-        R idxp = R(0);
-#pragma unroll
-        for (int k = 0; k < DB; k++) { fxs[k] = fyl[k] = qp[k] = fep[k] = R(0); }
-        if (pok) {  // the inputs of the pencil's first cell; the later ones are loaded a step ahead
-            const int ix0 = fx ? 0 : nx - 1;
-            const long long c0 = ix0 + (long long)nx * (iy + (long long)ny * iz);
-            const PS *pq = psi + first + (long long)nd * c0;
-#pragma unroll
-            for (int k = 0; k < DB; k++) qp[k] = k < cnt ? (R)pq[k] : R(0);
-            if (CSD && phiE_in) {
-#pragma unroll
-                for (int k = 0; k < DB; k++) fep[k] = k < cnt ? (R)phiE_in[first + k + (long long)nd * c0] : R(0);
-            }
-            mp = P.mat[c0];
-            idxp = (R)(1.0 / P.dx[ix0]);
+        if (me < TP) {
+            pcb[me] = pok ? (long long)nx * (iy + (long long)ny * iz) : -1;
+            pjs[me] = jy + jz;
         }
+        __syncthreads();
+        // Step sg's cells are staged cooperatively: element e = me + TP·r (r < cnt) of the step
+        // is direction k = e % cnt of pencil p = e / cnt, so consecutive lanes read consecutive
+        // directions of a cell (one contiguous run of cnt values per cell) instead of one lane
+        // per cell.
+        const int qd = cnt > 0 ? TP / cnt : 0, rm = cnt > 0 ? TP % cnt : 0;
+        const int p0 = cnt > 0 ? me / cnt : 0, k0 = cnt > 0 ? me % cnt : 0;
+        auto cell_of = [&](int p, int sg) -> long long {  // cell of pencil p at step sg, −1 if none
+            const long long cb = pcb[p];
+            const int ixx = sg - pjs[p];
+            if (cb < 0 || ixx < 0 || ixx >= nx) return -1;
+            return cb + (fx ? ixx : nx - 1 - ixx);
+        };
+        auto issue = [&](int sg) {  // step sg's cells into buffer sg % NB (one commit group)
+            if (cnt > 0 && sg >= 0 && sg < nsteps) {
+                const int st = sg % NB;
+                int p = p0, k = k0;
+                for (int r = 0; r < cnt; r++) {
+                    const long long c = cell_of(p, sg);
+                    if (c >= 0) {
+                        cp_async<sizeof(PS)>(qb + ((long long)st * TP + p) * DB + k, psi + first + k + (long long)nd * c);
+                        if (CSD && phiE_in)
+                            cp_async<8>(eb + ((long long)st * TP + p) * DB + k, phiE_in + first + k + (long long)nd * c);
+                    }
+                    p += qd;
+                    k += rm;
+                    if (k >= cnt) { k -= cnt; p++; }
+                }
+                if (me < TP) {
+                    const long long c = cell_of(me, sg);
+                    if (c >= 0) cp_async<4>(mb + st * TP + me, P.mat + c);
+                }
+            }
+            cp_async_commit();
+        };
+        const R idy = pok ? (R)(1.0 / P.dy[iy]) : R(0), idz = pok ? (R)(1.0 / P.dz[iz]) : R(0);
+        R fxs[DB], fyl[DB];
+#pragma unroll
+        for (int k = 0; k < DB; k++) fxs[k] = fyl[k] = R(0);
+        issue(0);
         for (int st = 0; st < nstage; st++) {
             const int s0 = (st - dly) * K;
             for (int u = 0; u < K; u++) {
                 const int sg = s0 + u;
                 if (cnt == 0 || sg < 0 || sg >= nsteps) continue;  // uniform over the CTA
+                cp_async_wait<0>();  // this thread's copies of step sg have landed
+                __syncthreads();     // everyone's, and step sg − 1's buffer is free again
+                issue(sg + 1);       // in flight while step sg is solved
                 const int ixx = sg - jy - jz;
-                const int rd = (sg + 1) & 1, wr = sg & 1;
+                const int rd = (sg + 1) & 1, wr = sg & 1, sb = sg % NB;
                 R fyi[DB];
 #pragma unroll
                 for (int k = 0; k < DB; k++) fyi[k] = __shfl_up_sync(0xffffffffu, fyl[k], 1);
-                // the next cell's inputs, in flight while this cell is solved
-                R qn[DB], fen[DB];
-                int mn_ = 0;
-                R idxn = R(0);
-                const bool nxt = pok && ixx >= 0 && ixx + 1 < nx;
-                if (nxt) {
-                    const int ixn = fx ? ixx + 1 : nx - 2 - ixx;
-                    const long long cn = ixn + (long long)nx * (iy + (long long)ny * iz);
-                    const PS *pq = psi + first + (long long)nd * cn;
-#pragma unroll
-                    for (int k = 0; k < DB; k++) qn[k] = k < cnt ? (R)pq[k] : R(0);
-                    if (CSD) {
-                        const double *pe = phiE_in ? phiE_in + first + (long long)nd * cn : nullptr;
-#pragma unroll
-                        for (int k = 0; k < DB; k++) fen[k] = (pe && k < cnt) ? (R)pe[k] : R(0);
-                    }
-                    mn_ = P.mat[cn];
-                    idxn = (R)(1.0 / P.dx[ixn]);
-                }
                 if (pok && ixx >= 0 && ixx < nx) {
                     const int ix = fx ? ixx : nx - 1 - ixx;
-                    const long long c = ix + (long long)nx * (iy + (long long)ny * iz);
                     const long long yk = (ix + (long long)nx * iz) * nfm, zk = (ix + (long long)nx * iy) * nfm;
                     R fzi[DB];
                     // faces entering the pencil: the domain's incoming fluxes (boundary_in_phase),
@@ -199,58 +236,76 @@ __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShar
 #pragma unroll
                         for (int k = 0; k < DB; k++) fzi[k] = sfz[(rd * DB + k) * TP + me - TY];
                     }
-                    const int m = mp;
+                    const int m = mb[sb * TP + me];
                     const R sigt = (R)gs.sigt[m];
                     R scs = R(0), srcE = R(0);
                     if (CSD) {
                         scs = (R)P.scsd[m];
                         srcE = esa * (R)gs.sp[m] - esb * (R)gs.sm[m];
                     }
-                    const R idx = idxp;
-                    PS *pc = psi + first + (long long)nd * c;
+                    const R idx = (R)(1.0 / P.dx[ix]);
+                    PS *qc = qb + ((long long)sb * TP + me) * DB;
+                    double *ec = eb + ((long long)sb * TP + me) * DB;
 #pragma unroll
                     for (int k = 0; k < DB; k++) {
-                        if (k >= cnt) break;
+                        if (k >= cnt) continue;
                         const R *d = dc + k * 9;
+                        const R fe = (CSD && phiE_in) ? (R)ec[k] : R(0);
                         const R S = (scs + sigt) + d[0] * idx + d[1] * idy + d[2] * idz;
-                        R q = qp[k] + (d[3] * idx) * fxs[k] + (d[4] * idy) * fyi[k] + (d[5] * idz) * fzi[k];
-                        if (CSD) q -= srcE * fep[k];
+                        R q = (R)qc[k] + (d[3] * idx) * fxs[k] + (d[4] * idy) * fyi[k] + (d[5] * idz) * fzi[k];
+                        if (CSD) q -= srcE * fe;
                         const R v = q / S;
                         fxs[k] = w1x * fxs[k] + d[6] * v;
                         fyi[k] = w1y * fyi[k] + d[7] * v;
                         fzi[k] = w1z * fzi[k] + d[8] * v;
-                        pc[k] = (PS)v;
-                        if (CSD) phiE_out[first + k + (long long)nd * c] = (double)(w1e * fep[k] + eout * v);
+                        qc[k] = (PS)v;
+                        if (CSD) ec[k] = (double)(w1e * fe + eout * v);
                         sfz[(wr * DB + k) * TP + me] = fzi[k];
                     }
-                    // faces leaving the tile or the domain
+                    // faces leaving the tile or the domain (loops over the compile-time DB keep
+                    // the per-direction arrays in registers)
                     if (jy == TY - 1 || iyy == ny - 1) {
                         const long long off = iyy < ny - 1 ? yoff : eyo;
-                        for (int k = 0; k < cnt; k++) P.fexit[(long long)(first + k) * sstride + off + yk] = (double)fyi[k];
+#pragma unroll
+                        for (int k = 0; k < DB; k++)
+                            if (k < cnt) P.fexit[(long long)(first + k) * sstride + off + yk] = (double)fyi[k];
                     }
                     if (jz == TZ - 1 || izz == nz - 1) {
                         const long long off = izz < nz - 1 ? zoff : ezo;
-                        for (int k = 0; k < cnt; k++) P.fexit[(long long)(first + k) * sstride + off + zk] = (double)fzi[k];
+#pragma unroll
+                        for (int k = 0; k < DB; k++)
+                            if (k < cnt) P.fexit[(long long)(first + k) * sstride + off + zk] = (double)fzi[k];
                     }
-                    if (ixx == nx - 1)
-                        for (int k = 0; k < cnt; k++)
-                            P.fexit[(long long)(first + k) * sstride + (iy + (long long)ny * iz) * nfm] = (double)fxs[k];
+                    if (ixx == nx - 1) {
+                        const long long o = (iy + (long long)ny * iz) * nfm;
+#pragma unroll
+                        for (int k = 0; k < DB; k++)
+                            if (k < cnt) P.fexit[(long long)(first + k) * sstride + o] = (double)fxs[k];
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < DB; k++) fyl[k] = fyi[k];
-                if (nxt) {
-#pragma unroll
-                    for (int k = 0; k < DB; k++) {
-                        qp[k] = qn[k];
-                        if (CSD) fep[k] = fen[k];
-                    }
-                    mp = mn_;
-                    idxp = idxn;
-                }
                 __syncthreads();
+                // the step's angular flux (and outgoing energy-face flux) back to global memory,
+                // consecutive lanes on consecutive directions of a cell
+                {
+                    int p = p0, k = k0;
+                    for (int r = 0; r < cnt; r++) {
+                        const long long c = cell_of(p, sg);
+                        if (c >= 0) {
+                            psi[first + k + (long long)nd * c] = qb[((long long)sb * TP + p) * DB + k];
+                            if (CSD) phiE_out[first + k + (long long)nd * c] = eb[((long long)sb * TP + p) * DB + k];
+                        }
+                        p += qd;
+                        k += rm;
+                        if (k >= cnt) { k -= cnt; p++; }
+                    }
+                }
             }
             t.sync();
         }
+        cp_async_wait<0>();
+        __syncthreads();
     }
 }
 

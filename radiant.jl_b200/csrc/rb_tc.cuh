@@ -127,7 +127,8 @@ __host__ __device__ constexpr long long stage_bytes(int parts, int mtiles, int n
 
 // C[i, col] = Σ_k A_p[i,k]·B_b(p)[k,col] for every operator part p (b(p) = min(p, nb−1)) over
 // column tiles of N columns dealt to the team's CTAs; B_0[k,col] = scale0(k,col)·X[k + ldx·col],
-// B_1[k,col] = X[k + ldx·col]. epi(i, col, acc_part0, acc_part1) stores row i of column col.
+// B_1[k,col] = X[k + ldx·col]. The epilogue object provides pre(i, col) (the term added to the
+// product), scale(col) (the factor of part 1) and store(i, col, acc0 + scale·acc1, pre).
 // opA: packed operator, block (p, mtile, kchunk) at ((p·mtiles + m)·kchunks + kc)·2·RB_TC_BLOCK
 // floats (hi block, then lo). Returns false (without touching any output) if it does not fit.
 template <int N, class TX, class Team, class Scale, class Epi>
@@ -142,7 +143,11 @@ __device__ bool tc_product(Team &t, TcState &ts, unsigned char *sm, long long sm
     float *sA = reinterpret_cast<float *>(sm);  // [parts·mtiles][hi,lo][RB_TC_BLOCK]
     float *sB = sA + (long long)parts * mtiles * 2 * RB_TC_BLOCK;  // [nb][hi,lo][N·32]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int k4 = tid >> 5;  // this thread's 4-deep K group of the chunk (0..7)
+    // B staging: a warp covers 8 columns × 16 K of each 32 columns (lanes 8·q..8·q+7 take the
+    // 4-deep K group k4 of 8 neighbouring columns), so a load instruction touches 8 columns'
+    // contiguous K runs and a quarter-warp stores 128 contiguous bytes
+    const int k4 = (lane >> 3) + 4 * (warp & 1);  // this thread's 4-deep K group of the chunk (0..7)
+    const int cw = (lane & 7) + 8 * (warp >> 1);   // its column inside each group of 32
     const long long ntile = (ncol + N - 1) / N;
     uint32_t ph = ts.phase;  // parity of the next MMA completion (identical in every thread)
     for (long long tl = t.crank; tl < ntile; tl += t.ncta) {
@@ -152,7 +157,7 @@ __device__ bool tc_product(Team &t, TcState &ts, unsigned char *sm, long long sm
             float xv[CPT][4], x0[CPT][4];
 #pragma unroll
             for (int j = 0; j < CPT; j++) {
-                const long long col = c0 + lane + 32 * j;
+                const long long col = c0 + cw + 32 * j;
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     const int k = kc * RB_TC_KC + 4 * k4 + e;
@@ -186,7 +191,7 @@ __device__ bool tc_product(Team &t, TcState &ts, unsigned char *sm, long long sm
                 float *hi = sB + (long long)b * 2 * N * RB_TC_KC, *lo = hi + N * RB_TC_KC;
 #pragma unroll
                 for (int j = 0; j < CPT; j++) {
-                    const int cl = lane + 32 * j;
+                    const int cl = cw + 32 * j;
                     float h[4], l[4];
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
@@ -243,12 +248,22 @@ __device__ bool tc_product(Team &t, TcState &ts, unsigned char *sm, long long sm
                 else
 #pragma unroll
                     for (int q = 0; q < 16; q++) a1[q] = 0.0f;
-                if (i < ni)
+                if (i < ni) {
+                    // every load the epilogue makes for the 16 outputs first, then the stores
+                    // (a store may alias those loads, so they are not interleaved)
+                    double pv[16], sv[16];
 #pragma unroll
                     for (int q = 0; q < 16; q++) {
                         const long long col = c0 + cbase + cc + q;
-                        if (col < ncol) epi(i, col, a0[q], a1[q]);
+                        pv[q] = col < ncol ? epi.pre(i, col) : 0.0;
+                        sv[q] = col < ncol ? epi.scale(col) : 0.0;
                     }
+#pragma unroll
+                    for (int q = 0; q < 16; q++) {
+                        const long long col = c0 + cbase + cc + q;
+                        if (col < ncol) epi.store(i, col, (double)a0[q] + sv[q] * (double)a1[q], pv[q]);
+                    }
+                }
             }
         }
         tc::fence_before();
@@ -273,11 +288,15 @@ __device__ bool m2d_tc(Team &t, const DevProblem &P, GroupShared &gs, TcState &t
     float *psi = P.psi32;
     const long long ncol = (long long)nm * P.ncell;
     auto sc = [=] __device__(int k, long long col) { return ys[(long long)mat[col / nm] * np + k]; };
-    auto epi = [=] __device__(int i, long long col, float a0, float a1) {
-        double v = (double)a0;
-        if (parts > 1) v += tg[mat[col / nm]] * (double)a1;
-        psi[col * nd + i] = (float)((add ? add[col * nd + i] : 0.0) + v);
-    };
+    struct {
+        const double *add, *tg;
+        const int *mat;
+        float *psi;
+        int nd, nm, parts;
+        __device__ double pre(int i, long long col) const { return add ? add[col * nd + i] : 0.0; }
+        __device__ double scale(long long col) const { return parts > 1 ? tg[mat[col / nm]] : 0.0; }
+        __device__ void store(int i, long long col, double v, double p) const { psi[col * nd + i] = (float)(p + v); }
+    } epi{add, tg, mat, psi, nd, nm, parts};
     unsigned char *sm = reinterpret_cast<unsigned char *>(smem);
     if (tc_product<128>(t, ts, sm, smem_bytes, P.tc_m2d, parts, nd, np, parts, zin, np, ncol, sc, epi, P.status))
         return true;
@@ -293,10 +312,14 @@ __device__ bool d2m_tc(Team &t, const DevProblem &P, TcState &ts, void *smem, lo
     const int nd = P.nd, np = P.np, nm = P.nm5;
     const long long ncol = (long long)nm * P.ncell;
     auto one = [] __device__(int, long long) { return 1.0; };
-    auto epi = [=] __device__(int i, long long col, float a0, float) {
-        const double v = (double)a0;
-        zout[col * np + i] = matvec ? zin[col * np + i] - v : v;
-    };
+    struct {
+        const double *zin;
+        double *zout;
+        int np, matvec;
+        __device__ double pre(int i, long long col) const { return matvec ? zin[col * np + i] : 0.0; }
+        __device__ double scale(long long) const { return 0.0; }
+        __device__ void store(int i, long long col, double v, double p) const { zout[col * np + i] = matvec ? p - v : v; }
+    } epi{zin, zout, np, matvec};
     unsigned char *sm = reinterpret_cast<unsigned char *>(smem);
     if (tc_product<128>(t, ts, sm, smem_bytes, P.tc_d2m, 1, np, nd, 1, P.psi32, nd, ncol, one, epi, P.status))
         return true;
