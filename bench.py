@@ -1,27 +1,32 @@
 #!/usr/bin/env python
 """Benchmark of the SN transport solve: cell-direction-group updates per second.
 
-Workload (one step): a batch of independent 1D slab coupled-BFP particle solves with the
-shapes of the 1D coupled Boltzmann Fokker-Planck configuration -- water 0-3 cm / cortical
-bone 3-5 cm / water 5-15 cm, 300 voxels, 80 log groups 1 keV-20 MeV, S32 Gauss-Legendre,
-P15, linear DG in x (and in E for the charged particles), Galerkin angular Fokker-Planck,
-normal beam in the 6 MeV group -- one photon (BTE), one electron (BFP) and one positron
-(BFP) solve per seed, `--seeds` seeds. Cross sections are seeded synthetic tables with the
-configuration's shapes (the reference's physics generator is not available here).
+Headline workload (one step; --workload c4, the default): the 3D Cartesian photon-electron
+configuration -- 64^3 voxels over a 16 cm cube, water with a seeded 16^3-voxel bone block,
+40 photon + 40 electron groups (10 keV - 6 MeV), level-symmetric S8 (80 directions, Galerkin
+basis: 80 moments), P3, diamond difference, reflective Z-, isotropic volume source in the top
+group inside the central 8^3 voxels, BiCGStab to 1e-6 -- in the configuration's mixed form
+(FP32 sweeps, split-TF32 tensor-core moment products, FP64 Krylov and defect correction): the
+photon and the electron solve of one seed per GPU, each on the whole GPU (one cooperative
+launch per problem). The plain FP64 form of the same problems runs beside it, with the mixed
+form's error against it. Cross sections are seeded synthetic tables with the configuration's
+shapes (the reference's physics generator is not available here).
 
-  value  updates/s over the batch, inputs resident in HBM, one persistent launch per step
+  value  updates/s of the step, inputs resident in HBM
   e2e    the same through the C ABI with host buffers: upload (H2D) + solve + download (D2H)
   unit   of work: one (cell, direction) visit inside one transport pass of one group;
-         updates = Σ passes × cells × directions, passes as counted by the reference.
+         updates = sum of passes x cells x directions, passes as the reference counts them.
 
-`--impl reference` times the oracle port of the reference's CPU solve (the reference is
-Julia, unavailable here) on all host cores over a bounded sample of the same workload.
+Second section: the 1D coupled-BFP batch (150 slab solves of the 1D configuration's shapes in
+one persistent launch), FP64 and mixed. Third: a bounded serving run.
+
+`--impl reference` times the oracle (the C restatement of the reference's Julia solve; Julia
+is not installed) on all host cores over a bounded sample of the same 3D workload.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import multiprocessing as mp
 import os
 import statistics
 import subprocess
@@ -36,18 +41,20 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "cell-dir-group updates/s"
-# DRAM bytes per update of solve_local1d_kernel, from one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum) of 18 electron solves of this workload reduced to 8 groups, FP64;
-# traffic grows in proportion to the updates, so a launch's traffic is this times its updates.
-TRAFFIC_BYTES_PER_UPDATE = 399.8
+# DRAM bytes per update of the workloads' dominant kernels, each from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of a reduced case; traffic grows in
+# proportion to the updates, so a launch's traffic is this times its updates:
+#   solve_local1d_kernel, 18 electron solves of the 1D batch reduced to 8 groups, FP64;
+#   solve_grid_kernel, the 3D photon problem reduced to one group, mixed and FP64 forms.
+TRAFFIC_BYTES_PER_UPDATE = {("c2", "fp64"): 399.8}
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
-def kernel_name(workload="c2"):
+def kernel_name(workload="c4"):
     """The persistent kernel the workload runs on: every 1D problem of the benchmark's workloads
     takes the local (cell-split) pass, whose batches run on their own kernel; a 3D problem runs on
     the whole GPU as one cooperative launch."""
-    if workload == "c4g1":
+    if workload in ("c4", "c4g1"):
         return "solve_grid_kernel"
     return "solve_batch_kernel" if os.environ.get("RB_LOCAL1D", "1") == "0" else "solve_local1d_kernel"
 
@@ -61,16 +68,22 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def workload_tables(seeds, precision, workload="c2"):
+def workload_tables(seeds, precision, workload="c4", groups=None):
     from radiant_b200 import workloads as W
 
     tabs = []
+    if workload in ("c4", "c4g1"):  # the 3D configuration: photon and electron solve per seed
+        ng = 1 if workload == "c4g1" else (groups or 40)
+        for s in seeds:
+            for part in ("photon", "electron"):
+                t = W.c4_tables(seed=s, particle=part, precision=precision, ng=ng)
+                t["particle"] = part
+                tabs.append(t)
+        return tabs
     if workload == "c1":  # small case (profiling): the 1D photon BTE slab, one solve per seed
         return [W.c1_tables(seed=s, precision=precision) for s in seeds]
     if workload == "c2e8":  # small case (profiling): the electron BFP solve of the workload, 8 groups
         return [W.c2_tables(seed=s, precision=precision, ng=8) for s in seeds]
-    if workload == "c4g1":  # small case (profiling): the C4-shaped 3D photon solve, one group
-        return [W.c4_tables(seed=s, ng=1) for s in seeds]
     for s in seeds:
         for part in ("photon", "electron", "positron"):
             t = W.c2_tables(seed=s * 3 + {"photon": 0, "electron": 1, "positron": 2}[part], precision=precision,
@@ -150,6 +163,51 @@ class ClockSampler:
 # ------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------
+def updates_of(rbs, tabs):
+    return sum(rb.passes * int(np.prod(t["ns"])) * t["nd"] for rb, t in zip(rbs, tabs))
+
+
+def deposition(tabs, rbs):
+    """Energy deposition summed over the particles (energy_deposition.jl:36-78), from the
+    downloaded fluxes through rb_energy_deposition."""
+    import ctypes as C
+
+    from radiant_b200._abi import load_library
+
+    lib = load_library()
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    tot = None
+    for t, rb in zip(tabs, rbs):
+        xs = t["xs"]
+        ncell = int(np.prod(t["ns"]))
+        mat = np.asfortranarray(t["mat"].astype(np.int32))
+        se, rho = np.asfortranarray(xs.sigma_e), np.asfortranarray(xs.density)
+        out = np.zeros(ncell)
+        cf = rb.flux_cutoff if t["solver_type"] >= 2 else None
+        st = lib.rb_energy_deposition(t["ng"], t["np"], t["nm"][4], ncell, t["nmat"], mat.ctypes.data_as(ip),
+                                      rb.flux.ctypes.data_as(dp), None if cf is None else cf.ctypes.data_as(dp),
+                                      se.ctypes.data_as(dp), rho.ctypes.data_as(dp), 1.0, out.ctypes.data_as(dp))
+        assert st == 0
+        tot = out if tot is None else tot + out
+    return tot
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+def time_steps(ctx, handles, sptr, stream, steps):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.solve_batch(handles, sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -158,7 +216,8 @@ def run_ours(args, rank, world):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     seeds = [1 + rank * 1000 + k for k in range(args.seeds)]
-    tabs = workload_tables(seeds, args.precision, args.workload)
+    prec = args.precision or ("mixed" if args.workload in ("c4", "c4g1") else "fp64")
+    tabs = workload_tables(seeds, prec, args.workload, args.groups)
     ctx = Context(dev, 0)
     packs = [PackedProblem(t) for t in tabs]
     handles = [ctx.upload(p) for p in packs]
@@ -167,38 +226,57 @@ def run_ours(args, rank, world):
     sptr = stream.cuda_stream
     rbs = [ResultBuffers(p) for p in packs]
 
-    def step():
-        ctx.solve_batch(handles, sptr)
-
     for _ in range(args.warmup):
-        step()
+        ctx.solve_batch(handles, sptr)
     torch.cuda.synchronize()
     # passes per problem (identical every step: the solve is deterministic)
     for h, rb in zip(handles, rbs):
         ctx.download(h, rb)
-    updates = sum(rb.passes * int(np.prod(t["ns"])) * t["nd"] for rb, t in zip(rbs, tabs))
-    abytes = sum(algorithmic_bytes(t, rb.passes, 8 if args.precision == "fp64" else 4) for rb, t in zip(rbs, tabs))
+    updates = updates_of(rbs, tabs)
+    w = 8 if prec == "fp64" else 4
+    abytes = sum(algorithmic_bytes(t, rb.passes, w) for rb, t in zip(rbs, tabs))
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+        ms = max_over_ranks(time_steps(ctx, handles, sptr, stream, args.steps), world)
     value = updates * world / (ms / 1e3)
+    for h in handles:
+        ctx.release(h)
+
+    # the plain FP64 form of the same problems (the drop-in), and the chosen form's error
+    # against it on the flux moments and on the energy deposition
+    plain = None
+    if prec != "fp64" and not args.no_fp64:
+        ftabs = workload_tables(seeds, "fp64", args.workload, args.groups)
+        fpacks = [PackedProblem(t) for t in ftabs]
+        fh = [ctx.upload(p) for p in fpacks]
+        ctx.solve_batch(fh, sptr)
+        torch.cuda.synchronize()
+        frbs = [ResultBuffers(p) for p in fpacks]
+        for h, rb in zip(fh, frbs):
+            ctx.download(h, rb)
+        fms = max_over_ranks(time_steps(ctx, fh, sptr, stream, max(1, min(args.steps, 2))), world)
+        for h in fh:
+            ctx.release(h)
+        fupd = updates_of(frbs, ftabs)
+        err_flux = max(rel_l2(a.flux, b.flux) for a, b in zip(rbs, frbs))
+        err_cut = max((rel_l2(a.flux_cutoff, b.flux_cutoff) for a, b, t in zip(rbs, frbs, tabs)
+                       if t["solver_type"] >= 2), default=0.0)
+        err_dep = rel_l2(deposition(tabs, rbs), deposition(ftabs, frbs)) if "xs" in tabs[0] else None
+        plain = {"value": fupd * world / (fms / 1e3), "unit": "updates/s", "ms_per_step": fms,
+                 "solves_per_s": len(ftabs) * world / (fms / 1e3), "passes": int(sum(rb.passes for rb in frbs)),
+                 "chosen_form_solves_per_s": len(tabs) * world / (ms / 1e3),
+                 "chosen_form_speedup_solves": fms / ms, "chosen_form_passes": int(sum(rb.passes for rb in rbs)),
+                 "chosen_form_max_rel_l2_flux": err_flux, "chosen_form_max_rel_l2_cutoff": err_cut,
+                 "chosen_form_rel_l2_energy_deposition": err_dep}
 
     # e2e through the C ABI with host buffers: upload + solve + download per step
     h2d = sum(p_bytes(t) for t in tabs)
     d2h = sum(rb.flux.nbytes + (rb.flux_cutoff.nbytes if rb.flux_cutoff is not None else 0)
               + rb.rho.nbytes + rb.group_iters.nbytes + rb.group_resid.nbytes + rb.group_converged.nbytes
               for rb in rbs)
-    for h in handles:
-        ctx.release(h)
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = max(5, args.steps)
 
     def e2e_step():
         hs = [ctx.upload(p) for p in packs]
@@ -218,65 +296,83 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, world)
 
-    # the mixed-precision form on the same batch (FP32 angular work, FP64 Krylov; 1e-5 contract)
-    mixed = None
-    if args.precision == "fp64" and not args.no_mixed:
-        mtabs = workload_tables(seeds, "mixed", args.workload)
-        mpacks = [PackedProblem(t) for t in mtabs]
-        mh = [ctx.upload(p) for p in mpacks]
-        for _ in range(max(1, args.warmup)):
-            ctx.solve_batch(mh, sptr)
-        torch.cuda.synchronize()
-        mrbs = [ResultBuffers(p) for p in mpacks]
-        for h, rb in zip(mh, mrbs):
-            ctx.download(h, rb)
-        mupd = sum(rb.passes * int(np.prod(t["ns"])) * t["nd"] for rb, t in zip(mrbs, mtabs))
-        err = max(float(np.linalg.norm(a.flux - b.flux) / max(np.linalg.norm(b.flux), 1e-300)) for a, b in zip(mrbs, rbs))
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            ctx.solve_batch(mh, sptr)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        mms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
-        for h in mh:
-            ctx.release(h)
-        mixed = {"value": mupd * world / (mms / 1e3), "unit": "updates/s", "ms_per_step": mms,
-                 "solves_per_s": len(mtabs) * world / (mms / 1e3), "fp64_solves_per_s": len(tabs) * world / (ms / 1e3),
-                 "max_rel_l2_vs_fp64": err, "passes": int(sum(rb.passes for rb in mrbs)),
-                 "fp64_passes": int(sum(rb.passes for rb in rbs))}
-
+    c2 = run_c2_section(args, ctx, sptr, stream, rank, world) if args.workload == "c4" and not args.no_c2 else None
     serving = run_serving(args, ctx, dev) if (args.serve > 0 and rank == 0) else None
     ctx.close()
 
     peak, pk = peaks()
     achieved = abytes / (ms / 1e3) / 1e9
+    tpu = TRAFFIC_BYTES_PER_UPDATE.get((args.workload, prec))
+    if args.workload == "c4":
+        cfg = {"workload": "3D 64^3 photon-electron: 16 cm water cube with a 16^3 bone block, 40+40 groups, "
+                           "S8 (80 directions, Galerkin 80 moments), P3, DD, reflective Z-, central 8^3 volume "
+                           f"source, BiCGStab 1e-6; photon + electron solve x {args.seeds} seed(s) per GPU",
+               "groups_per_particle": args.groups or 40, "problems_per_gpu": len(tabs), "precision": prec,
+               "l2": "per-step working set (flux, Krylov vectors, angular flux of each problem) exceeds the 126 MB L2",
+               "parallelism": f"replicas x{world}", "launches": "one cooperative launch per problem (whole GPU)"}
+    else:
+        cfg = {"workload": args.workload, "problems_per_gpu": len(tabs), "precision": prec,
+               "parallelism": f"replicas x{world}"}
     line = {
         "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32 sweep + tf32x3 tensor-core products + f64 Krylov",
         "data": "synthetic (seeded cross-section tables with the configuration's shapes)",
-        "config": {"workload": "1D slab coupled BFP: 300 voxels (water/bone/water), 80 groups, S32, P15, "
-                               "linear DG in x and E, Galerkin angular FP, 6 MeV beam; photon+electron+positron "
-                               f"solves x {args.seeds} seeds per GPU", "problems_per_gpu": len(tabs),
-                   "precision": args.precision, "accel": "gmres(30)", "tol": 1e-8,
-                   "l2": "per-step working set (flux + Krylov vectors of every problem) exceeds the 126 MB L2",
-                   "parallelism": f"replicas x{world}"},
+        "config": cfg,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
-                     "traffic": TRAFFIC_BYTES_PER_UPDATE * updates if args.workload == "c2" and args.precision == "fp64" else None,
-                     "traffic_note": "bytes per launch, scaled from an ncu capture of the reduced workload",
-                     "algorithmic_bytes": abytes, "peak_source": pk, "kernel": kernel_name(args.workload)},
+                     "traffic": tpu * updates / len(tabs) if tpu else None,
+                     "traffic_note": "DRAM bytes per launch, scaled from an ncu capture of the reduced case",
+                     "algorithmic_bytes_per_launch": abytes / len(tabs), "peak_source": pk,
+                     "kernel": kernel_name(args.workload)},
         "e2e": {"value": updates * world / (e2e_ms / 1e3), "unit": "updates/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
-        "gpu_launches": args.steps,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps},
+        "gpu_launches": args.steps * (len(tabs) if args.workload in ("c4", "c4g1") else 1),
         "clocks": clk.summary(),
     }
-    if mixed:
-        line["mixed_form"] = mixed
+    if plain:
+        line["plain_fp64_form"] = plain
+    if c2:
+        line["c2_batch"] = c2
     if serving:
         line["serving"] = serving
     return line
+
+
+def run_c2_section(args, ctx, sptr, stream, rank, world):
+    """The 1D coupled-BFP batch: 150 slab solves (photon BTE, electron and positron BFP; 300
+    voxels, 80 groups, S32, P15, linear DG in x and E) in one persistent launch, FP64 and mixed."""
+    from radiant_b200._abi import PackedProblem, ResultBuffers
+
+    seeds = [1 + rank * 1000 + k for k in range(50)]
+    out = {"workload": "1D slab coupled BFP (300 voxels, 80 groups, S32, P15, linear DG x and E, Galerkin FP, "
+                       "6 MeV beam): photon+electron+positron x 50 seeds, one persistent launch",
+           "kernel": kernel_name("c2")}
+    rbs_by = {}
+    for prec in ("fp64", "mixed"):
+        tabs = workload_tables(seeds, prec, "c2")
+        packs = [PackedProblem(t) for t in tabs]
+        hs = [ctx.upload(p) for p in packs]
+        ctx.solve_batch(hs, sptr)
+        import torch
+
+        torch.cuda.synchronize()
+        rbs = [ResultBuffers(p) for p in packs]
+        for h, rb in zip(hs, rbs):
+            ctx.download(h, rb)
+        ms = max_over_ranks(time_steps(ctx, hs, sptr, stream, 2), world)
+        for h in hs:
+            ctx.release(h)
+        upd = updates_of(rbs, tabs)
+        rbs_by[prec] = rbs
+        out[prec] = {"value": upd * world / (ms / 1e3), "unit": "updates/s", "ms_per_step": ms,
+                     "solves_per_s": len(tabs) * world / (ms / 1e3)}
+        if prec == "fp64":
+            ab = sum(algorithmic_bytes(t, rb.passes, 8) for rb, t in zip(rbs, tabs))
+            peak, pk = peaks()
+            out["fp64"]["roofline_frac"] = ab / (ms / 1e3) / 1e9 / peak
+    out["mixed"]["max_rel_l2_vs_fp64"] = max(rel_l2(a.flux, b.flux) for a, b in zip(rbs_by["mixed"], rbs_by["fp64"]))
+    return out
 
 
 def run_serving(args, ctx, dev):
@@ -334,57 +430,63 @@ def p_bytes(t):
 
 
 # ------------------------------------------------------------------------------------------
-# CPU legs (the oracle port of the reference's CPU solve)
+# CPU legs (the oracle: the C restatement of the reference's CPU solve, on all host cores)
 # ------------------------------------------------------------------------------------------
-def _cpu_one(args_):
-    seed, particle = args_
-    sys.path.insert(0, os.path.join(ROOT, "radiant.jl_b200"))
-    sys.path.insert(0, ROOT)
-    from oracle import run as orun
+CPU_SAMPLE_ITERS = 3
+
+
+def cpu_sample_tables():
+    """The bounded sample of the 3D workload the CPU legs time: the photon problem of the 3D
+    configuration (64^3, S8, 80 moments, reflective Z-, BiCGStab) reduced to one group and at
+    most CPU_SAMPLE_ITERS BiCGStab iterations: the same shapes, passes and per-update work."""
     from radiant_b200 import workloads as W
 
-    t = W.c2_tables(seed=seed, particle="photon" if particle == "photon" else "electron")
+    t = W.c4_tables(seed=1, particle="photon", ng=1)
+    t["max_iter"] = CPU_SAMPLE_ITERS
+    return t
+
+
+def cpu_sample(tabs):
+    from oracle import run as orun
+
     t0 = time.perf_counter()
-    rb = orun.solve(t)
+    rb = orun.solve(tabs)
     dt = time.perf_counter() - t0
-    return rb.passes * int(np.prod(t["ns"])) * t["nd"], dt
+    return rb.passes * int(np.prod(tabs["ns"])) * tabs["nd"], dt, rb.passes
 
 
 def cpu_baseline_single():
-    """~10-15 s of single-thread CPU work: one photon and one electron solve."""
-    u1, t1 = _cpu_one((1, "photon"))
-    u2, t2 = _cpu_one((2, "electron"))
-    return {"value": (u1 + u2) / (t1 + t2), "unit": "updates/s", "cores": 1, "kind": "port",
-            "sample": "one photon (BTE) and one electron (BFP) solve of the workload, single thread, "
-                      f"{t1 + t2:.1f} s of CPU work"}
+    """One bounded sample on the host's cores (the oracle threads over the directions)."""
+    t = cpu_sample_tables()
+    upd, dt, passes = cpu_sample(t)
+    ncores = os.cpu_count() or 1
+    return {"value": upd / dt, "unit": "updates/s", "cores": ncores, "kind": "port",
+            "sample": f"the 3D photon problem (64^3, S8, 80 moments) reduced to one group, {passes} passes "
+                      f"({CPU_SAMPLE_ITERS} BiCGStab iterations at most), {dt:.1f} s on {ncores} threads"}
 
 
 def run_reference(args):
     ncores = os.cpu_count() or 1
-    jobs = [(k + 1, "photon" if k % 3 == 0 else "electron") for k in range(ncores)]
-    ctxmp = mp.get_context("spawn")
-    with ctxmp.Pool(ncores) as pool:
-        for _ in range(args.warmup):
-            pool.map(_cpu_one, jobs[:ncores])
-        vals = []
-        t_all = 0.0
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            res = pool.map(_cpu_one, jobs)
-            dt = time.perf_counter() - t0
-            t_all += dt
-            vals.append(sum(u for u, _ in res) / dt)
+    t = cpu_sample_tables()
+    for _ in range(args.warmup):
+        cpu_sample(t)
+    vals, t_all, passes = [], 0.0, 0
+    for _ in range(args.steps):
+        upd, dt, passes = cpu_sample(t)
+        t_all += dt
+        vals.append(upd / dt)
     value = statistics.mean(vals)
+    sample = (f"the 3D photon problem (64^3, S8, 80 moments, reflective Z-, BiCGStab) reduced to one group and "
+              f"{CPU_SAMPLE_ITERS} iterations ({passes} passes) per step, {ncores} threads (C restatement of the "
+              "reference's Julia solve; Julia is not installed)")
     line = {
         "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_all * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
         "data": "synthetic (seeded cross-section tables with the configuration's shapes)",
-        "config": {"workload": "1D slab coupled BFP (same shapes as our arm); one photon or electron solve "
-                               "per host core per step", "precision": "fp64"},
-        "cpu_baseline": {"value": value, "unit": "updates/s", "cores": ncores, "kind": "port",
-                         "sample": f"{len(jobs)} solves per step on {ncores} processes (C restatement of the "
-                                   "reference's Julia solve; Julia is not installed)"},
+        "config": {"workload": "3D 64^3 photon-electron configuration (same shapes as our arm); bounded sample: "
+                               "the photon problem, one group, 3 BiCGStab iterations per step", "precision": "fp64"},
+        "cpu_baseline": {"value": value, "unit": "updates/s", "cores": ncores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
@@ -396,19 +498,25 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--seeds", type=int, default=50)
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c2e8", "c4g1"],
-                    help="c2: the benchmark workload; c1 / c2e8 / c4g1: small cases for profiling captures")
+    ap.add_argument("--precision", default=None, choices=["fp64", "mixed"],
+                    help="arithmetic form of the headline (default: mixed for c4, fp64 otherwise)")
+    ap.add_argument("--seeds", type=int, default=1, help="seeds per GPU (c4: one photon + one electron solve each)")
+    ap.add_argument("--groups", type=int, default=None, help="groups per particle (c4; default 40)")
+    ap.add_argument("--workload", default="c4", choices=["c4", "c2", "c1", "c2e8", "c4g1"],
+                    help="c4: the benchmark workload; c2: the 1D batch alone; c1 / c2e8 / c4g1: small cases "
+                         "for profiling captures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per problem team (0: library default)")
-    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision form")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form beside the chosen one")
+    ap.add_argument("--no-c2", action="store_true", help="skip the 1D batch section")
     ap.add_argument("--serve", type=int, default=60, help="requests of the serving run (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--serve-cells", type=int, default=2000)
     ap.add_argument("--serve-groups", type=int, default=120)
     ap.add_argument("--serve-side", type=int, default=128)
     args = ap.parse_args()
+    if args.workload == "c2" and args.seeds == 1:
+        args.seeds = 50
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if args.cluster:

@@ -44,6 +44,24 @@ __global__ void to_reference_layout(const double *__restrict__ src, double *__re
         if (g < ng && k < nphi) dst[(long long)ng * k + g] = tile[threadIdx.x][j];
     }
 }
+// [ng, nphi] (group fastest, the reference's layout) -> [ng][nphi] (group-major)
+__global__ void from_reference_layout(const double *__restrict__ src, double *__restrict__ dst, int ng,
+                                      long long nphi) {
+    __shared__ double tile[32][33];
+    const long long k0 = (long long)blockIdx.x * 32;
+    const int g0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const long long k = k0 + j;
+        const int g = g0 + threadIdx.x;
+        if (g < ng && k < nphi) tile[threadIdx.x][j] = src[(long long)ng * k + g];
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int g = g0 + j;
+        const long long k = k0 + threadIdx.x;
+        if (g < ng && k < nphi) dst[(long long)g * nphi + k] = tile[j][threadIdx.x];
+    }
+}
 }  // namespace rb
 
 namespace {
@@ -241,7 +259,7 @@ struct Derived {
     long long ncell, nphi, nstate, off_b[3], nb[3], fcells[3];
     int csd;
     std::vector<int> mat0;
-    std::vector<double> cosv, mn, dn, mnfp, frow_m, frow_d, G, Gsrc, Gout, Kcsd, Bcsd, EsA, EsB, Eout, vol;
+    std::vector<double> cosv, mn, dn, mnfp, frow_m, frow_d, G, Gsrc, Gout, Kcsd, Bcsd, EsA, EsB, Eout;
     std::vector<int> tang;
     // 2D/3D: the device holds the directions grouped by octant (quadrant in 2D), each group in
     // the reference's order; perm[k] is the reference index of device direction k, and
@@ -454,13 +472,6 @@ int validate_and_derive(rb_context *ctx, const rb_sn_problem *P, Derived &D) {
             D.Eout[e + (size_t)nE * j] = C[jE - 1] * m1pow(jE - 1) * wE[jE];
         }
     }
-    // volume sources, group-major
-    if (P->volume_sources) {
-        D.vol.resize((size_t)P->ng * D.nphi);
-        for (int g = 0; g < P->ng; g++)
-            for (long long k = 0; k < D.nphi; k++)
-                D.vol[(size_t)g * D.nphi + k] = P->volume_sources[g + (long long)P->ng * k];
-    }
     return RB_OK;
 }
 
@@ -501,7 +512,7 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     offs[k++] = L.take<double>(D.csd ? (size_t)ng * nmat * P->order[3] : 0); // 22 s_mom
     offs[k++] = L.take<double>(P->t_mom ? (size_t)ng * nmat : 0);     // 23 t_mom
     offs[k++] = L.take<double>(D.csd ? (size_t)ng : 0);               // 24 e_width
-    offs[k++] = L.take<double>(D.vol.size());                         // 25 vol
+    offs[k++] = L.take<double>(P->volume_sources ? (size_t)P->ng * D.nphi : 0);  // 25 vol (group-major)
     for (int f = 0; f < 6; f++)                                       // 26..31 surface
         offs[k++] = L.take<double>((f < 2 * P->ndims && P->surface_sources[f])
                                        ? (size_t)ng * P->np_source * face_cells(P->ndims, D.ns, f / 2) : 0);
@@ -731,7 +742,7 @@ ProblemRec *find(rb_context *ctx, rb_handle h) {
 // Lays one problem out in the device block `b` (offsets `o` from required()): fills the
 // device record `h`, queues the table copies on `s` and writes the record to *dptr.
 int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, const size_t *o, char *b,
-                  cudaStream_t s, DevProblem &h, DevProblem **dptr) {
+                  cudaStream_t s, DevProblem &h, DevProblem **dptr, double *stage) {
     memset(&h, 0, sizeof(h));
     const int nd = P->nd, np = P->np, nm5 = D.M.nm, ng = P->ng, nmat = P->nmat;
     h.ndims = P->ndims; h.nx = D.ns[0]; h.ny = D.ns[1]; h.nz = D.ns[2]; h.ncell = D.ncell;
@@ -759,7 +770,7 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     h.sigma_t = DP(double, 18); h.sigma_s = DP(double, 19);
     h.s_minus = D.csd ? DP(double, 20) : nullptr; h.s_plus = D.csd ? DP(double, 21) : nullptr;
     h.s_mom = D.csd ? DP(double, 22) : nullptr; h.t_mom = P->t_mom ? DP(double, 23) : nullptr;
-    h.e_width = D.csd ? DP(double, 24) : nullptr; h.vol = D.vol.empty() ? nullptr : DP(double, 25);
+    h.e_width = D.csd ? DP(double, 24) : nullptr; h.vol = P->volume_sources ? DP(double, 25) : nullptr;
     for (int f = 0; f < 6; f++) h.surf[f] = (f < 2 * P->ndims && P->surface_sources[f]) ? DP(double, 26 + f) : nullptr;
     h.flux = DP(double, 32); h.vecs = DP(double, 33); h.qlout = DP(double, 34); h.qnout = DP(double, 35);
     h.psi = DP(double, 36); h.kmat = DP(double, 37); h.scsd = DP(double, 38); h.fexit = DP(double, 39);
@@ -808,7 +819,14 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
         PUT(double, 24, P->e_width, ng);
     }
     if (P->t_mom) PUT(double, 23, P->t_mom, (size_t)ng * nmat);
-    PUT(double, 25, D.vol.data(), D.vol.size());
+    if (P->volume_sources) {
+        // the volume sources arrive in the reference's layout [ng, np, nm5, cells] (group
+        // fastest): copied to the staging buffer and turned group-major on the device
+        CK(cudaMemcpyAsync(stage, P->volume_sources, sizeof(double) * (size_t)ng * D.nphi, cudaMemcpyHostToDevice, s));
+        dim3 blk(32, 8), grd((unsigned)((D.nphi + 31) / 32), (unsigned)((ng + 31) / 32));
+        rb::from_reference_layout<<<grd, blk, 0, s>>>(stage, const_cast<double *>(h.vol), ng, D.nphi);
+        CK(cudaGetLastError());
+    }
     PUT(float, 52, D.tc_m2d.data(), D.tc_m2d.size());
     PUT(float, 53, D.tc_d2m.data(), D.tc_d2m.size());
     for (int f = 0; f < 2 * P->ndims; f++)
@@ -903,12 +921,22 @@ int32_t rb_upload(rb_context *ctx, const rb_sn_problem *P, rb_handle *out) {
     if (ctx->used + L.off > ctx->budget)
         return fail(ctx, RB_ERR_BUDGET, "problem needs %zu bytes, %llu of %llu budget bytes in use", L.off,
                     (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
+    if (P->volume_sources) {  // staging for the volume sources' layout change
+        const size_t need = (size_t)P->ng * D.nphi;
+        if (need > ctx->stage_cap) {
+            if (ctx->d_stage) cudaFree(ctx->d_stage);
+            ctx->d_stage = nullptr;
+            ctx->stage_cap = 0;
+            CK(cudaMalloc(&ctx->d_stage, need * sizeof(double)));
+            ctx->stage_cap = need;
+        }
+    }
     auto rec = std::make_unique<ProblemRec>();
     CK(cudaMalloc(&rec->block, L.off));
     rec->bytes = L.off;
     cudaStream_t s = ctx->stream;
     DevProblem &h = rec->h;
-    st = place_problem(ctx, P, D, o, rec->block, s, h, &rec->d);
+    st = place_problem(ctx, P, D, o, rec->block, s, h, &rec->d, ctx->d_stage);
     if (st) { cudaFree(rec->block); return st; }
     rec->own_list = reinterpret_cast<DevProblem **>(rec->block + o[50]);
     rec->own_queue = reinterpret_cast<int *>(rec->block + o[51]);
@@ -1132,11 +1160,11 @@ extern "C" int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_resul
     cudaStream_t s = (cudaStream_t)stream;
     DevProblem h;
     DevProblem *d = nullptr;
-    st = place_problem(nullptr, prob, D, o, base, s, h, &d);
+    double *d_stage = reinterpret_cast<double *>(base + off_stage);
+    st = place_problem(nullptr, prob, D, o, base, s, h, &d, d_stage);
     if (st) return st;
     DevProblem **d_list = reinterpret_cast<DevProblem **>(base + off_list);
     int *d_queue = reinterpret_cast<int *>(base + off_queue);
-    double *d_stage = reinterpret_cast<double *>(base + off_stage);
     // the array keeps the previous call's contents: zero the queue counter and status word
     CK(cudaMemcpyAsync(d_list, &d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(d_queue, 0, sizeof(int), s));

@@ -152,7 +152,7 @@ def prepare_sn_tables(xs: MultigroupXS, ndims: int, ns, ds, mat, bc, sn: SNSetti
         vol = None
     else:
         vol = np.asarray(volume_sources, dtype=float)
-        full = np.zeros((ng, Np, nm5, *ns))
+        full = np.zeros((ng, Np, nm5, *ns), order="F")  # the reference's column-major layout
         full[:, :vol.shape[1], :vol.shape[2]] = vol.reshape(vol.shape[0], vol.shape[1], vol.shape[2], *ns)
         vol = full
     surf = [None] * 6
