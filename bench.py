@@ -46,7 +46,7 @@ METRIC = "cell-dir-group updates/s"
 # proportion to the updates, so a launch's traffic is this times its updates:
 #   solve_local1d_kernel, 18 electron solves of the 1D batch reduced to 8 groups, FP64;
 #   solve_grid_kernel, the 3D photon problem reduced to one group, mixed and FP64 forms.
-TRAFFIC_BYTES_PER_UPDATE = {("c2", "fp64"): 399.8}
+TRAFFIC_BYTES_PER_UPDATE = {("c2", "fp64"): 399.8, ("c4", "mixed"): 139.2, ("c4", "fp64"): 157.3}
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -229,17 +229,17 @@ def run_ours(args, rank, world):
     for _ in range(args.warmup):
         ctx.solve_batch(handles, sptr)
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        ms = max_over_ranks(time_steps(ctx, handles, sptr, stream, args.steps), world)
     # passes per problem (identical every step: the solve is deterministic)
     for h, rb in zip(handles, rbs):
         ctx.download(h, rb)
     updates = updates_of(rbs, tabs)
     w = 8 if prec == "fp64" else 4
     abytes = sum(algorithmic_bytes(t, rb.passes, w) for rb, t in zip(rbs, tabs))
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(dev) as clk:
-        ms = max_over_ranks(time_steps(ctx, handles, sptr, stream, args.steps), world)
     value = updates * world / (ms / 1e3)
     for h in handles:
         ctx.release(h)
@@ -327,6 +327,7 @@ def run_ours(args, rank, world):
                      "kernel": kernel_name(args.workload)},
         "e2e": {"value": updates * world / (e2e_ms / 1e3), "unit": "updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps},
+        "updates_per_step": updates,
         "gpu_launches": args.steps * (len(tabs) if args.workload in ("c4", "c4g1") else 1),
         "clocks": clk.summary(),
     }
