@@ -377,46 +377,67 @@ def run_c2_section(args, ctx, sptr, stream, rank, world):
 
 
 def run_serving(args, ctx, dev):
-    """A bounded serving run: a seeded Poisson stream of requests from the serving mix through
-    rb_submit / rb_poll (continuous batching, mixed form for 1D requests), against plain FP64
-    per-request solves of the same requests, one at a time."""
+    """A bounded serving run: the first `--serve` requests of the seeded serving stream (70 % 1D
+    slabs / 30 % 2D grids, photon-only or photon+electron+positron sets, 10-`--serve-groups`
+    groups, log-uniform beam energy 0.1-20 MeV), Poisson arrivals, through rb_submit / rb_poll
+    (continuous batching: every admitted solve runs at once beside the others). The same stream
+    is served in the mixed form and in the plain FP64 form at the same arrivals and admission
+    (equal concurrency); plain FP64 per-request solves one at a time are timed on a prefix."""
     from radiant_b200 import serving as S
     from radiant_b200 import workloads as W
     from radiant_b200._abi import PackedProblem, ResultBuffers
 
     n = args.serve
-    reqs_t = W.serving_stream(n, seed=2024, precision="mixed", max_cells=args.serve_cells,
-                              max_groups=args.serve_groups, max_side=args.serve_side)
     arrivals = S.poisson_arrivals(n, args.serve_rate, seed=7)
-    # warm the request path once
-    S.ServingLoop(ctx).run([S.Request(0, reqs_t[0], 0.0)])
-    reqs = [S.Request(i, t, float(a)) for i, (t, a) in enumerate(zip(reqs_t, arrivals))]
-    S.ServingLoop(ctx).run(reqs)
-    served = S.latency_summary(reqs)
-    upd = sum(r.result.passes * int(np.prod(r.tables["ns"])) * r.tables["nd"] for r in reqs)
-    span = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
-    served["updates_per_s"] = upd / span
-    # plain FP64, one request at a time (per-request drop-in solves)
-    base_t = [dict(t, precision="fp64") for t in reqs_t]
-    lat = []
+    out = {"requests": n, "arrival_rate_per_s": args.serve_rate,
+           "stream": f"seeded serving stream: 70% 1D slabs (50-{args.serve_cells} cells, S8-S64, P1-P9, 1-5 layers "
+                     f"of 4 materials) / 30% 2D grids (side 32-{args.serve_side}, S4-S12); 10-{args.serve_groups} "
+                     "groups per particle; photon-only or photon+electron+positron sets with p=1/2; beam energy "
+                     "log-uniform 0.1-20 MeV"}
+
+    def solves_updates(reqs):
+        return sum(rb.passes * int(np.prod(t["ns"])) * t["nd"] for r in reqs for rb, t in zip(r.results, r.parts))
+
+    for prec in ("mixed", "fp64"):
+        reqs_t = W.c5_stream(n, 2024, prec, args.serve_cells, args.serve_groups, args.serve_side)
+        S.ServingLoop(ctx).run([S.Request(0, reqs_t[0], 0.0)])  # warm the request path
+        reqs = [S.Request(i, t, float(a)) for i, (t, a) in enumerate(zip(reqs_t, arrivals))]
+        S.ServingLoop(ctx).run(reqs)
+        summ = S.latency_summary(reqs)
+        span = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
+        summ["updates_per_s"] = solves_updates(reqs) / span
+        out["served_" + prec] = summ
+        if prec == "mixed":
+            served_mixed = reqs
+        else:
+            out["mixed_vs_fp64_max_rel_l2"] = max(
+                float(np.linalg.norm(a.flux - b.flux) / max(np.linalg.norm(b.flux), 1e-300))
+                for ra, rb_ in zip(served_mixed, reqs) for a, b in zip(ra.results, rb_.results))
+    out["mixed_over_fp64"] = {"solves_per_s": out["served_mixed"]["solves_per_s"] / out["served_fp64"]["solves_per_s"],
+                              "p50": out["served_mixed"]["p50_ms"] / out["served_fp64"]["p50_ms"],
+                              "p99": out["served_mixed"]["p99_ms"] / out["served_fp64"]["p99_ms"]}
+    # plain FP64 per-request solves, one request at a time (no overlap), on a prefix of the stream
+    m = min(n, args.serve_sequential)
+    base_t = W.c5_stream(m, 2024, "fp64", args.serve_cells, args.serve_groups, args.serve_side)
+    lat, nsolves = [], 0
     t_all = time.perf_counter()
-    bupd = 0
-    for t in base_t:
-        pp = PackedProblem(t)
-        rb = ResultBuffers(pp)
+    for parts in base_t:
         t0 = time.perf_counter()
-        h = ctx.upload(pp)
-        ctx.solve(h)
-        ctx.download(h, rb)
-        ctx.release(h)
+        for t in parts:
+            pp = PackedProblem(t)
+            rb = ResultBuffers(pp)
+            h = ctx.upload(pp)
+            ctx.solve(h)
+            ctx.download(h, rb)
+            ctx.release(h)
+            nsolves += 1
         lat.append(time.perf_counter() - t0)
-        bupd += rb.passes * int(np.prod(t["ns"])) * t["nd"]
     t_all = time.perf_counter() - t_all
     lat = np.array(lat)
-    return {"requests": n, "arrival_rate_per_s": args.serve_rate, "mix": "70% 1D slabs / 30% 2D grids (seeded)",
-            "served": served,
-            "fp64_per_request": {"p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                                 "solves_per_s": n / t_all, "updates_per_s": bupd / t_all}}
+    out["fp64_one_at_a_time"] = {"requests": m, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "requests_per_s": m / t_all,
+                                 "solves_per_s": nsolves / t_all}
+    return out
 
 
 def p_bytes(t):
@@ -510,11 +531,15 @@ def main():
     ap.add_argument("--cluster", type=int, default=0, help="CTAs per problem team (0: library default)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 form beside the chosen one")
     ap.add_argument("--no-c2", action="store_true", help="skip the 1D batch section")
-    ap.add_argument("--serve", type=int, default=60, help="requests of the serving run (0: skip)")
-    ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate (requests/s)")
-    ap.add_argument("--serve-cells", type=int, default=2000)
-    ap.add_argument("--serve-groups", type=int, default=120)
-    ap.add_argument("--serve-side", type=int, default=128)
+    ap.add_argument("--serve", type=int, default=100,
+                    help="requests of the serving run (0: skip); the full serving configuration is 2000")
+    ap.add_argument("--serve-rate", type=float, default=50.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--serve-cells", type=int, default=2000, help="largest 1D request (cells)")
+    ap.add_argument("--serve-groups", type=int, default=120, help="most groups per particle")
+    ap.add_argument("--serve-side", type=int, default=64,
+                    help="largest 2D request side (the configuration draws up to 128)")
+    ap.add_argument("--serve-sequential", type=int, default=30,
+                    help="requests of the one-at-a-time FP64 control")
     args = ap.parse_args()
     if args.workload == "c2" and args.seeds == 1:
         args.seeds = 50

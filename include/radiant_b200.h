@@ -190,12 +190,17 @@ RB_API int32_t rb_compute_flux(int32_t device, const rb_sn_problem *prob, rb_sn_
  * the results are in the caller's host buffers. The first call on a device looks the array's
  * device address up (cudaGetSymbolAddress) with that device current; make that first call
  * before any stream capture. Every call shares the one array and overwrites it: calls that
- * overlap on the GPU (other host threads, other streams) race and must be serialised. */
+ * overlap on the GPU (other host threads, other streams) race and must be serialised.
+ * The solve runs as one team of a single CTA (one SM of the GPU), whatever the dimension: the
+ * entry point is meant for the small problems that fit its array, not for throughput (larger
+ * or throughput-bound work belongs on rb_compute_flux / rb_solve_batch). */
 RB_API int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_result *res, void *stream);
 
-/* ---- serving: continuous batching over a device work queue --------------------------- */
-/* Admits a request when its state fits the remaining HBM budget (RB_ERR_BUDGET otherwise);
- * admitted requests run as soon as a slot of the persistent kernel frees up. */
+/* ---- serving: continuous batching ---------------------------------------------------- */
+/* Admits a request (one particle solve) when its state fits the remaining HBM budget
+ * (RB_ERR_BUDGET otherwise, nothing allocated). An admitted request is uploaded and launched at
+ * once as its own cluster team (one persistent-kernel launch on a stream of a pool of 32), so it
+ * runs beside the requests already on the device and its result never depends on them. */
 RB_API int32_t rb_submit(rb_context *ctx, const rb_sn_problem *prob, rb_handle *out);
 /* RB_OK when the request finished (results copied into res and the request released),
  * RB_ERR_NOT_READY while it is still running. */

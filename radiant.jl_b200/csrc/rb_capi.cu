@@ -1169,6 +1169,8 @@ extern "C" int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_resul
     CK(cudaMemcpyAsync(d_list, &d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(d_queue, 0, sizeof(int), s));
     CK(cudaMemsetAsync(h.status, 0, sizeof(int), s));
+    // one team of one CTA (one SM): the array holds no grid-team reduction slots, and the entry
+    // point serves small problems
     st = launch_solve(nullptr, d_list, 1, d_queue, 1, 1, s, {&h}, LAUNCH_FIXED);
     if (st) return st;
     const int ng = prob->ng;

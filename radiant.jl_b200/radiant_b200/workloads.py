@@ -347,3 +347,100 @@ def serving_stream(n: int, seed: int, precision: str = "mixed", max_cells: int =
         else:
             out.append(random_grid_tables(s, max_side=max_side))
     return out
+
+
+# ------------------------------------------------------------------------------------------
+# the serving stream (configuration C5)
+# ------------------------------------------------------------------------------------------
+C5_MATERIALS = 4  # water, cortical bone, lung-density water (0.3 g/cc), aluminium (synthetic tables)
+
+
+def _beam_group(eb, energy):
+    """Index of the group holding `energy` (boundaries highest first)."""
+    for g in range(len(eb) - 1):
+        if eb[g] >= energy > eb[g + 1]:
+            return g
+    return 0 if energy > eb[0] else len(eb) - 2
+
+
+def c5_request(seed: int, precision: str = "mixed", max_cells: int = 2000, max_groups: int = 120,
+               max_side: int = 128):
+    """One request of the serving stream, as the serving configuration draws it: a 1D slab with
+    probability 0.7 (cells U(50, max_cells), SN order in {8,16,32,64}, P order U(1,9), 1-5
+    layers of the four materials) or a 2D grid (side U(32, max_side), level-symmetric S4-S12,
+    vertical material layers); groups U(10, max_groups) per particle; a normal beam on the X-
+    face at an energy log-uniform in 0.1-20 MeV (group structure 20 MeV - 1 keV); particle set
+    photon only or photon + electron + positron with probability 1/2. Returns the list of the
+    request's particle solves (tables), photon first."""
+    rng = np.random.default_rng(seed)
+    is1d = rng.uniform() < 0.7
+    parts = ["photon"] if rng.uniform() < 0.5 else ["photon", "electron", "positron"]
+    energy = math.exp(rng.uniform(math.log(0.1), math.log(20.0)))
+    ng = int(rng.integers(10, max_groups + 1))
+    eb, _, _ = log_groups(ng, 20.0, 0.001)
+    gb = _beam_group(eb, energy)
+    L = int(rng.integers(1, 10))
+    out = []
+    if is1d:
+        nx = int(rng.integers(50, max_cells + 1))
+        N = int(rng.choice([8, 16, 32, 64]))
+        nlay = int(rng.integers(1, 6))
+        cuts = sorted(rng.choice(np.arange(1, nx), size=nlay - 1, replace=False)) if nlay > 1 else []
+        mats = np.ones(nx, dtype=np.int32)
+        start = 0
+        for cpos in list(cuts) + [nx]:
+            mats[start:cpos] = int(rng.integers(1, C5_MATERIALS + 1))
+            start = cpos
+        width = rng.uniform(2.0, 20.0)
+        for k, part in enumerate(parts):
+            bfp = part != "photon"
+            if bfp:
+                sn = SNSettings(solver_type="BFP", quadrature_type="gauss-legendre", quadrature_order=N,
+                                legendre_order=L, scheme_type={"x": "DD", "E": "DD"}, scheme_order={"x": 1, "E": 1},
+                                angular_fokker_planck="galerkin", acceleration="gmres", convergence_criterion=1e-7,
+                                angular_boltzmann="standard")
+            else:
+                sn = SNSettings(solver_type="BTE", quadrature_type="gauss-legendre", quadrature_order=N,
+                                legendre_order=L, scheme_type={"x": "DD"}, scheme_order={"x": 1},
+                                acceleration="gmres", convergence_criterion=1e-7, angular_boltzmann="standard")
+            xs = synthetic_xs(ng, C5_MATERIALS, L, seed * 7 + k + 7919, csd=bfp, e_top=20.0, e_cut=0.001)
+            t = slab_tables(nx, np.full(nx, width / nx), mats, ng, C5_MATERIALS, seed, sn, L, beam_group=gb,
+                            csd=bfp, precision=precision, xs=xs)
+            t["particle"] = part
+            out.append(t)
+        return out
+    n = int(rng.integers(32, max_side + 1))
+    N = int(rng.choice([4, 6, 8, 10, 12]))
+    L2 = min(L, 3)
+    nmat = int(rng.integers(1, C5_MATERIALS + 1))
+    mats = np.ones((n, n), dtype=np.int32)
+    cuts = np.linspace(0, n, nmat + 1).astype(int)
+    for k in range(nmat):
+        mats[cuts[k]:cuts[k + 1], :] = int(rng.integers(1, C5_MATERIALS + 1))
+    width = rng.uniform(5.0, 20.0)
+    d = width / n
+    for k, part in enumerate(parts):
+        bfp = part != "photon"
+        st = {"x": "DD", "y": "DD"}
+        so = {"x": 1, "y": 1}
+        if bfp:
+            st["E"] = "DD"
+            so["E"] = 1
+        sn = SNSettings(solver_type="BFP" if bfp else "BTE", quadrature_type="carlson", quadrature_order=N,
+                        legendre_order=L2, scheme_type=st, scheme_order=so, acceleration="gmres",
+                        convergence_criterion=1e-7, angular_boltzmann="standard", angular_fokker_planck="galerkin")
+        xs = synthetic_xs(ng, C5_MATERIALS, L2, seed * 7 + k + 104729, csd=bfp, e_top=20.0, e_cut=0.001)
+        t = grid_tables(2, [n, n], [np.full(n, d), np.full(n, d)], mats, ng, C5_MATERIALS, seed, sn, L2,
+                        beam=("X-", gb, (1.0, 0.0, 0.0), {1: (0.25 * width, 0.75 * width)}), csd=bfp,
+                        precision=precision, xs=xs)
+        t["particle"] = part
+        out.append(t)
+    return out
+
+
+def c5_stream(n: int, seed: int, precision: str = "mixed", max_cells: int = 2000, max_groups: int = 120,
+              max_side: int = 128):
+    """The first `n` requests of the seeded serving stream (c5_request each)."""
+    rng = np.random.default_rng(seed)
+    seeds = rng.integers(0, 2 ** 31 - 1, size=n)
+    return [c5_request(int(s), precision, max_cells, max_groups, max_side) for s in seeds]
