@@ -196,6 +196,39 @@ RB_API int32_t rb_compute_flux(int32_t device, const rb_sn_problem *prob, rb_sn_
  * or throughput-bound work belongs on rb_compute_flux / rb_solve_batch). */
 RB_API int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_result *res, void *stream);
 
+/* ---- coupled particles: transport() ----------------------------------------------------- */
+/* The coupling of particle i into particle j in the generation loop of transport()
+ * (transport.jl:79-143): the source of j produced by i's flux, particle_source(flux_i, ...)
+ * (particle_source.jl:23-79) =
+ *   Ql_in[gf,p,is,c]  = sum_gi sigma_s[mat,gi,gf,pl_i[p]] * flux_i[gi,p,is,c]   (particle_sources,
+ *                       scattering_source.jl:97-104)
+ *   Ql_out[gf,q,k,c]  = sum_p transfer[q,p] * Ql_in[gf,p,moment_map[k]-1,c]      (map_moments.jl:21-56)
+ * added to j's volume source. */
+typedef struct rb_coupling {
+    const double *sigma_s;      /* [nmat, ng_i, ng_j, ls+1]: get_scattering(particle_i, particle_j, maximum(pl_i));
+                                   NULL = i produces no j                                      */
+    int32_t ls;
+    const double *transfer;     /* [np_j, np_i]: angular_transfer_matrix(basis_i, basis_j)      */
+    const int32_t *moment_map;  /* [nm5_j]: 1-based cell moment of i feeding each moment of j, 0 = none */
+} rb_coupling;
+
+/* Replaces transport(cross_sections, geometry, solvers, sources) (transport.jl:21-147) for a
+ * set of SN particles on one geometry: every particle's problem, its accumulated particle source
+ * and its running total flux stay on the device for the whole generation loop; a generation
+ * solves the particles in order (starting from the first one with fixed sources), each solve
+ * followed by the sources it produces for the others (device kernels), and the fixed sources
+ * count in the first generation only. Convergence as the reference's "flux" criterion: after
+ * generation n > 1, every particle's max |Φ_n − Φ_(n−1)| / max(|Φ_n|, eps) over groups and cells
+ * (moment 1, cell moment 1) below eps_gen. couplings[i*npart + j] couples i into j (the diagonal
+ * is ignored). results[i]: flux and flux_cutoff summed over the generations (the reference's
+ * Flux_Per_Particle sums its solutions), rho / iterations / residuals / converged of the last
+ * generation's solve, passes summed over all solves. *generations: generations run; *eps_final:
+ * the last ϵ (NaN after one generation). conv_type: 0 = flux (energy and charge deposition
+ * criteria: RB_ERR_UNSUPPORTED). */
+RB_API int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_problem *const *probs,
+                            const rb_coupling *couplings, int32_t ngen_max, double eps_gen, int32_t conv_type,
+                            rb_sn_result *const *results, int32_t *generations, double *eps_final);
+
 /* ---- serving: continuous batching ---------------------------------------------------- */
 /* Admits a request (one particle solve) when its state fits the remaining HBM budget
  * (RB_ERR_BUDGET otherwise, nothing allocated). An admitted request is uploaded and launched at

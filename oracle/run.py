@@ -27,3 +27,30 @@ def solve(tables):
     if st != 0:
         raise RuntimeError(f"oracle status {st}")
     return rb
+
+
+def transport(parts, couplings, ngen_max=50, eps_gen=1e-6):
+    """oracle_transport on prepared tables of several particles; ``couplings[(i, j)]`` as in
+    radiant_b200.transport. Returns (ResultBuffers per particle, generations, eps)."""
+    from radiant_b200._abi import PackedProblem, ResultBuffers, RbCoupling, RbSnProblem, RbSnResult
+    from radiant_b200.transport import _CouplingPack
+
+    L = lib()
+    if not getattr(L, "_transport_declared", False):
+        L.oracle_transport.argtypes = [C.c_int32, C.POINTER(C.POINTER(RbSnProblem)), C.POINTER(RbCoupling),
+                                       C.c_int32, C.c_double, C.c_int32, C.POINTER(C.POINTER(RbSnResult)),
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_double)]
+        L.oracle_transport.restype = C.c_int
+        L._transport_declared = True
+    packs = [PackedProblem(t) for t in parts]
+    res = [ResultBuffers(p) for p in packs]
+    n = len(parts)
+    probs = (C.POINTER(RbSnProblem) * n)(*[C.pointer(p.P) for p in packs])
+    results = (C.POINTER(RbSnResult) * n)(*[C.pointer(r.R) for r in res])
+    cp = _CouplingPack(n, couplings)
+    ngen = C.c_int32(0)
+    eps = C.c_double(0.0)
+    st = L.oracle_transport(n, probs, cp.arr, int(ngen_max), float(eps_gen), 0, results, C.byref(ngen), C.byref(eps))
+    if st != 0:
+        raise RuntimeError(f"oracle status {st}")
+    return res, int(ngen.value), float(eps.value)

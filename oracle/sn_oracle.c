@@ -1058,3 +1058,149 @@ int oracle_energy_deposition(int32_t ng, int32_t np, int32_t nm5, int64_t ncell,
     (void)nmat;
     return RB_OK;
 }
+
+/* ------------------------------------------------------------------------------------ */
+/* coupled particles: transport() (transport.jl:21-147)                                  */
+/* ------------------------------------------------------------------------------------ */
+/* particle_source (particle_source.jl:23-77) of particle i's flux phi_i (reference layout
+ * [ng_i,np_i,nm_i,cells]) into particle j, added to ps_j ([ng_j,np_j,nm_j,cells]):
+ * Ql_in from particle_sources (scattering_source.jl:97-104), then the transfer over the
+ * mapped cell moments, then particle_sources[j] += ps (transport.jl:105). */
+static void oracle_particle_source(const rb_sn_problem *Pi, const rb_sn_problem *Pj, const rb_coupling *cp,
+                                   const double *phi_i, double *ps_j) {
+    const int ngi = Pi->ng, ngf = Pj->ng, npi = Pi->np, npo = Pj->np, nmi = Pi->nm[4], nmo = Pj->nm[4];
+    const int nmat = Pi->nmat;
+    const int64_t ncell = (int64_t)Pi->nx * (Pi->ndims >= 2 ? Pi->ny : 1) * (Pi->ndims >= 3 ? Pi->nz : 1);
+    double *ql_in = zalloc((int64_t)ngf * npi * nmi * ncell);
+    double *ql_out = zalloc((int64_t)ngf * npo * nmo * ncell);
+    for (int gf = 0; gf < ngf; gf++)
+        for (int64_t c = 0; c < ncell; c++) {
+            const int m = Pi->mat[c] - 1;
+            for (int gi = 0; gi < ngi; gi++)
+                for (int is = 0; is < nmi; is++)
+                    for (int p = 0; p < npi; p++) {
+                        const int64_t k = p + (int64_t)npi * (is + (int64_t)nmi * c);
+                        ql_in[gf + (int64_t)ngf * k] +=
+                            cp->sigma_s[m + (int64_t)nmat * (gi + (int64_t)ngi * (gf + (int64_t)ngf * Pi->pl[p]))] *
+                            phi_i[gi + (int64_t)ngi * k];
+                    }
+        }
+    for (int i = 0; i < nmo; i++) {
+        const int mm = cp->moment_map[i];
+        if (mm == 0) continue;
+        for (int pin = 0; pin < npi; pin++)
+            for (int pout = 0; pout < npo; pout++) {
+                const double t = cp->transfer[pout + (int64_t)npo * pin];
+                if (t == 0.0) continue;
+                for (int64_t c = 0; c < ncell; c++)
+                    for (int g = 0; g < ngf; g++)
+                        ql_out[g + (int64_t)ngf * (pout + (int64_t)npo * (i + (int64_t)nmo * c))] +=
+                            t * ql_in[g + (int64_t)ngf * (pin + (int64_t)npi * (mm - 1 + (int64_t)nmi * c))];
+            }
+    }
+    const int64_t n = (int64_t)ngf * npo * nmo * ncell;
+    for (int64_t k = 0; k < n; k++) ps_j[k] += ql_out[k];
+    free(ql_in);
+    free(ql_out);
+}
+
+int oracle_transport(int32_t npart, const rb_sn_problem *const *probs, const rb_coupling *couplings, int32_t ngen_max,
+                     double eps_gen, int32_t conv_type, rb_sn_result *const *results, int32_t *generations,
+                     double *eps_final) {
+    if (npart < 1 || ngen_max < 1) return RB_ERR_INVALID;
+    if (conv_type != 0) return RB_ERR_UNSUPPORTED;
+    int i0 = -1;
+    for (int i = 0; i < npart && i0 < 0; i++) {
+        int any = probs[i]->volume_sources != NULL;
+        for (int f = 0; f < 6; f++) any = any || probs[i]->surface_sources[f] != NULL;
+        if (any) i0 = i;
+    }
+    if (i0 < 0) return RB_ERR_INVALID; /* "No fixed sources are defined." */
+    int *order = (int *)malloc(sizeof(int) * npart);
+    for (int p = 0; p < npart; p++) order[p] = (i0 + p) % npart;
+    double **tot = (double **)calloc(npart, sizeof(double *)), **tot_cut = (double **)calloc(npart, sizeof(double *));
+    double **ps = (double **)calloc(npart, sizeof(double *)), **prev = (double **)calloc(npart, sizeof(double *));
+    double **gen = (double **)calloc(npart, sizeof(double *)), **gen_cut = (double **)calloc(npart, sizeof(double *));
+    double **src = (double **)calloc(npart, sizeof(double *));
+    int64_t *nall = (int64_t *)calloc(npart, sizeof(int64_t)), *nphi = (int64_t *)calloc(npart, sizeof(int64_t));
+    for (int i = 0; i < npart; i++) {
+        const rb_sn_problem *P = probs[i];
+        const int64_t ncell = (int64_t)P->nx * (P->ndims >= 2 ? P->ny : 1) * (P->ndims >= 3 ? P->nz : 1);
+        nphi[i] = (int64_t)P->np * P->nm[4] * ncell;
+        nall[i] = (int64_t)P->ng * nphi[i];
+        tot[i] = zalloc(nall[i]); ps[i] = zalloc(nall[i]); prev[i] = zalloc(nall[i]);
+        gen[i] = zalloc(nall[i]); src[i] = zalloc(nall[i]);
+        tot_cut[i] = zalloc(nphi[i]); gen_cut[i] = zalloc(nphi[i]);
+        results[i]->passes = 0;
+    }
+    int ngen = 0, st = RB_OK;
+    double eps_last = NAN;
+    for (int n = 1; n <= ngen_max && st == RB_OK; n++) {
+        ngen = n;
+        for (int i = 0; i < npart; i++) memcpy(prev[i], tot[i], sizeof(double) * nall[i]); /* flux⁻ */
+        for (int p = 0; p < npart && st == RB_OK; p++) {
+            const int i = order[p];
+            rb_sn_problem Q = *probs[i];
+            /* source = particle_sources[i] (+ fixed_source[i] when n == 1), transport.jl:90-91 */
+            for (int64_t k = 0; k < nall[i]; k++)
+                src[i][k] = (n == 1 && probs[i]->volume_sources) ? ps[i][k] + probs[i]->volume_sources[k] : ps[i][k];
+            Q.volume_sources = src[i];
+            if (n > 1) {
+                Q.np_source = 0;
+                for (int f = 0; f < 6; f++) Q.surface_sources[f] = NULL;
+            }
+            rb_sn_result R = *results[i];
+            R.flux = gen[i];
+            R.flux_cutoff = gen_cut[i];
+            st = oracle_compute_flux(&Q, &R);
+            if (st != RB_OK) break;
+            results[i]->passes += R.passes;
+            for (int64_t k = 0; k < nall[i]; k++) tot[i][k] += gen[i][k];   /* flux.add_flux, summed */
+            for (int64_t k = 0; k < nphi[i]; k++) tot_cut[i][k] += gen_cut[i][k];
+            if (n == ngen_max && p == npart - 1) continue;
+            for (int q = 0; q < npart; q++) {
+                const int j = order[q];
+                if (n == ngen_max && q <= p) continue;
+                if (i != j) {
+                    const rb_coupling *cp = couplings ? &couplings[(int64_t)i * npart + j] : NULL;
+                    if (cp && cp->sigma_s) oracle_particle_source(probs[i], probs[j], cp, gen[i], ps[j]);
+                } else {
+                    memset(ps[i], 0, sizeof(double) * nall[i]);
+                }
+            }
+        }
+        if (st != RB_OK) break;
+        if (n != 1) { /* the "flux" criterion, transport.jl:116-121 */
+            int px = 0;
+            double emax = 0.0;
+            for (int i = 0; i < npart; i++) {
+                const int ng = probs[i]->ng, np = probs[i]->np, nm = probs[i]->nm[4];
+                double e = 0.0;
+                for (int64_t c = 0; c < nphi[i] / ((int64_t)np * nm); c++)
+                    for (int g = 0; g < ng; g++) {
+                        const int64_t k = g + (int64_t)ng * ((int64_t)np * nm * c);
+                        const double r = fabs(tot[i][k] - prev[i][k]) / fmax(fabs(tot[i][k]), 2.220446049250313e-16);
+                        if (r > e) e = r;
+                    }
+                if (e > emax) emax = e;
+                if (e < eps_gen) px++;
+            }
+            eps_last = emax;
+            if (px == npart) break;
+        }
+    }
+    if (st == RB_OK)
+        for (int i = 0; i < npart; i++) {
+            if (results[i]->flux) memcpy(results[i]->flux, tot[i], sizeof(double) * nall[i]);
+            if (results[i]->flux_cutoff && probs[i]->solver_type >= 2)
+                memcpy(results[i]->flux_cutoff, tot_cut[i], sizeof(double) * nphi[i]);
+        }
+    if (generations) *generations = ngen;
+    if (eps_final) *eps_final = eps_last;
+    for (int i = 0; i < npart; i++) {
+        free(tot[i]); free(ps[i]); free(prev[i]); free(gen[i]); free(src[i]); free(tot_cut[i]); free(gen_cut[i]);
+    }
+    free(tot); free(ps); free(prev); free(gen); free(src); free(tot_cut); free(gen_cut); free(nall); free(nphi);
+    free(order);
+    return st;
+}

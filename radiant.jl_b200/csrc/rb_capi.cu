@@ -62,6 +62,80 @@ __global__ void from_reference_layout(const double *__restrict__ src, double *__
         if (g < ng && k < nphi) dst[(long long)g * nphi + k] = tile[j][threadIdx.x];
     }
 }
+
+// ---- coupled transport (rb_transport) ------------------------------------------------------
+// tot += gen over [ng][nphi]; for the entries of angular moment 1, cell moment 1 also the
+// largest |tot_new − tot_old| / max(|tot_new|, eps) (the reference's flux criterion,
+// transport.jl:114-118), as the bits of a non-negative double in *maxrel.
+__global__ void accumulate_generation(double *__restrict__ tot, const double *__restrict__ gen, long long n,
+                                      long long nphi, int np, int nm5, unsigned long long *maxrel) {
+    __shared__ double red[32];
+    double m = 0.0;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double t0 = tot[e], t1 = t0 + gen[e];
+        tot[e] = t1;
+        if (maxrel) {
+            const long long o = e % nphi;
+            if (o % ((long long)np * nm5) == 0) {  // p = 1 and is = 1 of a cell
+                const double r = fabs(t1 - t0) / fmax(fabs(t1), 2.220446049250313e-16);
+                m = fmax(m, r);
+            }
+        }
+    }
+    if (!maxrel) return;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x + 31) / 32; w++) m = fmax(m, red[w]);
+        atomicMax(maxrel, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// particle_source (particle_source.jl:23-79) of one cell and one cell moment k of the outgoing
+// particle, added to its particle source: one CTA per (cell, k). Shared memory: the incoming
+// flux of the cell [ng_i][np_i] and the group-transferred source [ng_o][np_i].
+__global__ void particle_source_kernel(const double *__restrict__ flux_i, int ng_i, int np_i, int nm_i,
+                                       const int *__restrict__ mat, int nmat, const double *__restrict__ sigma_s,
+                                       int ls, const int *__restrict__ pl_i, const double *__restrict__ transfer,
+                                       const int *__restrict__ moment_map, double *__restrict__ pvol_o, int ng_o,
+                                       int np_o, int nm_o, long long ncell) {
+    extern __shared__ double sm[];
+    double *phi = sm;                        // [ng_i][np_i]
+    double *ql = sm + (long long)ng_i * np_i;  // [ng_o][np_i]
+    const long long c = blockIdx.x;
+    const int k = blockIdx.y;
+    const int kin = moment_map[k] - 1;
+    if (kin < 0 || c >= ncell) return;
+    const long long nphi_i = (long long)np_i * nm_i * ncell, nphi_o = (long long)np_o * nm_o * ncell;
+    const int m = mat[c];
+    for (int e = threadIdx.x; e < ng_i * np_i; e += blockDim.x) {
+        const int gi = e / np_i, p = e % np_i;
+        phi[e] = flux_i[(long long)gi * nphi_i + p + (long long)np_i * (kin + (long long)nm_i * c)];
+    }
+    __syncthreads();
+    // Ql_in[gf,p] = Σ_gi Σs[m,gi,gf,pl[p]]·𝚽[gi,p], gi in increasing order (particle_sources)
+    for (int e = threadIdx.x; e < ng_o * np_i; e += blockDim.x) {
+        const int gf = e / np_i, p = e % np_i;
+        const double *ss = sigma_s + m + (long long)nmat * (long long)ng_i * (gf + (long long)ng_o * pl_i[p]);
+        double q = 0.0;
+        for (int gi = 0; gi < ng_i; gi++) q += ss[(long long)nmat * gi] * phi[(long long)gi * np_i + p];
+        ql[e] = q;
+    }
+    __syncthreads();
+    // Ql_out[gf,q] = Σ_p T[q,p]·Ql_in[gf,p] over the non-zero T, p in increasing order, then added
+    // to the particle source
+    for (int e = threadIdx.x; e < ng_o * np_o; e += blockDim.x) {
+        const int gf = e / np_o, qo = e % np_o;
+        double v = 0.0;
+        for (int p = 0; p < np_i; p++) {
+            const double tq = transfer[qo + (long long)np_o * p];
+            if (tq != 0.0) v += tq * ql[(long long)gf * np_i + p];
+        }
+        double *dst = pvol_o + (long long)gf * nphi_o + qo + (long long)np_o * (k + (long long)nm_o * c);
+        *dst = *dst + v;
+    }
+}
 }  // namespace rb
 
 namespace {
@@ -1195,4 +1269,230 @@ extern "C" int32_t rb_compute_flux_static(const rb_sn_problem *prob, rb_sn_resul
     if (status & RB_DEV_TIMEOUT) return fail(nullptr, RB_ERR_TIMEOUT, "a device wait gave up");
     if (status & RB_DEV_BAD_TABLE) return fail(nullptr, RB_ERR_INVALID, "singular cell system or bad table");
     return RB_OK;
+}
+
+// =============================================================================================
+// Coupled particles: the generation loop of transport() on the device
+// =============================================================================================
+namespace {
+struct CoupledPart {
+    rb_handle h = 0;
+    ProblemRec *r = nullptr;
+    double *tot = nullptr, *tot_cut = nullptr, *pvol = nullptr;  // summed flux, summed cutoff, particle source
+    unsigned long long *maxrel = nullptr;                          // ϵ of the last generation (double bits)
+    DevProblem with_fixed{}, without_fixed{};                      // records of generation 1 / later ones
+    long long passes = 0;
+};
+struct CoupledPair {
+    double *sigma_s = nullptr, *transfer = nullptr;
+    int *map = nullptr;
+    int ls = 0;
+};
+}  // namespace
+
+extern "C" int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_problem *const *probs,
+                                const rb_coupling *couplings, int32_t ngen_max, double eps_gen, int32_t conv_type,
+                                rb_sn_result *const *results, int32_t *generations, double *eps_final) {
+    rb_context *ctx = nullptr;
+    if (npart < 1 || !probs || !results) return fail(nullptr, RB_ERR_INVALID, "bad particle list");
+    if (ngen_max < 1) return fail(nullptr, RB_ERR_INVALID, "ngen_max must be >= 1");
+    if (conv_type != 0)
+        return fail(nullptr, RB_ERR_UNSUPPORTED, "only the flux convergence criterion of transport() is built");
+    for (int i = 0; i < npart; i++) {
+        const rb_sn_problem *a = probs[i], *b = probs[0];
+        if (!a || !results[i]) return fail(nullptr, RB_ERR_INVALID, "null problem or result %d", i);
+        if (a->ndims != b->ndims || a->nx != b->nx || (a->ndims > 1 && a->ny != b->ny) ||
+            (a->ndims > 2 && a->nz != b->nz) || a->nmat != b->nmat)
+            return fail(nullptr, RB_ERR_INVALID, "particle %d is not on the geometry of particle 1", i);
+    }
+    // the first particle with fixed sources leads the order (transport.jl:60-73)
+    int i0 = -1;
+    for (int i = 0; i < npart && i0 < 0; i++) {
+        bool any = probs[i]->volume_sources != nullptr;
+        for (int f = 0; f < 6; f++) any = any || probs[i]->surface_sources[f] != nullptr;
+        if (any) i0 = i;
+    }
+    if (i0 < 0) return fail(nullptr, RB_ERR_INVALID, "No fixed sources are defined.");
+    std::vector<int> order;
+    for (int i = i0; i < npart; i++) order.push_back(i);
+    for (int i = 0; i < i0; i++) order.push_back(i);
+    int st = rb_create(device, 0, &ctx);
+    if (st) return st;
+    std::vector<CoupledPart> parts(npart);
+    std::vector<CoupledPair> pairs((size_t)npart * npart);
+    auto cleanup = [&](int code) {
+        cudaStreamSynchronize(ctx->stream);
+        for (auto &p : parts) {
+            if (p.tot) cudaFree(p.tot);
+            if (p.tot_cut) cudaFree(p.tot_cut);
+            if (p.pvol) cudaFree(p.pvol);
+            if (p.maxrel) cudaFree(p.maxrel);
+        }
+        for (auto &q : pairs) {
+            if (q.sigma_s) cudaFree(q.sigma_s);
+            if (q.transfer) cudaFree(q.transfer);
+            if (q.map) cudaFree(q.map);
+        }
+        if (code != RB_OK) g_create_error = ctx->err;  // the message outlives the context
+        rb_destroy(ctx);
+        return code;
+    };
+#define CKT(call)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return cleanup(fail(ctx, RB_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_))); \
+    } while (0)
+    cudaStream_t s = ctx->stream;
+    for (int i = 0; i < npart; i++) {
+        CoupledPart &P = parts[i];
+        st = rb_upload(ctx, probs[i], &P.h);
+        if (st) return cleanup(st);
+        P.r = find(ctx, P.h);
+        const size_t n = (size_t)P.r->ng * P.r->nphi;
+        CKT(cudaMalloc(&P.tot, n * sizeof(double)));
+        CKT(cudaMalloc(&P.pvol, n * sizeof(double)));
+        CKT(cudaMalloc(&P.maxrel, sizeof(unsigned long long)));
+        CKT(cudaMemsetAsync(P.tot, 0, n * sizeof(double), s));
+        CKT(cudaMemsetAsync(P.pvol, 0, n * sizeof(double), s));
+        if (P.r->csd) {
+            CKT(cudaMalloc(&P.tot_cut, P.r->nphi * sizeof(double)));
+            CKT(cudaMemsetAsync(P.tot_cut, 0, P.r->nphi * sizeof(double), s));
+        }
+        P.with_fixed = P.r->h;
+        P.with_fixed.pvol = P.pvol;
+        P.without_fixed = P.with_fixed;  // later generations: the particle source alone
+        P.without_fixed.vol = nullptr;
+        P.without_fixed.np_source = 0;
+        for (int f = 0; f < 6; f++) P.without_fixed.surf[f] = nullptr;
+    }
+    for (int i = 0; i < npart; i++)
+        for (int j = 0; j < npart; j++) {
+            const rb_coupling *c = couplings ? &couplings[(size_t)i * npart + j] : nullptr;
+            if (i == j || !c || !c->sigma_s) continue;
+            const DevProblem &a = parts[i].r->h, &b = parts[j].r->h;
+            if (!c->transfer || !c->moment_map || c->ls < 0)
+                return cleanup(fail(ctx, RB_ERR_INVALID, "coupling %d->%d without transfer matrix or moment map", i, j));
+            for (int k = 0; k < b.nm5; k++)
+                if (c->moment_map[k] < 0 || c->moment_map[k] > a.nm5)
+                    return cleanup(fail(ctx, RB_ERR_INVALID, "moment_map[%d] of coupling %d->%d out of range", k, i, j));
+            for (int p = 0; p < a.np; p++)
+                if (probs[i]->pl[p] > c->ls)
+                    return cleanup(fail(ctx, RB_ERR_INVALID, "coupling %d->%d: ls below the incoming Legendre orders", i, j));
+            const long long smem = 8LL * ((long long)a.ng * a.np + (long long)b.ng * a.np);
+            if (smem > 200 * 1024)
+                return cleanup(fail(ctx, RB_ERR_UNSUPPORTED, "coupling %d->%d: groups x moments too large (%lld B)", i, j, smem));
+            CoupledPair &q = pairs[(size_t)i * npart + j];
+            q.ls = c->ls;
+            const size_t nss = (size_t)a.nmat * a.ng * b.ng * (c->ls + 1);
+            CKT(cudaMalloc(&q.sigma_s, nss * sizeof(double)));
+            CKT(cudaMalloc(&q.transfer, (size_t)b.np * a.np * sizeof(double)));
+            CKT(cudaMalloc(&q.map, (size_t)b.nm5 * sizeof(int)));
+            CKT(cudaMemcpyAsync(q.sigma_s, c->sigma_s, nss * sizeof(double), cudaMemcpyHostToDevice, s));
+            CKT(cudaMemcpyAsync(q.transfer, c->transfer, (size_t)b.np * a.np * sizeof(double), cudaMemcpyHostToDevice, s));
+            CKT(cudaMemcpyAsync(q.map, c->moment_map, (size_t)b.nm5 * sizeof(int), cudaMemcpyHostToDevice, s));
+        }
+    CKT(cudaFuncSetAttribute(rb::particle_source_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CKT(cudaStreamSynchronize(s));
+    double eps_last = NAN;
+    int ngen = 0;
+    for (int n = 1; n <= ngen_max; n++) {
+        ngen = n;
+        for (int p = 0; p < npart; p++) {
+            const int i = order[p];
+            CoupledPart &P = parts[i];
+            const DevProblem &hv = n == 1 ? P.with_fixed : P.without_fixed;
+            P.r->h = hv;
+            CKT(cudaMemcpyAsync(P.r->d, &hv, sizeof(DevProblem), cudaMemcpyHostToDevice, s));
+            std::vector<ProblemRec *> one{P.r};
+            st = launch(ctx, one, s);
+            if (st) return cleanup(st);
+            // the solution of this generation into the particle's sum, with its change
+            const long long nall = (long long)P.r->ng * P.r->nphi;
+            CKT(cudaMemsetAsync(P.maxrel, 0, sizeof(unsigned long long), s));
+            const int blocks = (int)std::min<long long>((nall + 255) / 256, (long long)ctx->nsm * 8);
+            rb::accumulate_generation<<<blocks, 256, 0, s>>>(P.tot, hv.flux, nall, P.r->nphi, hv.np, hv.nm5, P.maxrel);
+            CKT(cudaGetLastError());
+            if (P.r->csd) {
+                rb::accumulate_generation<<<blocks, 256, 0, s>>>(P.tot_cut, hv.cutoff, P.r->nphi, P.r->nphi, hv.np,
+                                                                 hv.nm5, nullptr);
+                CKT(cudaGetLastError());
+            }
+            long long ps = 0;
+            int status = 0;
+            CKT(cudaMemcpyAsync(&ps, hv.passes, sizeof(long long), cudaMemcpyDeviceToHost, s));
+            CKT(cudaMemcpyAsync(&status, hv.status, sizeof(int), cudaMemcpyDeviceToHost, s));
+            CKT(cudaStreamSynchronize(s));
+            P.passes += ps;
+            if (status & RB_DEV_TIMEOUT) return cleanup(fail(ctx, RB_ERR_TIMEOUT, "a device wait gave up"));
+            if (status & RB_DEV_BAD_TABLE) return cleanup(fail(ctx, RB_ERR_INVALID, "singular cell system or bad table"));
+            // the sources this solution produces (transport.jl:96-107)
+            if (n == ngen_max && p == npart - 1) continue;
+            for (int qq = 0; qq < npart; qq++) {
+                const int j = order[qq];
+                if (n == ngen_max && qq <= p) continue;
+                if (i == j) {
+                    CKT(cudaMemsetAsync(P.pvol, 0, (size_t)nall * sizeof(double), s));
+                    continue;
+                }
+                const CoupledPair &q = pairs[(size_t)i * npart + j];
+                if (!q.sigma_s) continue;
+                const DevProblem &a = hv, &b = parts[j].with_fixed;
+                const size_t smem = 8 * ((size_t)a.ng * a.np + (size_t)b.ng * a.np);
+                dim3 grd((unsigned)a.ncell, (unsigned)b.nm5);
+                rb::particle_source_kernel<<<grd, 256, smem, s>>>(hv.flux, a.ng, a.np, a.nm5, a.mat, a.nmat, q.sigma_s,
+                                                                 q.ls, a.pl, q.transfer, q.map, parts[j].pvol, b.ng, b.np,
+                                                                 b.nm5, a.ncell);
+                CKT(cudaGetLastError());
+            }
+        }
+        if (n > 1) {  // the flux criterion (transport.jl:111-118)
+            int px = 0;
+            double emax = 0.0;
+            for (int i = 0; i < npart; i++) {
+                unsigned long long bits = 0;
+                CKT(cudaMemcpyAsync(&bits, parts[i].maxrel, sizeof(bits), cudaMemcpyDeviceToHost, s));
+                CKT(cudaStreamSynchronize(s));
+                double e;
+                memcpy(&e, &bits, sizeof(e));
+                emax = std::max(emax, e);
+                if (e < eps_gen) px++;
+            }
+            eps_last = emax;
+            if (px == npart) break;
+        }
+    }
+    // the summed solutions out, in the reference's layouts
+    for (int i = 0; i < npart; i++) {
+        CoupledPart &P = parts[i];
+        rb_sn_result *res = results[i];
+        const DevProblem &h = P.r->h;
+        if (res->flux) {
+            const size_t need = (size_t)P.r->ng * P.r->nphi;
+            if (need > ctx->stage_cap) {
+                if (ctx->d_stage) cudaFree(ctx->d_stage);
+                ctx->d_stage = nullptr;
+                ctx->stage_cap = 0;
+                CKT(cudaMalloc(&ctx->d_stage, need * sizeof(double)));
+                ctx->stage_cap = need;
+            }
+            dim3 blk(32, 8), grd((unsigned)((P.r->nphi + 31) / 32), (unsigned)((P.r->ng + 31) / 32));
+            rb::to_reference_layout<<<grd, blk, 0, s>>>(P.tot, ctx->d_stage, P.r->ng, P.r->nphi);
+            CKT(cudaGetLastError());
+            CKT(cudaMemcpyAsync(res->flux, ctx->d_stage, need * sizeof(double), cudaMemcpyDeviceToHost, s));
+            CKT(cudaStreamSynchronize(s));
+        }
+        if (res->flux_cutoff && P.r->csd)
+            CKT(cudaMemcpyAsync(res->flux_cutoff, P.tot_cut, P.r->nphi * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (res->rho) CKT(cudaMemcpyAsync(res->rho, h.rho, P.r->ng * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (res->group_resid) CKT(cudaMemcpyAsync(res->group_resid, h.resid, P.r->ng * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (res->group_iters) CKT(cudaMemcpyAsync(res->group_iters, h.iters, P.r->ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (res->group_converged)
+            CKT(cudaMemcpyAsync(res->group_converged, h.conv, P.r->ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CKT(cudaStreamSynchronize(s));
+        res->passes = P.passes;
+    }
+#undef CKT
+    if (generations) *generations = ngen;
+    if (eps_final) *eps_final = eps_last;
+    return cleanup(RB_OK);
 }

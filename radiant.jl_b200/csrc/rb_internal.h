@@ -67,7 +67,8 @@ struct DevProblem {
     const double *sigma_t;  // [ng,nmat]
     const double *sigma_s;  // [nmat,ng,ng,ls+1]
     const double *s_minus, *s_plus, *s_mom, *t_mom, *e_width;
-    const double *vol;      // [ng, nphi] or null
+    const double *vol;      // [ng][nphi] fixed volume sources (group-major) or null
+    const double *pvol;     // [ng][nphi] particle source of a coupled transport (rb_transport) or null
     const double *surf[6];  // [ng, np_source, face cells] or null
     int bc[6];
     // ---- work ---------------------------------------------------------------------------

@@ -643,7 +643,12 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, voi
                 const double *ss = P.sigma_s + m + (long long)nmat * (long long)ng * (ig + (long long)ng * P.pl[p]);
                 for (int gi = 0; gi < ig; gi++) q += ss[(long long)nmat * gi] * P.flux[(long long)gi * nphi + o];
             }
-            if (P.vol) q += P.vol[(long long)ig * nphi + o];
+            // the volume source: particle source + fixed source (transport.jl:89-90)
+            if (P.pvol || P.vol) {
+                double vs = P.pvol ? P.pvol[(long long)ig * nphi + o] : 0.0;
+                if (P.vol) vs = vs + P.vol[(long long)ig * nphi + o];
+                q += vs;
+            }
             P.qlout[o] = q;
         }
         if (P.csd && ig != 0) {  // 𝚽E12 .* ΔE[ig] / ΔE[ig-1]

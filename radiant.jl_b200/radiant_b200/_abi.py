@@ -51,6 +51,10 @@ class RbSnProblem(C.Structure):
     ]
 
 
+class RbCoupling(C.Structure):
+    _fields_ = [("sigma_s", _dp), ("ls", C.c_int32), ("transfer", _dp), ("moment_map", _ip)]
+
+
 class RbSnResult(C.Structure):
     _fields_ = [
         ("flux", _dp), ("flux_cutoff", _dp), ("rho", _dp), ("group_iters", _ip),
@@ -214,6 +218,8 @@ def load_library(path: str | None = None):
         "rb_poll": (C.c_int32, [vp, h64, RP]),
         "rb_energy_deposition": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32, _ip,
                                              _dp, _dp, _dp, _dp, C.c_double, _dp]),
+        "rb_transport": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(PP), C.POINTER(RbCoupling), C.c_int32,
+                                     C.c_double, C.c_int32, C.POINTER(RP), _ip, _dp]),
         "rb_version": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
@@ -228,7 +234,7 @@ def load_library(path: str | None = None):
 EXPORTED_SYMBOLS = (
     "rb_create", "rb_destroy", "rb_last_error", "rb_upload", "rb_solve", "rb_solve_batch",
     "rb_download", "rb_release", "rb_required_bytes", "rb_compute_flux", "rb_submit", "rb_poll",
-    "rb_energy_deposition", "rb_version",
+    "rb_energy_deposition", "rb_transport", "rb_version",
 )
 
 

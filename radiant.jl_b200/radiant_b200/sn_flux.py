@@ -172,6 +172,7 @@ def prepare_sn_tables(xs: MultigroupXS, ndims: int, ns, ds, mat, bc, sn: SNSetti
         ndims=ndims, ns=ns[:3], ds=[np.asarray(d, dtype=float) for d in ds], mat=np.asarray(mat).reshape(ns, order="F"),
         nmat=nmat, bc=list(bc) + [0] * (6 - len(bc)),
         nd=Nd, omega=[np.asarray(Om[0]), np.asarray(Om[1]), np.asarray(Om[2])], w=np.asarray(w),
+        qdims=Qdims, btype=sn.angular_boltzmann,
         np=Np, mn=Mn, dn=Dn, pl=pl, pm=pm, np_surf=Np_surf, mn_surf=Mn_s, dn_surf=Dn_s, n_to_nplus=n_to_np,
         order=O, nm=Nm, is_fc=sn.is_full_coupling, w_axis=w_axis, cc=Cc, ww=W, is_adaptive=is_adaptive,
         solver_type=st, ng=ng, sigma_t=sigma_t, ls=Ls, sigma_s=sigma_s, s_minus=s_minus, s_plus=s_plus,

@@ -444,3 +444,85 @@ def c5_stream(n: int, seed: int, precision: str = "mixed", max_cells: int = 2000
     rng = np.random.default_rng(seed)
     seeds = rng.integers(0, 2 ** 31 - 1, size=n)
     return [c5_request(int(s), precision, max_cells, max_groups, max_side) for s in seeds]
+
+
+# ------------------------------------------------------------------------------------------
+# coupled particles (transport())
+# ------------------------------------------------------------------------------------------
+def synthetic_coupling_xs(ng_in: int, ng_out: int, nmat: int, L: int, seed: int, strength: float) -> np.ndarray:
+    """Synthetic production cross sections Σs(i→j) [nmat, ng_in, ng_out, L+1] of a secondary
+    particle (labelled synthetic): from group gi into the groups gf ≥ gi of the other particle,
+    geometric fall-off, row sum `strength`·U(0.5, 1), anisotropy a^l."""
+    rng = np.random.default_rng(seed)
+    ss = np.zeros((nmat, ng_in, ng_out, L + 1))
+    for m in range(nmat):
+        c = strength * rng.uniform(0.5, 1.0)
+        aniso = rng.uniform(0.2, 0.8)
+        rate = rng.uniform(0.3, 1.5)
+        for gi in range(min(ng_in, ng_out)):
+            k = np.arange(ng_out - gi)
+            prof = np.exp(-k * rate)
+            prof /= prof.sum()
+            for l in range(L + 1):
+                ss[m, gi, gi:, l] = c * prof * aniso ** l
+    return ss
+
+
+COUPLING_STRENGTH = {(0, 1): 0.4, (0, 2): 0.1, (1, 0): 0.05, (2, 0): 0.3}  # γ→e⁻, γ→e⁺, e⁻→γ, e⁺→γ
+
+
+def coupled_particles(ndims: int = 1, seed: int = 1, precision: str = "fp64", ng: int = 10, n=None,
+                      photon_quad: int = 8, positron_quad: int | None = None, L: int = 3, dg_electron: bool = True,
+                      tol: float = 1e-9):
+    """Photon (BTE), electron and positron (BFP, CSD) on one geometry with the synthetic
+    couplings γ→e⁻, γ→e⁺, e⁻→γ, e⁺→γ; photon beam on the X- face in the top group. The electron
+    uses the photon's quadrature (identity angular transfer); the positron another order
+    (transfer through its Dn); with `dg_electron` the electron carries linear DG moments in x and
+    E (a non-trivial cell-moment map). Returns (tables per particle, {(i, j): Coupling})."""
+    from .transport import build_coupling
+
+    positron_quad = positron_quad or max(2, photon_quad - 2)
+    nmat = 2
+    parts = []
+    if ndims == 1:
+        nx = n or 60
+        mats = np.ones(nx, dtype=np.int32)
+        mats[nx // 3:nx // 2] = 2
+        widths = np.full(nx, 6.0 / nx)
+    else:
+        n = list(n or ([12, 10] if ndims == 2 else [6, 5, 4]))
+        mats = np.ones(n, dtype=np.int32)
+        sl = tuple(slice(k // 3, k // 2 + 1) for k in n)
+        mats[sl] = 2
+        widths = [np.full(k, 3.0 / k) for k in n]
+    for k, part in enumerate(("photon", "electron", "positron")):
+        bfp = part != "photon"
+        quad = positron_quad if part == "positron" else photon_quad
+        dg = dg_electron and part == "electron"
+        axes = ["x", "y", "z"][:ndims]
+        st = {a: "DD" for a in axes}
+        so = {a: 1 for a in axes}
+        if dg:
+            st["x"], so["x"] = "DG", 2
+        if bfp:
+            st["E"], so["E"] = ("DG", 2) if dg else ("DD", 1)
+        sn = SNSettings(solver_type="BFP" if bfp else "BTE",
+                        quadrature_type="gauss-legendre" if ndims == 1 else "carlson", quadrature_order=quad,
+                        legendre_order=L, scheme_type=st, scheme_order=so, acceleration="gmres",
+                        convergence_criterion=tol, angular_fokker_planck="galerkin")
+        xs = synthetic_xs(ng, nmat, L, seed * 17 + k, csd=bfp, e_top=6.0, e_cut=0.01)
+        if ndims == 1:
+            t = slab_tables(nx, widths, mats, ng, nmat, seed, sn, L, beam_group=0 if k == 0 else None, csd=bfp,
+                            precision=precision, xs=xs)
+        else:
+            beam = ("X-", 0, (0.8, 0.6, 0.0), {1: (0.5, 2.5)}) if k == 0 else None
+            t = grid_tables(ndims, n, widths, mats, ng, nmat, seed, sn, L, beam=beam, csd=bfp,
+                            precision=precision, xs=xs)
+        t["particle"] = part
+        parts.append(t)
+    couplings = {}
+    for (i, j), s in COUPLING_STRENGTH.items():
+        Li = int(np.max(parts[i]["pl"]))
+        ss = synthetic_coupling_xs(ng, ng, nmat, Li, seed * 31 + 3 * i + j, s)
+        couplings[(i, j)] = build_coupling(parts[i], parts[j], ss)
+    return parts, couplings
