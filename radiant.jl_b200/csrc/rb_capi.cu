@@ -300,28 +300,26 @@ float tf32_round(float x) {
     return r;
 }
 
-// Packs operator parts A_p[i + lda·k] (ni rows, nk columns) for tc_product (rb_tc.cuh): blocks of
-// 128 rows × 32 K, block (p, m, kc) at ((p·mtiles + m)·kchunks + kc)·2·4096 floats, the TF32 high
-// part then the low part v − hi, each element (r, k) at byte (r%8)·16 + (r/8)·1024 + (k%4)·4 +
-// (k/4)·128 of its block (the K-major, no-swizzle canonical layout). Zero outside the operator.
+// Packs operator parts A_p[i + lda·k] (ni rows, nk columns each) for tc_product (rb_tc.cuh), the
+// parts stacked along K (K = parts·nk, k' = p·nk + k): NJ = ni rounded up to 16 rows, chunks of 32
+// K, chunk kc at kc·2·NJ·32 floats holding the TF32 high block then the low block v − hi, element
+// (r, k') at byte (r%8)·16 + (r/8)·1024 + (k'%4)·4 + ((k'%32)/4)·128 of its block (the K-major,
+// no-swizzle canonical layout). Zero outside the operator.
 std::vector<float> pack_tc_operator(const std::vector<const double *> &parts, int lda, int ni, int nk) {
-    const int mtiles = (ni + 127) / 128, kch = (nk + 31) / 32;
-    std::vector<float> out((size_t)parts.size() * mtiles * kch * 2 * 4096, 0.0f);
-    for (size_t p = 0; p < parts.size(); p++)
-        for (int m = 0; m < mtiles; m++)
-            for (int kc = 0; kc < kch; kc++) {
-                const size_t base = ((((size_t)p * mtiles + m) * kch + kc) * 2) * 4096;
-                for (int r = 0; r < 128; r++)
-                    for (int kk = 0; kk < 32; kk++) {
-                        const int i = 128 * m + r, k = 32 * kc + kk;
-                        if (i >= ni || k >= nk) continue;
-                        const double v = parts[p][i + (size_t)lda * k];
-                        const float hi = tf32_round((float)v);
-                        const float lo = (float)(v - (double)hi);
-                        const size_t e = (size_t)((r % 8) * 16 + (r / 8) * 1024 + (kk % 4) * 4 + (kk / 4) * 128) / 4;
-                        out[base + e] = hi;
-                        out[base + 4096 + e] = lo;
-                    }
+    const int NJ = (ni + 15) & ~15, K = (int)parts.size() * nk, kch = (K + 31) / 32;
+    const size_t blk = (size_t)NJ * 32;
+    std::vector<float> out((size_t)kch * 2 * blk, 0.0f);
+    for (int kc = 0; kc < kch; kc++)
+        for (int r = 0; r < ni; r++)
+            for (int kk = 0; kk < 32; kk++) {
+                const int k = 32 * kc + kk;
+                if (k >= K) continue;
+                const double v = parts[k / nk][r + (size_t)lda * (k % nk)];
+                const float hi = tf32_round((float)v);
+                const float lo = (float)(v - (double)hi);
+                const size_t e = (size_t)((r % 8) * 16 + (r / 8) * 1024 + (kk % 4) * 4 + (kk / 4) * 128) / 4;
+                out[(size_t)kc * 2 * blk + e] = hi;
+                out[(size_t)kc * 2 * blk + blk + e] = lo;
             }
     return out;
 }
@@ -730,13 +728,13 @@ int launch_grid(rb_context *ctx, DevProblem *prob, const DevProblem &hp, cudaStr
     if (h.ndims == 3 && h.nm5 == 1 && h.nm4 == 1 && h.nmf[0] == 1 && h.nmf[1] == 1 && h.nmf[2] == 1)
         need = mixed ? (h.csd ? rb::oct3d_smem<float, true>() : rb::oct3d_smem<float, false>())
                      : (h.csd ? rb::oct3d_smem<double, true>() : rb::oct3d_smem<double, false>());
-    if (mixed && h.tc_m2d) {
+    if (mixed && h.tc_m2d) {  // the products: operator resident where it fits, else streamed
         const int parts = h.mnfp ? 2 : 1;
-        const int mt_m = (h.nd + 127) / 128, mt_d = (h.np + 127) / 128;
-        long long tcn = std::max(rb::tc::stage_bytes(parts, mt_m, parts, 128), rb::tc::stage_bytes(1, mt_d, 1, 128));
-        if (tcn > avail)
-            tcn = std::max(rb::tc::stage_bytes(parts, mt_m, parts, 64), rb::tc::stage_bytes(1, mt_d, 1, 64));
-        need = std::max(need, tcn);
+        auto plan = [&](int nj, int nk) {
+            const long long r = rb::tc::bytes_resident(rb::tc::round16(nj), nk);
+            return r <= avail ? r : rb::tc::bytes_streamed(rb::tc::round16(nj));
+        };
+        need = std::max(need, std::max(plan(h.nd, parts * h.np), plan(h.np, h.nd)));
     }
     if (need > avail) need = 0;  // the problem then takes the paths that need no region
     const int local_bytes = (int)((need + 1023) & ~1023LL);

@@ -13,7 +13,7 @@ __global__ void __launch_bounds__(RB_THREADS, 1) solve_grid_kernel(DevProblem *p
     GridTeam t;
     t.init(&gs.team, gpart);
     // the mixed form's 2D/3D products run on the tensor cores: every CTA holds TMEM columns for
-    // their accumulators and an mbarrier for MMA completion for the whole launch
+    // their accumulators and the mbarriers of MMA completion for the whole launch
     const bool use_tc = prob->precision == 1 && prob->ndims >= 2 && prob->tc_m2d != nullptr;
     if (threadIdx.x == 0) {
         gs.tc.ready = 0;
@@ -21,7 +21,10 @@ __global__ void __launch_bounds__(RB_THREADS, 1) solve_grid_kernel(DevProblem *p
     }
     if (use_tc) {
         if (threadIdx.x < 32) tc::tmem_alloc(&gs.tc.tmem, RB_TC_TMEM_COLS);
-        if (threadIdx.x == 0) tc::mbar_init(&gs.tc.mbar);
+        if (threadIdx.x == 0) {
+            tc::mbar_init(&gs.tc.mbar[0]);
+            tc::mbar_init(&gs.tc.mbar[1]);
+        }
         tc::fence_before();
         __syncthreads();
         tc::fence_after();

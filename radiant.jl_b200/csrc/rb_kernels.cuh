@@ -221,10 +221,11 @@ __device__ void lu_solve_rt(R *S, R *q, int n) {  // S is n×n, leading dimensio
 // ------------------------------------------------------------------------------------------
 // per-CTA shared state
 // ------------------------------------------------------------------------------------------
-// The tensor-core state of a CTA (rb_tc.cuh): TMEM base address, the MMA-completion mbarrier
-// and the parity of its next phase. ready = 0 in kernels that do not allocate TMEM.
+// The tensor-core state of a CTA (rb_tc.cuh): TMEM base address, the MMA-completion mbarriers
+// of the two column stages and the parities of their next phases (bit s). ready = 0 in kernels
+// that do not allocate TMEM.
 struct TcState {
-    uint64_t mbar;
+    uint64_t mbar[2];
     unsigned tmem;
     unsigned phase;
     int ready;

@@ -5,33 +5,41 @@
 // (Qn = Mn[n,:]·Ql, 𝚽l += Dn[:,n]·𝚽n) with the in-group scattering (scattering_source.jl:25-30)
 // and Fokker-Planck (fokker_planck_source.jl:29-33) sources folded in, as team_product does in
 // FP64 (rb_kernels.cuh):
-//   M2D  ψ[n,col] = pre + Σ_p Mn[n,p]·ys[mat,p]·𝚽[p,col] + T[mat]·Σ_p (Mn·ℳ)[n,p]·𝚽[p,col]
-//   D2M  z[p,col] = pre ∓ Σ_n Dn[p,n]·ψ[n,col]
-// The operator (Mn, Mn·ℳ or Dn, "A") is small and fixed per problem; the columns (cells × cell
-// moments, "B") are many. Split precision: every FP32 value x is hi + lo with hi = tf32(x) and
-// lo = x − hi, and a product is A_hi·B_hi + A_hi·B_lo + A_lo·B_hi (the dropped A_lo·B_lo is
-// ~2^-22 of it), accumulated in FP32 in TMEM: about FP32 accuracy at tensor-core rate.
+//   M2D  ψ[col,n] = pre + Σ_p ys[mat,p]·𝚽[col,p]·Mn[n,p] + Σ_p T[mat]·𝚽[col,p]·(Mn·ℳ)[n,p]
+//   D2M  z[col,p] = pre ∓ Σ_n ψ[col,n]·Dn[p,n]
+// A column ("col") is one cell moment of one cell; its values are contiguous in memory (the
+// moments 𝚽[col·np + p], the directions ψ[col·nd + n]). The products run with the columns as
+// the M side of the MMA (128 columns per tile, TMEM lane = column) and the operator as the N side
+// (N = directions or moments, up to 256), so a thread stages and stores the contiguous run of one
+// column. Operator parts are stacked along K (K = parts·nk): the Fokker-Planck part of M2D takes
+// its per-cell factor T[mat] on the column side, and one accumulator holds the whole sum.
 //
-// Layout. A is packed on the host (rb_capi.cu, pack_tc_operator) into blocks of 128 rows × 32 K,
-// hi block then lo block, each in the K-major no-swizzle canonical layout of the UMMA
-// descriptors: element (r, k) at byte (r%8)·16 + (r/8)·1024 + (k%4)·4 + (k/4)·128, i.e. 8×16-byte
-// core matrices, K-adjacent core matrices 128 bytes apart (LBO) and 8-row groups 1024 bytes apart
-// (SBO). B is staged by the CTA's threads into the same layout (N columns × 32 K): each thread
-// reads 4 consecutive K of a column (32 contiguous bytes) and writes one 16-byte row of a core
-// matrix, so a quarter-warp writes 128 contiguous bytes (no bank conflict).
+// Split precision: every FP32 value x is hi + lo with hi = tf32(x) and lo = x − hi, and a product
+// is A_hi·B_hi + A_hi·B_lo + A_lo·B_hi (the dropped A_lo·B_lo is ~2^-22 of it), accumulated in
+// FP32 in TMEM: about FP32 accuracy at tensor-core rate.
 //
-// Per CTA and column tile of N columns: for each 32-deep K chunk the threads load the next
-// chunk's B values into registers, wait for the MMAs of the previous chunk (mbarrier signalled
-// by tcgen05.commit), stage A and B in shared memory, and one thread issues 4 K-steps × 3 split
-// terms of tcgen05.mma per (part, 128-row tile). The epilogue reads the accumulators back with
-// tcgen05.ld (warp w reads TMEM lanes 32·(w%4)..+31, i.e. 32 consecutive output rows, so the
-// stores of a column are coalesced) and applies the scale, the pre-added term and the store.
+// Layout. Both operands are K-major, no swizzle, in the canonical layout of the UMMA
+// descriptors: 8 rows × 16 bytes core matrices, K-adjacent core matrices 128 bytes apart (LBO),
+// 8-row groups 1024 bytes apart (SBO): element (r, k) of a 32-deep K chunk at byte
+// (r%8)·16 + (k%4)·4 + (k/4)·128 + (r/8)·1024. The operator is packed on the host
+// (rb_capi.cu, pack_tc_operator): chunk kc of NJ rows (NJ = rows rounded up to 16), TF32 high
+// block then low block, NJ·32 floats each. It is either copied into shared memory once per
+// product (when it fits beside two column stages) or streamed chunk by chunk with the columns.
+//
+// Pipeline of one CTA over its column tiles: for each 32-deep K chunk the threads load the
+// chunk of their column (two threads per column, 16 K each), wait until the MMAs that last read
+// the stage are done (one mbarrier per stage, signalled by tcgen05.commit), write the split
+// values into the stage, and one thread issues 4 K-steps × 3 split terms of tcgen05.mma; the
+// two stages alternate, so a chunk's loads overlap the previous chunk's MMAs. After a tile's last
+// chunk the epilogue reads the accumulators with tcgen05.ld (warp w reads TMEM lanes
+// 32·(w%4)..+31, i.e. 32 columns, and half of the 8-wide output groups), adds the pre term and
+// stores each column's contiguous run. Every wait is bounded (RB_DEV_TIMEOUT on expiry).
 // This code runs on one GPU only and reads only this GPU's memory; it issues no TMA copies.
 #pragma once
 #include "rb_kernels.cuh"
 
 #define RB_TC_KC 32          // K per staged chunk
-#define RB_TC_BLOCK 4096     // floats in one 128×32 operator block
+#define RB_TC_M 128          // columns per tile (MMA M)
 #define RB_TC_TMEM_COLS 512  // tensor-memory columns a CTA allocates for the accumulators
 
 namespace rb {
@@ -97,18 +105,15 @@ __device__ __forceinline__ void tmem_alloc(uint32_t *dst, uint32_t ncols) {
 __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
 }
-// 16 consecutive FP32 columns of the warp's 32 TMEM lanes (one value per lane and column).
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(addr));
+// 8 consecutive FP32 columns of the warp's 32 TMEM lanes (one value per lane and column).
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, float (&v)[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(addr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ float tf32_hi(float x) {
@@ -117,158 +122,177 @@ __device__ __forceinline__ float tf32_hi(float x) {
     return __uint_as_float(r);
 }
 
-// Shared memory (bytes) a product with `parts` operator parts of `mtiles` 128-row tiles, `nb` B
-// operands and N columns per tile stages per K chunk.
-__host__ __device__ constexpr long long stage_bytes(int parts, int mtiles, int nb, int N) {
-    return (long long)parts * mtiles * 2 * RB_TC_BLOCK * 4 + (long long)nb * 2 * N * RB_TC_KC * 4;
+// 16-byte asynchronous copy global -> shared, L2 only
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_commit_wait_all() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+// Bytes of one column stage (hi and lo of 128 columns × 32 K) and of one operator chunk.
+__host__ __device__ constexpr long long col_stage_bytes() { return 2LL * RB_TC_M * RB_TC_KC * 4; }
+__host__ __device__ constexpr long long op_chunk_bytes(int nj) { return 2LL * nj * RB_TC_KC * 4; }
+// Shared memory of a product whose operator has nj rows (rounded to 16) and K = nk: resident
+// operator (all chunks) plus two column stages, or two stages of (column chunk + operator chunk).
+__host__ __device__ constexpr long long bytes_resident(int nj, int nk) {
+    return ((nk + RB_TC_KC - 1) / RB_TC_KC) * op_chunk_bytes(nj) + 2 * col_stage_bytes();
+}
+__host__ __device__ constexpr long long bytes_streamed(int nj) { return 2 * (col_stage_bytes() + op_chunk_bytes(nj)); }
+__host__ __device__ constexpr int round16(int n) { return (n + 15) & ~15; }
 
 }  // namespace tc
 
-// C[i, col] = Σ_k A_p[i,k]·B_b(p)[k,col] for every operator part p (b(p) = min(p, nb−1)) over
-// column tiles of N columns dealt to the team's CTAs; B_0[k,col] = scale0(k,col)·X[k + ldx·col],
-// B_1[k,col] = X[k + ldx·col]. The epilogue object provides pre(i, col) (the term added to the
-// product), scale(col) (the factor of part 1) and store(i, col, acc0 + scale·acc1, pre).
-// opA: packed operator, block (p, mtile, kchunk) at ((p·mtiles + m)·kchunks + kc)·2·RB_TC_BLOCK
-// floats (hi block, then lo). Returns false (without touching any output) if it does not fit.
-template <int N, class TX, class Team, class Scale, class Epi>
-__device__ bool tc_product(Team &t, TcState &ts, unsigned char *sm, long long sm_bytes, const float *opA, int parts,
-                           int ni, int nk, int nb, const TX *X, int ldx, long long ncol, Scale scale0, Epi epi,
-                           int *status) {
-    const int mtiles = (ni + 127) / 128, kchunks = (nk + RB_TC_KC - 1) / RB_TC_KC;
-    if (!ts.ready || ni > 256 || parts * mtiles * N > RB_TC_TMEM_COLS || tc::stage_bytes(parts, mtiles, nb, N) > sm_bytes)
-        return false;
-    constexpr int CPT = N / 32;                 // columns per thread in the B staging
-    constexpr uint32_t IDESC = tc::idesc_tf32(128, N);
-    float *sA = reinterpret_cast<float *>(sm);  // [parts·mtiles][hi,lo][RB_TC_BLOCK]
-    float *sB = sA + (long long)parts * mtiles * 2 * RB_TC_BLOCK;  // [nb][hi,lo][N·32]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // B staging: a warp covers 8 columns × 16 K of each 32 columns (lanes 8·q..8·q+7 take the
-    // 4-deep K group k4 of 8 neighbouring columns), so a load instruction touches 8 columns'
-    // contiguous K runs and a quarter-warp stores 128 contiguous bytes
-    const int k4 = (lane >> 3) + 4 * (warp & 1);  // this thread's 4-deep K group of the chunk (0..7)
-    const int cw = (lane & 7) + 8 * (warp >> 1);   // its column inside each group of 32
-    const long long ntile = (ncol + N - 1) / N;
-    uint32_t ph = ts.phase;  // parity of the next MMA completion (identical in every thread)
-    for (long long tl = t.crank; tl < ntile; tl += t.ncta) {
-        const long long c0 = tl * N;
-        for (int kc = 0; kc < kchunks; kc++) {
-            // this chunk's B values: CPT columns × 4 K
-            float xv[CPT][4], x0[CPT][4];
+// One 16-K half chunk of a column into registers: k0 = first K (stacked over the parts: part
+// k / nkp, index k % nkp), X[col·ldx + index], times scale(part, col, index); zero past K.
+template <class TX, class Scale>
+__device__ __forceinline__ void tc_load_half(float (&xv)[16], const TX *X, long long ldx, long long col, bool colok,
+                                             int k0, int nk, int nkp, bool vec, Scale scale) {
+    const int part = k0 / nkp, kk0 = k0 % nkp;
+    if (colok && vec && (kk0 * (int)sizeof(TX)) % 16 == 0 && kk0 + 16 <= nkp && k0 + 16 <= nk) {
+        // one part, aligned: 16-byte loads of the contiguous run
+        const TX *src = X + col * ldx + kk0;
+        double v[16];
+        if constexpr (sizeof(TX) == 8) {
 #pragma unroll
-            for (int j = 0; j < CPT; j++) {
-                const long long col = c0 + cw + 32 * j;
+            for (int q = 0; q < 8; q++) {
+                const double2 d = *reinterpret_cast<const double2 *>(src + 2 * q);
+                v[2 * q] = d.x;
+                v[2 * q + 1] = d.y;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const float4 f = *reinterpret_cast<const float4 *>(src + 4 * q);
+                v[4 * q] = f.x; v[4 * q + 1] = f.y; v[4 * q + 2] = f.z; v[4 * q + 3] = f.w;
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 16; e++) xv[e] = (float)(scale(part, col, kk0 + e) * v[e]);
+        return;
+    }
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+        const int k = k0 + e;
+        float x = 0.0f;
+        if (colok && k < nk) {
+            const int p = k / nkp, kk = k % nkp;
+            x = (float)(scale(p, col, kk) * (double)X[col * ldx + kk]);
+        }
+        xv[e] = x;
+    }
+}
+
+// D[col, j] = Σ_k Xs[col, k]·Op[j, k] over the team's column tiles (tiles dealt round robin to
+// the CTAs), k over the stacked parts (K = parts·nkp), Xs[col, k] = scale(k / nkp, col, k % nkp)·
+// X[col·ldx + k % nkp]; then epi(col, j0, acc[8]) stores the outputs j0..j0+7 of a column.
+// opA: the packed operator (NJ = round16(nj) rows). Returns false (no output touched) where it
+// does not fit.
+template <class TX, class Team, class Scale, class Epi>
+__device__ bool tc_product(Team &t, TcState &ts, unsigned char *sm, long long sm_bytes, const float *opA, int nj,
+                           int nkp, int parts, const TX *X, long long ldx, long long ncol, Scale scale, Epi epi,
+                           int *status) {
+    const int NJ = tc::round16(nj), nk = nkp * parts, kch = (nk + RB_TC_KC - 1) / RB_TC_KC;
+    if (!ts.ready || NJ > 256 || NJ > RB_TC_TMEM_COLS) return false;
+    const bool resident = tc::bytes_resident(NJ, nk) <= sm_bytes;
+    if (!resident && tc::bytes_streamed(NJ) > sm_bytes) return false;
+    const long long opc = tc::op_chunk_bytes(NJ) / 4, cst = tc::col_stage_bytes() / 4;  // floats
+    // regions: [operator: all chunks (resident) | one chunk per stage][column stages]
+    float *sOp = reinterpret_cast<float *>(sm);
+    float *sCol = sOp + (resident ? kch * opc : 2 * opc);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int half = tid >> 7, cm = tid & 127;  // this thread's half chunk and column of a tile
+    const bool vec = ((ldx * (long long)sizeof(TX)) % 16 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+    const uint32_t IDESC = tc::idesc_tf32(RB_TC_M, NJ);
+    if (resident) {  // the whole operator, once
+        const float4 *src = reinterpret_cast<const float4 *>(opA);
+        for (long long e = tid; e < kch * opc / 4; e += blockDim.x) tc::cp16(reinterpret_cast<float4 *>(sOp) + e, src + e);
+        tc::cp_commit_wait_all();
+    }
+    uint32_t ph = ts.phase;  // bit s: parity of the next completion of stage s (same in all threads)
+    int pend = 0;            // bit s: stage s has MMAs not yet waited for
+    int g = 0;               // chunks issued in this call (stage = g & 1)
+    const long long ntile = (ncol + RB_TC_M - 1) / RB_TC_M;
+    for (long long tl = t.crank; tl < ntile; tl += t.ncta) {
+        const long long c0 = tl * RB_TC_M;
+        const long long col = c0 + cm;
+        const bool colok = col < ncol;
+        for (int kc = 0; kc < kch; kc++, g++) {
+            const int s = g & 1;
+            float xv[16];
+            tc_load_half(xv, X, ldx, col, colok, kc * RB_TC_KC + 16 * half, nk, nkp, vec, scale);
+            // the stage's previous MMAs are done
+            if (pend & (1 << s)) {
+                if (!tc::mbar_wait(&ts.mbar[s], (ph >> s) & 1) && tid == 0) atomicOr(status, RB_DEV_TIMEOUT);
+                ph ^= 1u << s;
+                pend &= ~(1 << s);
+            }
+            float *sO = resident ? sOp + kc * opc : sOp + s * opc;
+            if (!resident) {
+                const float4 *src = reinterpret_cast<const float4 *>(opA + kc * opc);
+                for (long long e = tid; e < opc / 4; e += blockDim.x) tc::cp16(reinterpret_cast<float4 *>(sO) + e, src + e);
+            }
+            // the column's 16 K, hi and lo, as four 16-byte rows of core matrices
+            float *hi = sCol + s * cst, *lo = hi + cst / 2;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                float h[4], l[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
-                    const int k = kc * RB_TC_KC + 4 * k4 + e;
-                    const bool in = col < ncol && k < nk;
-                    const double x = in ? (double)X[k + (long long)ldx * col] : 0.0;
-                    xv[j][e] = (float)x;
-                    x0[j][e] = in ? (float)(scale0(k, col) * x) : 0.0f;
+                    h[e] = tc::tf32_hi(xv[4 * q + e]);
+                    l[e] = xv[4 * q + e] - h[e];
                 }
+                const int k4 = 4 * half + q;
+                const int off = ((cm & 7) * 16 + (cm >> 3) * 1024 + k4 * 128) / 4;
+                *reinterpret_cast<float4 *>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
             }
-            // the previous chunk's MMAs have read shared memory
-            if (kc > 0) {
-                if (!tc::mbar_wait(&ts.mbar, ph & 1) && tid == 0) atomicOr(status, RB_DEV_TIMEOUT);
-                ph++;
-            }
-            // stage A: every (part, mtile) block of this chunk, hi and lo (16-byte copies)
-            {
-                const int nblk = parts * mtiles * 2;
-                const float4 *src4 = reinterpret_cast<const float4 *>(opA);
-                float4 *dst4 = reinterpret_cast<float4 *>(sA);
-                for (int e = tid; e < nblk * (RB_TC_BLOCK / 4); e += blockDim.x) {
-                    const int b = e / (RB_TC_BLOCK / 4), w = e % (RB_TC_BLOCK / 4);
-                    const int pm = b >> 1, hl = b & 1;
-                    const long long gb = ((long long)pm * kchunks + kc) * 2 + hl;
-                    dst4[e] = src4[gb * (RB_TC_BLOCK / 4) + w];
-                }
-            }
-            // stage B: hi/lo of each operand in the canonical layout (one 16-byte row per store)
-#pragma unroll
-            for (int b = 0; b < 2; b++) {
-                if (b >= nb) break;
-                float *hi = sB + (long long)b * 2 * N * RB_TC_KC, *lo = hi + N * RB_TC_KC;
-#pragma unroll
-                for (int j = 0; j < CPT; j++) {
-                    const int cl = cw + 32 * j;
-                    float h[4], l[4];
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const float x = b == 0 ? x0[j][e] : xv[j][e];
-                        h[e] = tc::tf32_hi(x);
-                        l[e] = x - h[e];
-                    }
-                    const int off = ((cl & 7) * 16 + (cl >> 3) * 1024 + k4 * 128) / 4;
-                    *reinterpret_cast<float4 *>(hi + off) = make_float4(h[0], h[1], h[2], h[3]);
-                    *reinterpret_cast<float4 *>(lo + off) = make_float4(l[0], l[1], l[2], l[3]);
-                }
-            }
+            if (!resident) tc::cp_commit_wait_all();
             tc::fence_async_smem();
             tc::fence_before();
             __syncthreads();
             if (tid == 0) {
                 tc::fence_after();
-                for (int p = 0; p < parts; p++) {
-                    const int b = p < nb ? p : nb - 1;
-                    const uint32_t bh = tc::saddr(sB + (long long)b * 2 * N * RB_TC_KC), bl = bh + N * RB_TC_KC * 4;
-                    for (int m = 0; m < mtiles; m++) {
-                        const uint32_t ah = tc::saddr(sA + (long long)(p * mtiles + m) * 2 * RB_TC_BLOCK);
-                        const uint32_t al = ah + RB_TC_BLOCK * 4;
-                        const uint32_t d = ts.tmem + (uint32_t)((p * mtiles + m) * N);
+                const uint32_t ah = tc::saddr(hi), al = tc::saddr(lo);
+                const uint32_t bh = tc::saddr(sO), bl = bh + (uint32_t)(opc / 2) * 4;
 #pragma unroll
-                        for (int s = 0; s < RB_TC_KC / 8; s++) {
-                            const uint32_t o = s * 256;
-                            const uint32_t acc = (kc > 0 || s > 0) ? 1u : 0u;
-                            tc::mma_tf32(d, tc::sdesc(ah + o, 128, 1024), tc::sdesc(bh + o, 128, 1024), IDESC, acc);
-                            tc::mma_tf32(d, tc::sdesc(ah + o, 128, 1024), tc::sdesc(bl + o, 128, 1024), IDESC, 1u);
-                            tc::mma_tf32(d, tc::sdesc(al + o, 128, 1024), tc::sdesc(bh + o, 128, 1024), IDESC, 1u);
-                        }
-                    }
+                for (int st = 0; st < RB_TC_KC / 8; st++) {
+                    const uint32_t o = st * 256;
+                    const uint32_t acc = (kc > 0 || st > 0) ? 1u : 0u;
+                    tc::mma_tf32(ts.tmem, tc::sdesc(ah + o, 128, 1024), tc::sdesc(bh + o, 128, 1024), IDESC, acc);
+                    tc::mma_tf32(ts.tmem, tc::sdesc(ah + o, 128, 1024), tc::sdesc(bl + o, 128, 1024), IDESC, 1u);
+                    tc::mma_tf32(ts.tmem, tc::sdesc(al + o, 128, 1024), tc::sdesc(bh + o, 128, 1024), IDESC, 1u);
                 }
-                tc::commit(&ts.mbar);
+                tc::commit(&ts.mbar[s]);
             }
+            pend |= 1 << s;
         }
-        // epilogue: the accumulators of this column tile
-        if (!tc::mbar_wait(&ts.mbar, ph & 1) && tid == 0) atomicOr(status, RB_DEV_TIMEOUT);
-        ph++;
+        // the tile's accumulators: wait for its last chunk's MMAs
+        {
+            const int s = (g - 1) & 1;
+            if (!tc::mbar_wait(&ts.mbar[s], (ph >> s) & 1) && tid == 0) atomicOr(status, RB_DEV_TIMEOUT);
+            ph ^= 1u << s;
+            pend &= ~(1 << s);
+        }
         tc::fence_after();
-        const int lg = warp & 3;                   // TMEM lane quarter of this warp
-        const int cbase = (warp >> 2) * (N / 2);   // its half of the columns
-#pragma unroll 1
-        for (int m = 0; m < mtiles; m++) {
-            const int i = 128 * m + 32 * lg + lane;
-#pragma unroll 1
-            for (int cc = 0; cc < N / 2; cc += 16) {
-                float a0[16], a1[16];
-                const uint32_t lanes = (uint32_t)(32 * lg) << 16;
-                tc::tmem_ld16(ts.tmem + lanes + (uint32_t)(m * N + cbase + cc), a0);
-                if (parts > 1)
-                    tc::tmem_ld16(ts.tmem + lanes + (uint32_t)((mtiles + m) * N + cbase + cc), a1);
-                else
-#pragma unroll
-                    for (int q = 0; q < 16; q++) a1[q] = 0.0f;
-                if (i < ni) {
-                    // every load the epilogue makes for the 16 outputs first, then the stores
-                    // (a store may alias those loads, so they are not interleaved)
-                    double pv[16], sv[16];
-#pragma unroll
-                    for (int q = 0; q < 16; q++) {
-                        const long long col = c0 + cbase + cc + q;
-                        pv[q] = col < ncol ? epi.pre(i, col) : 0.0;
-                        sv[q] = col < ncol ? epi.scale(col) : 0.0;
-                    }
-#pragma unroll
-                    for (int q = 0; q < 16; q++) {
-                        const long long col = c0 + cbase + cc + q;
-                        if (col < ncol) epi.store(i, col, (double)a0[q] + sv[q] * (double)a1[q], pv[q]);
-                    }
-                }
-            }
+        const int lq = warp & 3;  // TMEM lane quarter of this warp: columns c0 + 32·lq + lane
+        const long long ecol = c0 + 32 * lq + lane;
+        for (int j0 = 8 * (warp >> 2); j0 < NJ; j0 += 16) {
+            float a[8];
+            tc::tmem_ld8(ts.tmem + ((uint32_t)(32 * lq) << 16) + (uint32_t)j0, a);
+            if (ecol < ncol) epi(ecol, j0, a);
         }
         tc::fence_before();
         __syncthreads();  // every accumulator read before the next tile's MMAs overwrite them
     }
+    // no MMA left unwaited, so the next call starts from settled barriers
+    for (int s = 0; s < 2; s++)
+        if (pend & (1 << s)) {
+            if (!tc::mbar_wait(&ts.mbar[s], (ph >> s) & 1) && tid == 0) atomicOr(status, RB_DEV_TIMEOUT);
+            ph ^= 1u << s;
+        }
+    __syncthreads();
     if (tid == 0) ts.phase = ph;
     __syncthreads();
     return true;
@@ -287,20 +311,38 @@ __device__ bool m2d_tc(Team &t, const DevProblem &P, GroupShared &gs, TcState &t
     const double *tg = gs.tg;
     float *psi = P.psi32;
     const long long ncol = (long long)nm * P.ncell;
-    auto sc = [=] __device__(int k, long long col) { return ys[(long long)mat[col / nm] * np + k]; };
-    struct {
-        const double *add, *tg;
-        const int *mat;
-        float *psi;
-        int nd, nm, parts;
-        __device__ double pre(int i, long long col) const { return add ? add[col * nd + i] : 0.0; }
-        __device__ double scale(long long col) const { return parts > 1 ? tg[mat[col / nm]] : 0.0; }
-        __device__ void store(int i, long long col, double v, double p) const { psi[col * nd + i] = (float)(p + v); }
-    } epi{add, tg, mat, psi, nd, nm, parts};
-    unsigned char *sm = reinterpret_cast<unsigned char *>(smem);
-    if (tc_product<128>(t, ts, sm, smem_bytes, P.tc_m2d, parts, nd, np, parts, zin, np, ncol, sc, epi, P.status))
-        return true;
-    return tc_product<64>(t, ts, sm, smem_bytes, P.tc_m2d, parts, nd, np, parts, zin, np, ncol, sc, epi, P.status);
+    // part 0: ys[mat, p]·𝚽 against Mn; part 1: T[mat]·𝚽 against Mn·ℳ
+    auto sc = [=] __device__(int part, long long col, int k) -> double {
+        const int m = mat[col / nm];
+        return part == 0 ? ys[(long long)m * np + k] : tg[m];
+    };
+    const bool v4 = (nd % 4) == 0, v2 = (nd % 2) == 0;
+    auto epi = [=] __device__(long long col, int j0, const float (&a)[8]) {
+        float *dst = psi + col * nd + j0;
+        const double *pre = add ? add + col * nd + j0 : nullptr;
+        float o[8];
+        if (pre && v2 && j0 + 8 <= nd) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const double2 p2 = *reinterpret_cast<const double2 *>(pre + 2 * q);
+                o[2 * q] = (float)(p2.x + (double)a[2 * q]);
+                o[2 * q + 1] = (float)(p2.y + (double)a[2 * q + 1]);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; q++) o[q] = (j0 + q < nd) ? (float)((pre ? pre[q] : 0.0) + (double)a[q]) : 0.0f;
+        }
+        if (v4 && j0 + 8 <= nd) {
+            *reinterpret_cast<float4 *>(dst) = make_float4(o[0], o[1], o[2], o[3]);
+            *reinterpret_cast<float4 *>(dst + 4) = make_float4(o[4], o[5], o[6], o[7]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (j0 + q < nd) dst[q] = o[q];
+        }
+    };
+    return tc_product(t, ts, reinterpret_cast<unsigned char *>(smem), smem_bytes, P.tc_m2d, nd, np, parts, zin,
+                      (long long)np, ncol, sc, epi, P.status);
 }
 
 // The D2M product of a mixed-form 2D/3D pass on the tensor cores (FP32 angular buffer in, FP64
@@ -311,19 +353,31 @@ __device__ bool d2m_tc(Team &t, const DevProblem &P, TcState &ts, void *smem, lo
     if (!P.tc_d2m) return false;
     const int nd = P.nd, np = P.np, nm = P.nm5;
     const long long ncol = (long long)nm * P.ncell;
-    auto one = [] __device__(int, long long) { return 1.0; };
-    struct {
-        const double *zin;
-        double *zout;
-        int np, matvec;
-        __device__ double pre(int i, long long col) const { return matvec ? zin[col * np + i] : 0.0; }
-        __device__ double scale(long long) const { return 0.0; }
-        __device__ void store(int i, long long col, double v, double p) const { zout[col * np + i] = matvec ? p - v : v; }
-    } epi{zin, zout, np, matvec};
-    unsigned char *sm = reinterpret_cast<unsigned char *>(smem);
-    if (tc_product<128>(t, ts, sm, smem_bytes, P.tc_d2m, 1, np, nd, 1, P.psi32, nd, ncol, one, epi, P.status))
-        return true;
-    return tc_product<64>(t, ts, sm, smem_bytes, P.tc_d2m, 1, np, nd, 1, P.psi32, nd, ncol, one, epi, P.status);
+    auto one = [] __device__(int, long long, int) -> double { return 1.0; };
+    const bool v2 = (np % 2) == 0;
+    auto epi = [=] __device__(long long col, int j0, const float (&a)[8]) {
+        double *dst = zout + col * np + j0;
+        const double *pre = zin + col * np + j0;
+        if (v2 && j0 + 8 <= np) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                double2 r;
+                if (matvec) {
+                    const double2 p2 = *reinterpret_cast<const double2 *>(pre + 2 * q);
+                    r = make_double2(p2.x - (double)a[2 * q], p2.y - (double)a[2 * q + 1]);
+                } else {
+                    r = make_double2((double)a[2 * q], (double)a[2 * q + 1]);
+                }
+                *reinterpret_cast<double2 *>(dst + 2 * q) = r;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                if (j0 + q < np) dst[q] = matvec ? pre[q] - (double)a[q] : (double)a[q];
+        }
+    };
+    return tc_product(t, ts, reinterpret_cast<unsigned char *>(smem), smem_bytes, P.tc_d2m, np, nd, 1, P.psi32,
+                      (long long)nd, ncol, one, epi, P.status);
 }
 
 }  // namespace rb
