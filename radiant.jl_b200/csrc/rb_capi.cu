@@ -576,7 +576,7 @@ int required(const rb_sn_problem *P, const Derived &D, Layout &L, size_t offs[64
     offs[k++] = L.take<double>(3 * D.EsA.size());         // 14 EsA, EsB, Eout
     offs[k++] = L.take<double>(D.Kcsd.size());            // 15
     offs[k++] = L.take<double>(D.Bcsd.size());            // 16
-    offs[k++] = L.take<double>(1);                        // 17 (unused)
+    offs[k++] = L.take<unsigned long long>(RB_OCT_MAXCTA); // 17 progress flags of the 3D octant sweep
     offs[k++] = L.take<double>((size_t)ng * nmat);        // 18 sigma_t
     offs[k++] = L.take<double>((size_t)nmat * ng * ng * (P->ls + 1)); // 19 sigma_s
     offs[k++] = L.take<double>(D.csd ? (size_t)ng * nmat : 0);        // 20 s_minus
@@ -837,6 +837,7 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     h.pl = DP(int, 6); h.mnfp = D.mnfp.empty() ? nullptr : DP(double, 7); h.frow_m = DP(double, 8);
     h.frow_d = DP(double, 9); h.G = DP(double, 10); h.Gsrc = DP(double, 11); h.Gout = DP(double, 12);
     h.tang = DP(int, 13); h.Kcsd = DP(double, 15); h.Bcsd = DP(double, 16);
+    h.oct_flags = DP(unsigned long long, 17);
     h.EsA = DP(double, 14); h.EsB = h.EsA + D.EsA.size(); h.Eout = h.EsA + 2 * D.EsA.size();
     h.nfmax = D.nfmax;
     h.sigma_t = DP(double, 18); h.sigma_s = DP(double, 19);

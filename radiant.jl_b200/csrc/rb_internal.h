@@ -10,6 +10,7 @@
 #define RB_MAXFACE 16 // largest face-moment count
 #define RB_MAXORD 8   // largest closure order per axis
 #define RB_MAXMAT 64  // materials per problem held in shared memory
+#define RB_OCT_MAXCTA 1024  // CTAs of a team the 3D octant sweep can pace with progress flags
 
 // mixed form: in-group tolerance floor of a solve with the FP32 operator (its noise floor is near
 // 1e-7), and the tolerance of the first Krylov solve before the FP64 defect correction
@@ -81,6 +82,7 @@ struct DevProblem {
     double *kmat;      // [nmat][np] per-group in-group Σs of each moment's Legendre order
     double *scsd;      // [nmat][nm5*nm5] per-group CSD part of the cell matrix
     double *fexit;     // 1D: [nd][RB_MAXFACE] exit faces; 2D/3D: per-direction exits and z-face plane
+    unsigned long long *oct_flags;  // [RB_OCT_MAXCTA] 3D octant sweep: steps each CTA has published
     double *phiE_a, *phiE_b; // [nd*nm4*ncell] energy-face fluxes (in / out, swapped per group)
     double *cutoff;    // [nphi]
     // ---- results ------------------------------------------------------------------------

@@ -252,6 +252,7 @@ struct alignas(16) GroupShared {
     };
     TeamShared team;
     TcState tc;
+    unsigned oct_epoch;  // 3D octant sweeps run so far in this solve (identical in every CTA)
 };
 
 // Incoming x-face flux of a 1D direction: surface source into moment 1 plus the lagged

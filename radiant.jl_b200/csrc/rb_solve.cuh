@@ -597,6 +597,10 @@ __device__ void solve_problem(Team &t, const DevProblem &P, GroupShared &gs, voi
     if (P.vstride > P.nstate)
         for (int k = t.rank(); k < P.nvec; k += t.size()) P.vecs[(long long)k * P.vstride + P.nstate] = 0.0;
     if (P.csd) { vzero(t, phiE_in, nE); vzero(t, phiE_out, nE); }
+    // the octant sweep's progress flags count up from zero within this solve
+    if (P.ndims == 3)
+        for (int k = t.rank(); k < RB_OCT_MAXCTA; k += t.size()) P.oct_flags[k] = 0ull;
+    if (threadIdx.x == 0) gs.oct_epoch = 0;
     t.sync();
     long long npass = 0;
     for (int ig = 0; ig < ng; ig++) {

@@ -429,13 +429,76 @@ __device__ void sweep_md(Team &t, const DevProblem &P, GroupShared &gs, const do
 // Outgoing boundary moments of every face: b[p,is,side,cell] = Σ_n Dn_face[n][p]·exit[n][cell][is]
 // over the directions leaving through that side (sn_sweep_2D.jl:146-179, accumulated over n in
 // order as sn_inner_pass.jl:127-129 does).
+//
+// One thread per (face cell, face moment, side, block of PB half-range moments), neighbouring
+// lanes on neighbouring face cells: the exit loads of a warp are contiguous and its cosine and
+// half-range row loads are one address (one request, no divergence). The loads of 8 directions
+// go out together; a direction leaving through the other side enters with weight 0, which adds
+// exactly zero, so each moment is the sum over its side's directions in increasing n, as with one
+// thread per output. PB trades exit re-reads against threads (boundary_out_md picks it).
+template <int PB, class Team>
+__device__ void boundary_out_pb(Team &t, const DevProblem &P, const double *zin, double *zout, int matvec) {
+    const int nd = P.nd, nps = P.npsurf, nfm = P.nfmax;
+    const int npb = (nps + PB - 1) / PB;
+    const long long sstride = md_scratch_stride(P);
+    for (int a = 0; a < P.ndims; a++) {
+        const int nf = P.nmf[a];
+        const long long nfc = P.nb[a] / ((long long)nps * nf * 2);
+        const long long off = a == 0 ? 0 : (a == 1 ? (long long)P.ny * P.nz * nfm : ((long long)P.ny * P.nz + (long long)P.nx * P.nz) * nfm);
+        const long long offb = P.off_b[a];
+        const double *crow = P.cosv + (long long)a * nd;
+        const double *frow = P.frow_d + (long long)a * nd * nps;
+        const double *fex = P.fexit;
+        const long long nitem = nfc * nf * 2 * npb;
+        for (long long u = t.rank(); u < nitem; u += t.size()) {
+            const long long cell = u % nfc;
+            const long long rest = u / nfc;
+            const int is = (int)(rest % nf);
+            const int side = (int)((rest / nf) % 2);
+            const int p0 = (int)(rest / (2LL * nf)) * PB;
+            const double *ex = fex + off + cell * nfm + is;
+            double acc[PB];
+#pragma unroll
+            for (int q = 0; q < PB; q++) acc[q] = 0.0;
+            for (int n0 = 0; n0 < nd; n0 += 8) {
+                double v[8];
+                bool use[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int n = min(n0 + e, nd - 1);
+                    v[e] = ex[(long long)n * sstride];
+                    use[e] = n0 + e < nd && ((crow[n] >= 0.0) == (side == 1));
+                }
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const int n = min(n0 + e, nd - 1);
+                    const double *fr = frow + (long long)n * nps;
+#pragma unroll
+                    for (int q = 0; q < PB; q++) {
+                        const double w = fr[min(p0 + q, nps - 1)];
+                        acc[q] = fma(use[e] ? w : 0.0, v[e], acc[q]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < PB; q++) {
+                if (p0 + q >= nps) continue;
+                const long long k = offb + (p0 + q) + (long long)nps * (is + (long long)nf * (side + 2 * cell));
+                zout[k] = matvec ? zin[k] - acc[q] : acc[q];
+            }
+        }
+    }
+}
+
+// One thread per output, neighbouring lanes on neighbouring moments of one face cell (the exit
+// loads of a warp are one address): the layout for faces too small to give the blocked form
+// above a few items per thread.
 template <class Team>
-__device__ void boundary_out_md(Team &t, const DevProblem &P, const double *zin, double *zout, int matvec) {
+__device__ void boundary_out_rows(Team &t, const DevProblem &P, const double *zin, double *zout, int matvec) {
     const int nd = P.nd, nps = P.npsurf, nfm = P.nfmax;
     const long long sstride = md_scratch_stride(P);
     for (int a = 0; a < P.ndims; a++) {
         const int nf = P.nmf[a];
-        const long long ncell = P.nb[a] / ((long long)nps * nf * 2);
         const long long off = a == 0 ? 0 : (a == 1 ? (long long)P.ny * P.nz * nfm : ((long long)P.ny * P.nz + (long long)P.nx * P.nz) * nfm);
         for (long long o = t.rank(); o < P.nb[a]; o += t.size()) {
             const int p = (int)(o % nps);
@@ -451,8 +514,20 @@ __device__ void boundary_out_md(Team &t, const DevProblem &P, const double *zin,
             const long long k = P.off_b[a] + o;
             zout[k] = matvec ? zin[k] - s : s;
         }
-        (void)ncell;
     }
+}
+
+// Faces with many outputs per thread of the team take the blocked form with the largest moment
+// block that still gives every thread about two items; small faces take one thread per output.
+// Both forms give the same sums, in the same order.
+template <class Team>
+__device__ void boundary_out_md(Team &t, const DevProblem &P, const double *zin, double *zout, int matvec) {
+    long long outs = 0;
+    for (int a = 0; a < P.ndims; a++) outs += P.nb[a];
+    const long long want = 2LL * t.size();
+    if (outs / 16 >= want) boundary_out_pb<16>(t, P, zin, zout, matvec);
+    else if (outs / 4 >= want) boundary_out_pb<4>(t, P, zin, zout, matvec);
+    else boundary_out_rows(t, P, zin, zout, matvec);
 }
 
 }  // namespace rb

@@ -9,11 +9,12 @@
 // the y face of the pencil below comes by warp shuffle (it is the neighbouring lane); the z face
 // of the pencil behind comes through shared memory, double-buffered by step parity. Tiles hand
 // their outgoing y/z faces to the downstream tiles through per-direction face planes in global
-// memory. Every (octant batch, tile) is one task on one CTA of the team; the team advances in
-// stages of K local steps separated by team barriers, and a tile runs H stages behind each
-// upwind tile (H·K ≥ the tile's depth), so every face it reads was written one barrier earlier.
-// The cell's inputs (angular source, material, width, incoming energy-face flux) are loaded one
-// step ahead. Each cell sees the same upwind faces as in the reference's lexicographic order
+// memory. Every (octant batch, tile) is one task on one CTA of the team; a tile is paced by its
+// upwind tiles through per-CTA progress flags (a release after each pair of steps, an acquire
+// before the faces of a step are staged), so it runs about one tile height behind them with no
+// team barrier inside the sweep. The cell's inputs (angular source, material, incoming
+// energy-face flux, and the faces entering the tile) are staged one step ahead with cp.async.
+// Each cell sees the same upwind faces as in the reference's lexicographic order
 // (sn_sweep_3D.jl:73-110), so the result equals it up to rounding.
 //
 // 2D: the KBA wavefront of sweep_md (rows of a direction skewed by one column per row, y faces
@@ -23,7 +24,6 @@
 #include "rb_sweep_md.cuh"
 #include "rb_tc.cuh"
 
-#define RB_OCT_K 16      // wavefront steps per stage (3D)
 #define RB_OCT_TILE 16   // tile edge in pencils (3D): 16×16 pencils, one per thread
 
 namespace rb {
@@ -57,17 +57,38 @@ __device__ __forceinline__ bool one_moment_md(const DevProblem &P) {
 template <typename R> struct OctDB { static constexpr int value = 10; };  // FP64: registers
 template <> struct OctDB<float> { static constexpr int value = 12; };
 
-#define RB_OCT_NB 2  // stages of the angular source (cp.async, one step ahead)
+#define RB_OCT_NB 2        // stages of a step's inputs (cp.async, one step ahead)
+#define RB_OCT_MAXNX 1024  // x widths whose inverses the sweep keeps in shared memory
+#define RB_OCT_PUB 2       // a CTA publishes its progress every RB_OCT_PUB steps (and after its last)
 
-// Shared memory the 3D octant sweep needs (bytes): direction constants, z-face buffers, RB_OCT_NB
-// stages of the angular flux of one step's cells (and of the energy-face flux, CSD), the cells'
-// materials, and each pencil's cell base and depth.
+// Shared-memory plan of the 3D octant sweep (byte offsets, each array 16-byte aligned): the
+// staged upwind faces of the tile's first row and layer of pencils, RB_OCT_NB stages of a step's
+// angular source / flux, energy-face flux (CSD) and materials, the z-face hand-off between
+// pencils (double-buffered by step parity), the direction constants of the octant batch, the
+// inverse x widths and the per-material cell terms, and each pencil's cell base and coordinates.
 template <typename R, bool CSD>
-__host__ __device__ constexpr long long oct3d_smem() {
-    constexpr long long DB = OctDB<R>::value, TP = RB_OCT_TILE * RB_OCT_TILE, NB = RB_OCT_NB;
-    return (long long)sizeof(R) * (DB * 9 + 2 * DB * TP) + NB * TP * DB * (long long)sizeof(R) +
-           (CSD ? NB * TP * DB * 8 : 0) + TP * 8 + NB * TP * 4 + TP * 4;
-}
+struct Oct3dSmem {
+    static constexpr long long DB = OctDB<R>::value, T = RB_OCT_TILE, TP = T * T, NB = RB_OCT_NB;
+    static constexpr long long RS = (long long)sizeof(R);
+    static constexpr long long al(long long b) { return (b + 15) & ~15LL; }
+    static constexpr long long fy = 0;                                      // double [NB][T][DB]
+    static constexpr long long fz = fy + al(NB * T * DB * 8);               // double [NB][T][DB]
+    static constexpr long long eb = fz + al(NB * T * DB * 8);               // double [NB][TP][DB]
+    static constexpr long long pcb = eb + (CSD ? al(NB * TP * DB * 8) : 0); // long long [TP]
+    static constexpr long long dc = pcb + al(TP * 8);                       // R [DB][9]
+    static constexpr long long sfz = dc + al(DB * 9 * RS);                  // R [2][DB][TP]
+    static constexpr long long qb = sfz + al(2 * DB * TP * RS);             // R [NB][TP][DB]
+    static constexpr long long ix = qb + al(NB * TP * DB * RS);             // R [RB_OCT_MAXNX]
+    static constexpr long long ms = ix + al(RB_OCT_MAXNX * RS);             // R [RB_MAXMAT]
+    static constexpr long long mq = ms + al(RB_MAXMAT * RS);                // R [RB_MAXMAT]
+    static constexpr long long mb = mq + al(RB_MAXMAT * RS);                // int [NB][TP]
+    static constexpr long long pj = mb + al(NB * TP * 4);                   // int [TP]
+    static constexpr long long py = pj + al(TP * 4);                        // int [TP]
+    static constexpr long long pz = py + al(TP * 4);                        // int [TP]
+    static constexpr long long bytes = pz + al(TP * 4);
+};
+template <typename R, bool CSD>
+__host__ __device__ constexpr long long oct3d_smem() { return Oct3dSmem<R, CSD>::bytes; }
 __host__ __device__ constexpr long long oct3d_smem_max() {
     return oct3d_smem<double, true>() > oct3d_smem<float, true>() ? oct3d_smem<double, true>()
                                                                   : oct3d_smem<float, true>();
@@ -81,9 +102,11 @@ __device__ __forceinline__ int oct_ty(int ny) {
     return ty;
 }
 
-// The 3D octant sweep applies: one-moment cells, and one octant batch's tiles fit in the team.
+// The 3D octant sweep applies: one-moment cells, one octant batch's tiles fit in the team, every
+// CTA of the team has a progress flag, and the step and round counts fit their bit fields.
 __device__ __forceinline__ bool oct3d_ok(const DevProblem &P, int ncta, long long smem_bytes, int mixed) {
-    if (P.ndims != 3 || !one_moment_md(P)) return false;
+    if (P.ndims != 3 || !one_moment_md(P) || ncta > RB_OCT_MAXCTA) return false;
+    if (P.nx + 2 * RB_OCT_TILE >= (1 << 20) || P.nd >= (1 << 12)) return false;
     const int TY = oct_ty(P.ny), TZ = min(P.nz, RB_OCT_TILE);
     const int ntiles = ((P.ny + TY - 1) / TY) * ((P.nz + TZ - 1) / TZ);
     const long long need = mixed ? (P.csd ? oct3d_smem<float, true>() : oct3d_smem<float, false>())
@@ -102,19 +125,53 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// progress flags between the CTAs of a team (GPU-scope release / acquire)
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+// Waits until *f >= target; `seen` keeps the last value read. Gives up (false) after a bounded
+// number of polls (about a second), so a wait can never hang the GPU.
+__device__ __forceinline__ bool wait_progress(const unsigned long long *f, unsigned long long target,
+                                              unsigned long long &seen) {
+    if (seen >= target) return true;
+    for (int it = 0; it < (1 << 24); it++) {
+        seen = ld_acquire_u64(f);
+        if (seen >= target) return true;
+        if (it >= 32) __nanosleep(64);
+    }
+    return false;
+}
+
+// q / S of a cell: IEEE division in FP64 (the plain form), the fast reciprocal-based division
+// in FP32 (the mixed form, whose FP64 defect correction absorbs its 2-ulp error)
+__device__ __forceinline__ double oct_div(double q, double s) { return q / s; }
+__device__ __forceinline__ float oct_div(float q, float s) { return __fdividef(q, s); }
+
+// The sweep of one octant batch over one tile of pencils is a task; the tasks of a round (one per
+// CTA) run concurrently, and a tile is paced by the tiles upwind of it in y and z: before it
+// stages the faces of step s, thread 0 waits until the upwind tiles have published the steps that
+// write them (s + TY − 1 and s + TZ − 1 of their own counts). A CTA publishes the number of steps
+// it has completed, tagged with the sweep's epoch and the round, after a barrier that follows the
+// face stores and a GPU-scope fence, so a downstream tile runs about TY steps behind its upwind
+// tile with no team barrier inside the sweep.
 template <typename R, typename PS, bool CSD, class Team>
 __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShared &gs, void *smem, const double *zin,
                                          int np_source, const double *phiE_in, double *phiE_out, int ig, PS *psi) {
-    constexpr int DB = OctDB<R>::value, K = RB_OCT_K, TP = RB_OCT_TILE * RB_OCT_TILE, NB = RB_OCT_NB;
+    using L = Oct3dSmem<R, CSD>;
+    static_assert(sizeof(PS) == sizeof(R), "angular buffer and arithmetic of one width");
+    constexpr int DB = OctDB<R>::value, TT = RB_OCT_TILE, TP = TT * TT, NB = RB_OCT_NB;
     const int nd = P.nd, nx = P.nx, ny = P.ny, nz = P.nz, nfm = P.nfmax;
     const int TY = oct_ty(ny), TZ = min(nz, RB_OCT_TILE);
     const int nty = (ny + TY - 1) / TY, ntz = (nz + TZ - 1) / TZ, ntiles = nty * ntz;
     const int ngrp = oct_groups(P, DB);
     const int gpr = (int)t.ncta / ntiles;  // octant batches per round (≥ 1: oct3d_ok)
     const int nround = (ngrp + gpr - 1) / gpr;
-    const int H = 1 + (max(TY, TZ) - 1 + K - 1) / K;  // stages per tile hop
     const int nsteps = nx + TY + TZ - 2;
-    const int nstage = (nsteps + K - 1) / K + H * (nty - 1 + ntz - 1);
     // per-direction scratch (md_scratch_stride): exits x [ny·nz], y [nx·nz], z [nx·ny], the
     // z-face plane [nx·ny] and the y-face plane [nx·nz] handed between tiles, then the incoming
     // boundary fluxes (boundary_in_phase)
@@ -122,187 +179,259 @@ __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShar
     const long long eyo = (long long)ny * nz * nfm, ezo = eyo + (long long)nx * nz * nfm;
     const long long zoff = ezo + (long long)nx * ny * nfm, yoff = zoff + (long long)nx * ny * nfm;
     const long long xin = md_in_offset(P, 0), yin = md_in_offset(P, 1), zin_ = md_in_offset(P, 2);
-    // shared memory (oct3d_smem)
-    R *dc = reinterpret_cast<R *>(smem);  // [DB][9]: |cos|·G (3), |cos|·Gsrc (3), Gout (3)
-    R *sfz = dc + DB * 9;                  // [2][DB][TP]
-    PS *qb = reinterpret_cast<PS *>(sfz + 2 * DB * TP);                  // [NB][TP][DB] angular source / flux
-    double *eb = reinterpret_cast<double *>(qb + NB * TP * DB);          // [NB][TP][DB] energy-face flux
-    long long *pcb = reinterpret_cast<long long *>(eb + (CSD ? NB * TP * DB : 0));  // [TP] cell base, −1: none
-    int *mb = reinterpret_cast<int *>(pcb + TP);  // [NB][TP] material of the pencil's cell
-    int *pjs = mb + NB * TP;                      // [TP] jy + jz
+    unsigned char *base = reinterpret_cast<unsigned char *>(smem);
+    double *fyb = reinterpret_cast<double *>(base + L::fy);
+    double *fzb = reinterpret_cast<double *>(base + L::fz);
+    double *eb = reinterpret_cast<double *>(base + L::eb);
+    long long *pcb = reinterpret_cast<long long *>(base + L::pcb);
+    R *dc = reinterpret_cast<R *>(base + L::dc);
+    R *sfz = reinterpret_cast<R *>(base + L::sfz);
+    PS *qb = reinterpret_cast<PS *>(base + L::qb);
+    R *idxs = reinterpret_cast<R *>(base + L::ix);
+    R *mS = reinterpret_cast<R *>(base + L::ms);
+    R *mQ = reinterpret_cast<R *>(base + L::mq);
+    int *mb = reinterpret_cast<int *>(base + L::mb);
+    int *pjs = reinterpret_cast<int *>(base + L::pj);
+    int *piy = reinterpret_cast<int *>(base + L::py);
+    int *piz = reinterpret_cast<int *>(base + L::pz);
     const int me = threadIdx.x, jy = me % TY, jz = me / TY;
     const R w1x = (R)P.w1[0], w1y = (R)P.w1[1], w1z = (R)P.w1[2], w1e = (R)P.w1[3];
     const R esa = CSD ? (R)P.EsA[0] : R(0), esb = CSD ? (R)P.EsB[0] : R(0), eout = CSD ? (R)P.Eout[0] : R(0);
+    // this sweep's tables: inverse x widths, and per material Σt (+ the CSD cell term) and the
+    // factor of the incoming energy-face flux
+    const bool xs_sm = nx <= RB_OCT_MAXNX;
+    __syncthreads();
+    if (xs_sm)
+        for (int i = me; i < nx; i += blockDim.x) idxs[i] = (R)(1.0 / P.dx[i]);
+    for (int m = me; m < P.nmat; m += blockDim.x) {
+        const R sigt = (R)gs.sigt[m];
+        R scs = R(0), sq = R(0);
+        if (CSD) {
+            scs = (R)P.scsd[m];
+            sq = esa * (R)gs.sp[m] - esb * (R)gs.sm[m];
+        }
+        mS[m] = scs + sigt;
+        mQ[m] = sq;
+    }
+    if (me == 0) gs.oct_epoch++;
+    __syncthreads();
+    const unsigned long long epoch = (unsigned long long)gs.oct_epoch;
+    unsigned long long seen_y = 0, seen_z = 0;  // thread 0: the upwind flags as last read
+    bool gave_up = false;
     for (int rnd = 0; rnd < nround; rnd++) {
         const int g = rnd * gpr + (int)t.crank / ntiles;
         const int tile = (int)t.crank % ntiles;
         int first = 0, cnt = 0, oc = 0;
         if ((int)t.crank < gpr * ntiles && g < ngrp) oc = oct_group(P, DB, g, first, cnt);
+        if (cnt == 0) continue;  // uniform over the CTA
         const bool fx = !(oc & 1), fy = !(oc & 2), fz = !(oc & 4);
         const int tyq = tile % nty, tzq = tile / nty;  // tile coordinates in sweep order
-        const int dly = H * (tyq + tzq);
         const int iyy = tyq * TY + jy, izz = tzq * TZ + jz;
-        const bool pok = cnt > 0 && me < TY * TZ && iyy < ny && izz < nz;
+        const bool pok = me < TY * TZ && iyy < ny && izz < nz;
         const int iy = fy ? iyy : ny - 1 - iyy, iz = fz ? izz : nz - 1 - izz;
-        __syncthreads();
-        if (me < cnt) {
+        const unsigned long long tagr = (epoch << 32) | ((unsigned long long)rnd << 20);
+        const unsigned long long *upy = tyq > 0 ? P.oct_flags + (t.crank - 1) : nullptr;
+        const unsigned long long *upz = tzq > 0 ? P.oct_flags + (t.crank - nty) : nullptr;
+        __syncthreads();  // the previous round's readers of the region are done
+        if (me < DB) {
             const int n = first + me;
             for (int a = 0; a < 3; a++) {
-                const double ac = fabs(P.cosv[(long long)a * nd + n]);
                 const long long blk = (long long)n * 3 + a;
-                dc[me * 9 + a] = (R)(ac * P.G[blk]);
-                dc[me * 9 + 3 + a] = (R)(ac * P.Gsrc[blk * nfm]);
-                dc[me * 9 + 6 + a] = (R)P.Gout[blk * nfm];
+                const double ac = me < cnt ? fabs(P.cosv[(long long)a * nd + n]) : 0.0;
+                dc[me * 9 + a] = me < cnt ? (R)(ac * P.G[blk]) : R(0);
+                dc[me * 9 + 3 + a] = me < cnt ? (R)(ac * P.Gsrc[blk * nfm]) : R(0);
+                dc[me * 9 + 6 + a] = me < cnt ? (R)P.Gout[blk * nfm] : R(0);
             }
         }
         if (me < TP) {
             pcb[me] = pok ? (long long)nx * (iy + (long long)ny * iz) : -1;
             pjs[me] = jy + jz;
+            piy[me] = iy;
+            piz[me] = iz;
         }
         __syncthreads();
-        // Step sg's cells are staged cooperatively: element e = me + TP·r (r < cnt) of the step
-        // is direction k = e % cnt of pencil p = e / cnt, so consecutive lanes read consecutive
-        // directions of a cell (one contiguous run of cnt values per cell) instead of one lane
-        // per cell.
-        const int qd = cnt > 0 ? TP / cnt : 0, rm = cnt > 0 ? TP % cnt : 0;
-        const int p0 = cnt > 0 ? me / cnt : 0, k0 = cnt > 0 ? me % cnt : 0;
+        // A step's cells are staged cooperatively: element e = me + TP·r (r < cnt) of the step is
+        // direction k = e % cnt of pencil p = e / cnt, so consecutive lanes read consecutive
+        // directions of a cell (one contiguous run of cnt values per cell).
+        const int qd = TP / cnt, rm = TP % cnt, p0 = me / cnt, k0 = me % cnt;
         auto cell_of = [&](int p, int sg) -> long long {  // cell of pencil p at step sg, −1 if none
             const long long cb = pcb[p];
             const int ixx = sg - pjs[p];
             if (cb < 0 || ixx < 0 || ixx >= nx) return -1;
             return cb + (fx ? ixx : nx - 1 - ixx);
         };
-        auto issue = [&](int sg) {  // step sg's cells into buffer sg % NB (one commit group)
-            if (cnt > 0 && sg >= 0 && sg < nsteps) {
-                const int st = sg % NB;
+        // thread 0: the upwind tiles have published the steps that write the faces of step s
+        auto wait_up = [&](int s) {
+            if (me != 0 || gave_up || s < 0 || s >= nsteps) return;
+            bool ok = true;
+            if (upy) ok = wait_progress(upy, tagr | (unsigned long long)(min(s + TY - 1, nsteps - 1) + 1), seen_y);
+            if (ok && upz) ok = wait_progress(upz, tagr | (unsigned long long)(min(s + TZ - 1, nsteps - 1) + 1), seen_z);
+            if (!ok) {
+                gave_up = true;
+                atomicOr(P.status, RB_DEV_TIMEOUT);
+            }
+        };
+        // step s's inputs into stage s % NB (one commit group): angular source, energy-face flux,
+        // materials, and the faces entering the tile's pencils (0, jz) and (jy, 0)
+        auto issue = [&](int s) {
+            if (s >= 0 && s < nsteps) {
+                const int st = s % NB;
                 int p = p0, k = k0;
-                for (int r = 0; r < cnt; r++) {
-                    const long long c = cell_of(p, sg);
-                    if (c >= 0) {
-                        cp_async<sizeof(PS)>(qb + ((long long)st * TP + p) * DB + k, psi + first + k + (long long)nd * c);
-                        if (CSD && phiE_in)
-                            cp_async<8>(eb + ((long long)st * TP + p) * DB + k, phiE_in + first + k + (long long)nd * c);
+#pragma unroll
+                for (int r = 0; r < DB; r++) {
+                    if (r < cnt) {
+                        const long long c = cell_of(p, s);
+                        if (c >= 0) {
+                            const long long so = ((long long)st * TP + p) * DB + k;
+                            const long long go = first + k + (long long)nd * c;
+                            cp_async<sizeof(PS)>(qb + so, psi + go);
+                            if (CSD && phiE_in) cp_async<8>(eb + so, phiE_in + go);
+                        }
                     }
                     p += qd;
                     k += rm;
                     if (k >= cnt) { k -= cnt; p++; }
                 }
-                if (me < TP) {
-                    const long long c = cell_of(me, sg);
+                {
+                    const long long c = cell_of(me, s);
                     if (c >= 0) cp_async<4>(mb + st * TP + me, P.mat + c);
+                }
+                const int nfy = TZ * cnt, nfz = TY * cnt;
+                for (int e = me; e < nfy + nfz; e += blockDim.x) {
+                    const bool isy = e < nfy;
+                    const int e2 = isy ? e : e - nfy;
+                    const int j = e2 / cnt, kk = e2 % cnt;  // pencil (0, j) for y faces, (j, 0) for z faces
+                    const int pp = isy ? TY * j : j;
+                    const int ixx = s - j;
+                    if (pcb[pp] >= 0 && ixx >= 0 && ixx < nx) {
+                        const int ix = fx ? ixx : nx - 1 - ixx;
+                        const long long o = isy ? (tyq == 0 ? yin : yoff) + (ix + (long long)nx * piz[pp]) * nfm
+                                                : (tzq == 0 ? zin_ : zoff) + (ix + (long long)nx * piy[pp]) * nfm;
+                        cp_async<8>((isy ? fyb : fzb) + ((long long)st * TT + j) * DB + kk,
+                                    P.fexit + (long long)(first + kk) * sstride + o);
+                    }
                 }
             }
             cp_async_commit();
         };
         const R idy = pok ? (R)(1.0 / P.dy[iy]) : R(0), idz = pok ? (R)(1.0 / P.dz[iz]) : R(0);
         R fxs[DB], fyl[DB];
+        {
+            const long long o = xin + (iy + (long long)ny * iz) * nfm;  // the domain's incoming x faces
 #pragma unroll
-        for (int k = 0; k < DB; k++) fxs[k] = fyl[k] = R(0);
+            for (int k = 0; k < DB; k++) {
+                fyl[k] = R(0);
+                fxs[k] = (pok && k < cnt) ? (R)P.fexit[(long long)(first + k) * sstride + o] : R(0);
+            }
+        }
+        wait_up(0);
+        __syncthreads();
         issue(0);
-        for (int st = 0; st < nstage; st++) {
-            const int s0 = (st - dly) * K;
-            for (int u = 0; u < K; u++) {
-                const int sg = s0 + u;
-                if (cnt == 0 || sg < 0 || sg >= nsteps) continue;  // uniform over the CTA
-                cp_async_wait<0>();  // this thread's copies of step sg have landed
-                __syncthreads();     // everyone's, and step sg − 1's buffer is free again
-                issue(sg + 1);       // in flight while step sg is solved
-                const int ixx = sg - jy - jz;
-                const int rd = (sg + 1) & 1, wr = sg & 1, sb = sg % NB;
-                R fyi[DB];
+        for (int sg = 0; sg < nsteps; sg++) {
+            wait_up(sg + 1);
+            cp_async_wait<0>();  // this thread's copies of step sg have landed
+            __syncthreads();     // everyone's; step sg − 1's stage is free; step sg + 1's faces are written
+            issue(sg + 1);       // in flight while step sg is solved
+            const int ixx = sg - jy - jz;
+            const int rd = (sg + 1) & 1, wr = sg & 1, sb = sg % NB;
+            R fyi[DB];
 #pragma unroll
-                for (int k = 0; k < DB; k++) fyi[k] = __shfl_up_sync(0xffffffffu, fyl[k], 1);
-                if (pok && ixx >= 0 && ixx < nx) {
-                    const int ix = fx ? ixx : nx - 1 - ixx;
-                    const long long yk = (ix + (long long)nx * iz) * nfm, zk = (ix + (long long)nx * iy) * nfm;
-                    R fzi[DB];
-                    // faces entering the pencil: the domain's incoming fluxes (boundary_in_phase),
-                    // the upwind tile's face planes, or the neighbouring pencils
-                    if (ixx == 0) {
-                        const long long o = xin + (iy + (long long)ny * iz) * nfm;
+            for (int k = 0; k < DB; k++) fyi[k] = __shfl_up_sync(0xffffffffu, fyl[k], 1);
+            if (pok && ixx >= 0 && ixx < nx) {
+                const int ix = fx ? ixx : nx - 1 - ixx;
+                const long long yk = (ix + (long long)nx * iz) * nfm, zk = (ix + (long long)nx * iy) * nfm;
+                // every input of the cell first, then the arithmetic, then the stores (no shared
+                // store sits between two loads, so the directions' chains overlap)
+                R fzi[DB], qv[DB], fe[DB];
+                PS *qc = qb + ((long long)sb * TP + me) * DB;
+                double *ec = eb + ((long long)sb * TP + me) * DB;
+                if (jy == 0) {
 #pragma unroll
-                        for (int k = 0; k < DB; k++) fxs[k] = k < cnt ? (R)P.fexit[(long long)(first + k) * sstride + o] : R(0);
-                    }
-                    if (jy == 0) {
-                        const long long o = (iyy == 0 ? yin : yoff) + yk;
+                    for (int k = 0; k < DB; k++) fyi[k] = (R)fyb[((long long)sb * TT + jz) * DB + k];
+                }
+                if (jz == 0) {
 #pragma unroll
-                        for (int k = 0; k < DB; k++) fyi[k] = k < cnt ? (R)P.fexit[(long long)(first + k) * sstride + o] : R(0);
-                    }
-                    if (jz == 0) {
-                        const long long o = (izz == 0 ? zin_ : zoff) + zk;
+                    for (int k = 0; k < DB; k++) fzi[k] = (R)fzb[((long long)sb * TT + jy) * DB + k];
+                } else {
 #pragma unroll
-                        for (int k = 0; k < DB; k++) fzi[k] = k < cnt ? (R)P.fexit[(long long)(first + k) * sstride + o] : R(0);
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < DB; k++) fzi[k] = sfz[(rd * DB + k) * TP + me - TY];
-                    }
-                    const int m = mb[sb * TP + me];
-                    const R sigt = (R)gs.sigt[m];
-                    R scs = R(0), srcE = R(0);
-                    if (CSD) {
-                        scs = (R)P.scsd[m];
-                        srcE = esa * (R)gs.sp[m] - esb * (R)gs.sm[m];
-                    }
-                    const R idx = (R)(1.0 / P.dx[ix]);
-                    PS *qc = qb + ((long long)sb * TP + me) * DB;
-                    double *ec = eb + ((long long)sb * TP + me) * DB;
-#pragma unroll
-                    for (int k = 0; k < DB; k++) {
-                        if (k >= cnt) continue;
-                        const R *d = dc + k * 9;
-                        const R fe = (CSD && phiE_in) ? (R)ec[k] : R(0);
-                        const R S = (scs + sigt) + d[0] * idx + d[1] * idy + d[2] * idz;
-                        R q = (R)qc[k] + (d[3] * idx) * fxs[k] + (d[4] * idy) * fyi[k] + (d[5] * idz) * fzi[k];
-                        if (CSD) q -= srcE * fe;
-                        const R v = q / S;
-                        fxs[k] = w1x * fxs[k] + d[6] * v;
-                        fyi[k] = w1y * fyi[k] + d[7] * v;
-                        fzi[k] = w1z * fzi[k] + d[8] * v;
-                        qc[k] = (PS)v;
-                        if (CSD) ec[k] = (double)(w1e * fe + eout * v);
-                        sfz[(wr * DB + k) * TP + me] = fzi[k];
-                    }
-                    // faces leaving the tile or the domain (loops over the compile-time DB keep
-                    // the per-direction arrays in registers)
-                    if (jy == TY - 1 || iyy == ny - 1) {
-                        const long long off = iyy < ny - 1 ? yoff : eyo;
-#pragma unroll
-                        for (int k = 0; k < DB; k++)
-                            if (k < cnt) P.fexit[(long long)(first + k) * sstride + off + yk] = (double)fyi[k];
-                    }
-                    if (jz == TZ - 1 || izz == nz - 1) {
-                        const long long off = izz < nz - 1 ? zoff : ezo;
-#pragma unroll
-                        for (int k = 0; k < DB; k++)
-                            if (k < cnt) P.fexit[(long long)(first + k) * sstride + off + zk] = (double)fzi[k];
-                    }
-                    if (ixx == nx - 1) {
-                        const long long o = (iy + (long long)ny * iz) * nfm;
-#pragma unroll
-                        for (int k = 0; k < DB; k++)
-                            if (k < cnt) P.fexit[(long long)(first + k) * sstride + o] = (double)fxs[k];
-                    }
+                    for (int k = 0; k < DB; k++) fzi[k] = sfz[(rd * DB + k) * TP + me - TY];
                 }
 #pragma unroll
-                for (int k = 0; k < DB; k++) fyl[k] = fyi[k];
-                __syncthreads();
-                // the step's angular flux (and outgoing energy-face flux) back to global memory,
-                // consecutive lanes on consecutive directions of a cell
-                {
-                    int p = p0, k = k0;
-                    for (int r = 0; r < cnt; r++) {
-                        const long long c = cell_of(p, sg);
-                        if (c >= 0) {
-                            psi[first + k + (long long)nd * c] = qb[((long long)sb * TP + p) * DB + k];
-                            if (CSD) phiE_out[first + k + (long long)nd * c] = eb[((long long)sb * TP + p) * DB + k];
-                        }
-                        p += qd;
-                        k += rm;
-                        if (k >= cnt) { k -= cnt; p++; }
-                    }
+                for (int k = 0; k < DB; k++) {
+                    qv[k] = (R)qc[k];
+                    fe[k] = (CSD && phiE_in) ? (R)ec[k] : R(0);
+                }
+                const int m = mb[sb * TP + me];
+                const R S0 = mS[m], sq = mQ[m];
+                const R idx = xs_sm ? idxs[ix] : (R)(1.0 / P.dx[ix]);
+                R v[DB];
+#pragma unroll
+                for (int k = 0; k < DB; k++) {
+                    const R *d = dc + k * 9;
+                    const R S = S0 + d[0] * idx + d[1] * idy + d[2] * idz;
+                    R q = qv[k] + (d[3] * idx) * fxs[k] + (d[4] * idy) * fyi[k] + (d[5] * idz) * fzi[k];
+                    if (CSD) q -= sq * fe[k];
+                    v[k] = oct_div(q, S);
+                    fxs[k] = w1x * fxs[k] + d[6] * v[k];
+                    fyi[k] = w1y * fyi[k] + d[7] * v[k];
+                    fzi[k] = w1z * fzi[k] + d[8] * v[k];
+                }
+#pragma unroll
+                for (int k = 0; k < DB; k++) {
+                    if (k >= cnt) continue;
+                    qc[k] = (PS)v[k];
+                    if (CSD) ec[k] = (double)(w1e * fe[k] + eout * v[k]);
+                    sfz[(wr * DB + k) * TP + me] = fzi[k];
+                }
+                // faces leaving the tile or the domain
+                if (jy == TY - 1 || iyy == ny - 1) {
+                    const long long off = iyy < ny - 1 ? yoff : eyo;
+#pragma unroll
+                    for (int k = 0; k < DB; k++)
+                        if (k < cnt) P.fexit[(long long)(first + k) * sstride + off + yk] = (double)fyi[k];
+                }
+                if (jz == TZ - 1 || izz == nz - 1) {
+                    const long long off = izz < nz - 1 ? zoff : ezo;
+#pragma unroll
+                    for (int k = 0; k < DB; k++)
+                        if (k < cnt) P.fexit[(long long)(first + k) * sstride + off + zk] = (double)fzi[k];
+                }
+                if (ixx == nx - 1) {
+                    const long long o = (iy + (long long)ny * iz) * nfm;
+#pragma unroll
+                    for (int k = 0; k < DB; k++)
+                        if (k < cnt) P.fexit[(long long)(first + k) * sstride + o] = (double)fxs[k];
                 }
             }
-            t.sync();
+#pragma unroll
+            for (int k = 0; k < DB; k++) fyl[k] = fyi[k];
+            __syncthreads();
+            // the faces of step sg are stored: publish (the barrier orders every thread's stores
+            // before thread 0's fence and release)
+            if (me == 0 && ((sg + 1) % RB_OCT_PUB == 0 || sg == nsteps - 1)) {
+                __threadfence();
+                st_release_u64(P.oct_flags + t.crank, tagr | (unsigned long long)(sg + 1));
+            }
+            // the step's angular flux (and outgoing energy-face flux) back to global memory,
+            // consecutive lanes on consecutive directions of a cell
+            {
+                int p = p0, k = k0;
+#pragma unroll
+                for (int r = 0; r < DB; r++) {
+                    if (r < cnt) {
+                        const long long c = cell_of(p, sg);
+                        if (c >= 0) {
+                            const long long so = ((long long)sb * TP + p) * DB + k;
+                            const long long go = first + k + (long long)nd * c;
+                            psi[go] = qb[so];
+                            if (CSD) phiE_out[go] = eb[so];
+                        }
+                    }
+                    p += qd;
+                    k += rm;
+                    if (k >= cnt) { k -= cnt; p++; }
+                }
+            }
         }
         cp_async_wait<0>();
         __syncthreads();
