@@ -217,17 +217,23 @@ typedef struct rb_coupling {
  * and its running total flux stay on the device for the whole generation loop; a generation
  * solves the particles in order (starting from the first one with fixed sources), each solve
  * followed by the sources it produces for the others (device kernels), and the fixed sources
- * count in the first generation only. Convergence as the reference's "flux" criterion: after
- * generation n > 1, every particle's max |Φ_n − Φ_(n−1)| / max(|Φ_n|, eps) over groups and cells
- * (moment 1, cell moment 1) below eps_gen. couplings[i*npart + j] couples i into j (the diagonal
- * is ignored). results[i]: flux and flux_cutoff summed over the generations (the reference's
- * Flux_Per_Particle sums its solutions), rho / iterations / residuals / converged of the last
- * generation's solve, passes summed over all solves. *generations: generations run; *eps_final:
- * the last ϵ (NaN after one generation). conv_type: 0 = flux (energy and charge deposition
- * criteria: RB_ERR_UNSUPPORTED). */
+ * count in the first generation only. couplings[i*npart + j] couples i into j (the diagonal is
+ * ignored). conv_type (transport.jl:112-137): 0 = "flux" (after generation n > 1, every
+ * particle's max |Φ_n − Φ_(n−1)| / max(|Φ_n|, eps) over groups and cells, moment 1 and cell
+ * moment 1, below eps_gen), 1 = "energy-deposition", 2 = "charge-deposition" (the summed
+ * deposition's max relative change below eps_gen); other values: RB_ERR_INVALID.
+ * sigma_dep[i] [ng_i+1, nmat] (Σe for energy, Σc for charge deposition: the same formula),
+ * density [nmat] and norm (the sources' normalization factor) are needed by criteria 1 and 2 and
+ * by `deposition` (else NULL). results[i]: flux and flux_cutoff summed over the generations
+ * (the reference's Flux_Per_Particle sums its solutions), rho / iterations / residuals /
+ * converged of the last generation's solve, passes summed over all solves. deposition (NULL =
+ * skip): [nx,ny,nz], the summed deposition of the final fluxes (energy_deposition.jl:24-87 with
+ * sigma_dep). *generations: generations run; *eps_final: the last ϵ (NaN after one). */
 RB_API int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_problem *const *probs,
                             const rb_coupling *couplings, int32_t ngen_max, double eps_gen, int32_t conv_type,
-                            rb_sn_result *const *results, int32_t *generations, double *eps_final);
+                            const double *const *sigma_dep, const double *density, double norm,
+                            rb_sn_result *const *results, double *deposition, int32_t *generations,
+                            double *eps_final);
 
 /* ---- serving: continuous batching ---------------------------------------------------- */
 /* Admits a request (one particle solve) when its state fits the remaining HBM budget
@@ -245,6 +251,13 @@ RB_API int32_t rb_poll(rb_context *ctx, rb_handle h, rb_sn_result *res);
 RB_API int32_t rb_energy_deposition(int32_t ng, int32_t np, int32_t nm5, int64_t ncell,
                              int32_t nmat, const int32_t *mat, const double *flux,
                              const double *flux_cutoff, const double *sigma_e,
+                             const double *density, double norm, double *dep);
+/* energy_deposition.jl:24-87 (sigma_dep = Σe) or charge_deposition.jl:26-89 (sigma_dep = Σc;
+ * the same formula) of problems already solved in the context (rb_solve / rb_solve_batch), on
+ * the device: dep[c] = Σ_particles (Σ_g sig_i[g,mat]·𝚽l_i[g,1,1,c] + sig_i[ng_i+1,mat]·
+ * 𝚽cutoff_i[1,1,c]) / (ρ[mat]·norm), particles summed in the order of `handles`; sigma_dep[i]
+ * [ng_i+1, nmat], dep [nx,ny,nz]. Only the voxel array crosses to the host. */
+RB_API int32_t rb_deposition(rb_context *ctx, int32_t npart, const rb_handle *handles, const double *const *sigma_dep,
                              const double *density, double norm, double *dep);
 
 /* Library version string. */

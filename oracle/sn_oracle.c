@@ -1104,11 +1104,28 @@ static void oracle_particle_source(const rb_sn_problem *Pi, const rb_sn_problem 
     free(ql_out);
 }
 
+/* summed deposition of the particles' totals (energy_deposition.jl:37-78 / charge_deposition.jl:
+ * 39-80): particles in `order`, each particle's D from oracle_energy_deposition, Dtot += D */
+static void oracle_total_deposition(int32_t npart, const int *order, const rb_sn_problem *const *probs,
+                                    double *const *tot, double *const *tot_cut, const double *const *sigma_dep,
+                                    const double *density, double norm, int64_t ncell, double *out, double *tmp) {
+    for (int64_t c = 0; c < ncell; c++) out[c] = 0.0;
+    for (int p = 0; p < npart; p++) {
+        const int i = order[p];
+        const rb_sn_problem *P = probs[i];
+        oracle_energy_deposition(P->ng, P->np, P->nm[4], ncell, P->nmat, P->mat, tot[i],
+                                 P->solver_type >= 2 ? tot_cut[i] : NULL, sigma_dep[i], density, norm, tmp);
+        for (int64_t c = 0; c < ncell; c++) out[c] += tmp[c];
+    }
+}
+
 int oracle_transport(int32_t npart, const rb_sn_problem *const *probs, const rb_coupling *couplings, int32_t ngen_max,
-                     double eps_gen, int32_t conv_type, rb_sn_result *const *results, int32_t *generations,
+                     double eps_gen, int32_t conv_type, const double *const *sigma_dep, const double *density,
+                     double norm, rb_sn_result *const *results, double *deposition, int32_t *generations,
                      double *eps_final) {
     if (npart < 1 || ngen_max < 1) return RB_ERR_INVALID;
-    if (conv_type != 0) return RB_ERR_UNSUPPORTED;
+    if (conv_type < 0 || conv_type > 2) return RB_ERR_INVALID; /* "Unknown convergence type." */
+    if ((conv_type != 0 || deposition) && (!sigma_dep || !density)) return RB_ERR_INVALID;
     int i0 = -1;
     for (int i = 0; i < npart && i0 < 0; i++) {
         int any = probs[i]->volume_sources != NULL;
@@ -1135,6 +1152,9 @@ int oracle_transport(int32_t npart, const rb_sn_problem *const *probs, const rb_
     }
     int ngen = 0, st = RB_OK;
     double eps_last = NAN;
+    const int64_t ncell0 = (int64_t)probs[0]->nx * (probs[0]->ndims >= 2 ? probs[0]->ny : 1) *
+                           (probs[0]->ndims >= 3 ? probs[0]->nz : 1);
+    double *dep = zalloc(ncell0), *dep_prev = zalloc(ncell0), *dtmp = zalloc(ncell0);
     for (int n = 1; n <= ngen_max && st == RB_OK; n++) {
         ngen = n;
         for (int i = 0; i < npart; i++) memcpy(prev[i], tot[i], sizeof(double) * nall[i]); /* flux⁻ */
@@ -1170,7 +1190,19 @@ int oracle_transport(int32_t npart, const rb_sn_problem *const *probs, const rb_
             }
         }
         if (st != RB_OK) break;
-        if (n != 1) { /* the "flux" criterion, transport.jl:116-121 */
+        if (conv_type != 0) { /* energy / charge deposition criterion, transport.jl:122-133 */
+            oracle_total_deposition(npart, order, probs, tot, tot_cut, sigma_dep, density, norm, ncell0, dep, dtmp);
+            if (n != 1) {
+                double e = 0.0;
+                for (int64_t c = 0; c < ncell0; c++) {
+                    const double r = fabs(dep[c] - dep_prev[c]) / fmax(fabs(dep[c]), 2.220446049250313e-16);
+                    if (r > e) e = r;
+                }
+                eps_last = e;
+            }
+            memcpy(dep_prev, dep, sizeof(double) * ncell0);
+            if (n != 1 && eps_last < eps_gen) break;
+        } else if (n != 1) { /* the "flux" criterion, transport.jl:116-121 */
             int px = 0;
             double emax = 0.0;
             for (int i = 0; i < npart; i++) {
@@ -1195,6 +1227,11 @@ int oracle_transport(int32_t npart, const rb_sn_problem *const *probs, const rb_
             if (results[i]->flux_cutoff && probs[i]->solver_type >= 2)
                 memcpy(results[i]->flux_cutoff, tot_cut[i], sizeof(double) * nphi[i]);
         }
+    if (st == RB_OK && deposition) {
+        oracle_total_deposition(npart, order, probs, tot, tot_cut, sigma_dep, density, norm, ncell0, dep, dtmp);
+        memcpy(deposition, dep, sizeof(double) * ncell0);
+    }
+    free(dep); free(dep_prev); free(dtmp);
     if (generations) *generations = ngen;
     if (eps_final) *eps_final = eps_last;
     for (int i = 0; i < npart; i++) {

@@ -136,6 +136,41 @@ __global__ void particle_source_kernel(const double *__restrict__ flux_i, int ng
         *dst = *dst + v;
     }
 }
+
+// ---- deposition (rb_deposition, rb_transport) ------------------------------------------------
+// energy_deposition.jl:65-77 / charge_deposition.jl:67-79 for one particle, per voxel c:
+// d = (Σ_g sig[g,mat]·𝚽[g,1,1,c] + sig[ng,mat]·𝚽cutoff[1,1,c]) / (ρ[mat]·norm), sig [ng+1, nmat]
+// (Σe or Σc) and mat 0-based; dep[c] = d, or dep[c] + d to sum particles (Dtot += D).
+__global__ void deposition_kernel(const double *__restrict__ flux, int ng, long long nphi, long long cstride,
+                                  const double *__restrict__ cutoff, const int *__restrict__ mat,
+                                  const double *__restrict__ sig, const double *__restrict__ rho, double norm,
+                                  long long ncell, double *__restrict__ dep, int accumulate) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const int m = mat[c];
+        const double *sg = sig + (long long)(ng + 1) * m;
+        double d = 0.0;
+        for (int g = 0; g < ng; g++) d += sg[g] * flux[(long long)g * nphi + cstride * c];
+        if (cutoff) d += sg[ng] * cutoff[cstride * c];
+        d = d / (rho[m] * norm);
+        dep[c] = accumulate ? dep[c] + d : d;
+    }
+}
+// max over c of |cur − prev| / max(|cur|, eps) (transport.jl:125, 131), as the bits of a
+// non-negative double in *maxrel
+__global__ void max_rel_change(const double *__restrict__ cur, const double *__restrict__ prev, long long n,
+                               unsigned long long *maxrel) {
+    __shared__ double red[32];
+    double m = 0.0;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(cur[c] - prev[c]) / fmax(fabs(cur[c]), 2.220446049250313e-16));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x + 31) / 32; w++) m = fmax(m, red[w]);
+        atomicMax(maxrel, (unsigned long long)__double_as_longlong(m));
+    }
+}
 }  // namespace rb
 
 namespace {
@@ -1173,6 +1208,58 @@ int32_t rb_energy_deposition(int32_t ng, int32_t np, int32_t nm5, int64_t ncell,
     return RB_OK;
 }
 
+int32_t rb_deposition(rb_context *ctx, int32_t npart, const rb_handle *handles, const double *const *sigma_dep,
+                      const double *density, double norm, double *dep) {
+    // energy_deposition.jl:24-87 / charge_deposition.jl:26-89 over resident, solved problems: a
+    // device reduction over groups per voxel, summed over the particles in the order given; only
+    // the voxel array comes back
+    if (!ctx || npart < 1 || !handles || !sigma_dep || !density || !dep)
+        return fail(ctx, RB_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    std::vector<ProblemRec *> recs;
+    size_t nsig = 0;
+    for (int i = 0; i < npart; i++) {
+        ProblemRec *r = find(ctx, handles[i]);
+        if (!r) return fail(ctx, RB_ERR_NOT_FOUND, "unknown problem handle %lld", (long long)handles[i]);
+        if (!r->solved) return fail(ctx, RB_ERR_INVALID, "problem %lld was not solved", (long long)handles[i]);
+        if (!sigma_dep[i]) return fail(ctx, RB_ERR_INVALID, "no deposition cross sections for particle %d", i);
+        if (i > 0 && (r->ncell != recs[0]->ncell || r->h.nmat != recs[0]->h.nmat))
+            return fail(ctx, RB_ERR_INVALID, "particle %d is not on the geometry of particle 1", i);
+        recs.push_back(r);
+        nsig += (size_t)(r->ng + 1) * r->h.nmat;
+    }
+    const int nmat = recs[0]->h.nmat;
+    const long long ncell = recs[0]->ncell;
+    for (auto *r : recs)
+        if (r->stream) CK(cudaStreamSynchronize(r->stream));
+    cudaStream_t s = ctx->stream;
+    double *buf = nullptr;
+    CK(cudaMalloc(&buf, (nsig + nmat + ncell) * sizeof(double)));
+    double *dsig = buf, *drho = buf + nsig, *ddep = drho + nmat;
+    int st = RB_OK;
+    auto run = [&]() -> int {
+        CK(cudaMemcpyAsync(drho, density, nmat * sizeof(double), cudaMemcpyHostToDevice, s));
+        size_t o = 0;
+        for (int i = 0; i < npart; i++) {
+            const ProblemRec *r = recs[i];
+            const size_t n = (size_t)(r->ng + 1) * nmat;
+            CK(cudaMemcpyAsync(dsig + o, sigma_dep[i], n * sizeof(double), cudaMemcpyHostToDevice, s));
+            const int blocks = (int)std::min<long long>((ncell + 255) / 256, (long long)ctx->nsm * 8);
+            rb::deposition_kernel<<<blocks, 256, 0, s>>>(r->h.flux, r->ng, r->nphi, (long long)r->np * r->nm5,
+                                                         r->csd ? r->h.cutoff : nullptr, r->h.mat, dsig + o, drho,
+                                                         norm, ncell, ddep, i > 0);
+            CK(cudaGetLastError());
+            o += n;
+        }
+        CK(cudaMemcpyAsync(dep, ddep, ncell * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        return RB_OK;
+    };
+    st = run();
+    cudaFree(buf);
+    return st;
+}
+
 }  // extern "C"
 
 // =============================================================================================
@@ -1291,12 +1378,19 @@ struct CoupledPair {
 
 extern "C" int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_problem *const *probs,
                                 const rb_coupling *couplings, int32_t ngen_max, double eps_gen, int32_t conv_type,
-                                rb_sn_result *const *results, int32_t *generations, double *eps_final) {
+                                const double *const *sigma_dep, const double *density, double norm,
+                                rb_sn_result *const *results, double *deposition, int32_t *generations,
+                                double *eps_final) {
     rb_context *ctx = nullptr;
     if (npart < 1 || !probs || !results) return fail(nullptr, RB_ERR_INVALID, "bad particle list");
     if (ngen_max < 1) return fail(nullptr, RB_ERR_INVALID, "ngen_max must be >= 1");
-    if (conv_type != 0)
-        return fail(nullptr, RB_ERR_UNSUPPORTED, "only the flux convergence criterion of transport() is built");
+    if (conv_type < 0 || conv_type > 2) return fail(nullptr, RB_ERR_INVALID, "Unknown convergence type.");
+    const bool use_dep = conv_type != 0 || deposition != nullptr;
+    if (use_dep) {
+        if (!sigma_dep || !density) return fail(nullptr, RB_ERR_INVALID, "deposition cross sections or densities missing");
+        for (int i = 0; i < npart; i++)
+            if (!sigma_dep[i]) return fail(nullptr, RB_ERR_INVALID, "no deposition cross sections for particle %d", i);
+    }
     for (int i = 0; i < npart; i++) {
         const rb_sn_problem *a = probs[i], *b = probs[0];
         if (!a || !results[i]) return fail(nullptr, RB_ERR_INVALID, "null problem or result %d", i);
@@ -1319,8 +1413,17 @@ extern "C" int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_probl
     if (st) return st;
     std::vector<CoupledPart> parts(npart);
     std::vector<CoupledPair> pairs((size_t)npart * npart);
+    // deposition buffers (the energy- and charge-deposition criteria, and the summed deposition)
+    std::vector<double *> dsig(npart, nullptr);
+    double *drho = nullptr, *dep_cur = nullptr, *dep_prev = nullptr;
+    unsigned long long *dmax = nullptr;
     auto cleanup = [&](int code) {
         cudaStreamSynchronize(ctx->stream);
+        for (auto q : dsig) if (q) cudaFree(q);
+        if (drho) cudaFree(drho);
+        if (dep_cur) cudaFree(dep_cur);
+        if (dep_prev) cudaFree(dep_prev);
+        if (dmax) cudaFree(dmax);
         for (auto &p : parts) {
             if (p.tot) cudaFree(p.tot);
             if (p.tot_cut) cudaFree(p.tot_cut);
@@ -1390,6 +1493,40 @@ extern "C" int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_probl
             CKT(cudaMemcpyAsync(q.transfer, c->transfer, (size_t)b.np * a.np * sizeof(double), cudaMemcpyHostToDevice, s));
             CKT(cudaMemcpyAsync(q.map, c->moment_map, (size_t)b.nm5 * sizeof(int), cudaMemcpyHostToDevice, s));
         }
+    // deposition (the energy- and charge-deposition criteria, and the summed deposition out):
+    // per-particle cross sections [ng+1, nmat], densities, this and the last generation's map
+    const long long ncell = parts[0].r->ncell;
+    const int nmat = parts[0].r->h.nmat;
+    if (use_dep) {
+        int e = RB_OK;
+        for (int i = 0; i < npart && e == RB_OK; i++) {
+            const size_t n = (size_t)(parts[i].r->ng + 1) * nmat;
+            if (cudaMalloc(&dsig[i], n * sizeof(double)) != cudaSuccess ||
+                cudaMemcpyAsync(dsig[i], sigma_dep[i], n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+                e = RB_ERR_CUDA;
+        }
+        if (e == RB_OK && (cudaMalloc(&drho, nmat * sizeof(double)) != cudaSuccess ||
+                           cudaMalloc(&dep_cur, ncell * sizeof(double)) != cudaSuccess ||
+                           cudaMalloc(&dep_prev, ncell * sizeof(double)) != cudaSuccess ||
+                           cudaMalloc(&dmax, sizeof(unsigned long long)) != cudaSuccess ||
+                           cudaMemcpyAsync(drho, density, nmat * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess))
+            e = RB_ERR_CUDA;
+        if (e != RB_OK) return cleanup(fail(ctx, RB_ERR_CUDA, "deposition buffers"));
+    }
+    // the summed deposition of the running totals into dep_cur, particles in the solve order (the
+    // order the reference's Flux holds them in)
+    auto deposit = [&]() -> int {
+        const int blocks = (int)std::min<long long>((ncell + 255) / 256, (long long)ctx->nsm * 8);
+        for (int p = 0; p < npart; p++) {
+            const int i = order[p];
+            const CoupledPart &P = parts[i];
+            rb::deposition_kernel<<<blocks, 256, 0, s>>>(P.tot, P.r->ng, P.r->nphi, (long long)P.r->np * P.r->nm5,
+                                                         P.r->csd ? P.tot_cut : nullptr, P.r->h.mat, dsig[i], drho,
+                                                         norm, ncell, dep_cur, p > 0);
+            if (cudaGetLastError() != cudaSuccess) return RB_ERR_CUDA;
+        }
+        return RB_OK;
+    };
     CKT(cudaFuncSetAttribute(rb::particle_source_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     CKT(cudaStreamSynchronize(s));
     double eps_last = NAN;
@@ -1444,7 +1581,7 @@ extern "C" int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_probl
                 CKT(cudaGetLastError());
             }
         }
-        if (n > 1) {  // the flux criterion (transport.jl:111-118)
+        if (conv_type == 0 && n > 1) {  // the flux criterion (transport.jl:116-121)
             int px = 0;
             double emax = 0.0;
             for (int i = 0; i < npart; i++) {
@@ -1459,6 +1596,31 @@ extern "C" int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_probl
             eps_last = emax;
             if (px == npart) break;
         }
+        if (conv_type != 0) {  // energy / charge deposition criterion (transport.jl:122-133)
+            const int e = deposit();
+            if (e != RB_OK) return cleanup(fail(ctx, e, "deposition kernel"));
+            if (n > 1) {
+                unsigned long long bits = 0;
+                CKT(cudaMemsetAsync(dmax, 0, sizeof(bits), s));
+                const int blocks = (int)std::min<long long>((ncell + 255) / 256, (long long)ctx->nsm * 8);
+                rb::max_rel_change<<<blocks, 256, 0, s>>>(dep_cur, dep_prev, ncell, dmax);
+                CKT(cudaGetLastError());
+                CKT(cudaMemcpyAsync(&bits, dmax, sizeof(bits), cudaMemcpyDeviceToHost, s));
+                CKT(cudaStreamSynchronize(s));
+                memcpy(&eps_last, &bits, sizeof(eps_last));
+            }
+            std::swap(dep_cur, dep_prev);  // dep_prev: the deposition of this generation's totals
+            if (n > 1 && eps_last < eps_gen) break;
+        }
+    }
+    if (deposition) {  // the summed deposition of the final totals
+        if (conv_type != 0) std::swap(dep_cur, dep_prev);
+        else {
+            const int e = deposit();
+            if (e != RB_OK) return cleanup(fail(ctx, e, "deposition kernel"));
+        }
+        CKT(cudaMemcpyAsync(deposition, dep_cur, ncell * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CKT(cudaStreamSynchronize(s));
     }
     // the summed solutions out, in the reference's layouts
     for (int i = 0; i < npart; i++) {

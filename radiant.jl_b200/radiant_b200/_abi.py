@@ -219,7 +219,9 @@ def load_library(path: str | None = None):
         "rb_energy_deposition": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32, _ip,
                                              _dp, _dp, _dp, _dp, C.c_double, _dp]),
         "rb_transport": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(PP), C.POINTER(RbCoupling), C.c_int32,
-                                     C.c_double, C.c_int32, C.POINTER(RP), _ip, _dp]),
+                                     C.c_double, C.c_int32, C.POINTER(_dp), _dp, C.c_double, C.POINTER(RP), _dp,
+                                     _ip, _dp]),
+        "rb_deposition": (C.c_int32, [vp, C.c_int32, C.POINTER(h64), C.POINTER(_dp), _dp, C.c_double, _dp]),
         "rb_version": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
@@ -234,7 +236,7 @@ def load_library(path: str | None = None):
 EXPORTED_SYMBOLS = (
     "rb_create", "rb_destroy", "rb_last_error", "rb_upload", "rb_solve", "rb_solve_batch",
     "rb_download", "rb_release", "rb_required_bytes", "rb_compute_flux", "rb_submit", "rb_poll",
-    "rb_energy_deposition", "rb_transport", "rb_version",
+    "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_version",
 )
 
 
@@ -249,6 +251,7 @@ class Context:
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
         self.lib = load_library()
+        self._ncell = {}  # voxels of each uploaded problem (deposition maps)
         self.h = C.c_void_p()
         st = self.lib.rb_create(device, hbm_budget_bytes, C.byref(self.h))
         if st != RB_OK:
@@ -266,6 +269,7 @@ class Context:
     def upload(self, pp: PackedProblem) -> int:
         h = C.c_int64()
         self.check(self.lib.rb_upload(self.h, C.byref(pp.P), C.byref(h)))
+        self._ncell[h.value] = int(np.prod(pp.tables["ns"]))
         return h.value
 
     def solve(self, h: int, stream=None):
@@ -292,6 +296,18 @@ class Context:
             return False
         self.check(st)
         return True
+
+    def deposition(self, handles, sigma_dep, density, norm: float = 1.0) -> np.ndarray:
+        """Summed energy (Σe) or charge (Σc) deposition of solved resident problems, on the device
+        (rb_deposition); sigma_dep: one [ng+1, nmat] array per handle. Returns [ncell] (x fastest)."""
+        n = len(handles)
+        sig = [np.asfortranarray(x, dtype=float) for x in sigma_dep]
+        rho = np.ascontiguousarray(density, dtype=float)
+        arr = (C.c_int64 * n)(*handles)
+        ptrs = (_dp * n)(*[_ptr(x) for x in sig])
+        out = np.zeros(self._ncell[handles[0]])
+        self.check(self.lib.rb_deposition(self.h, n, arr, ptrs, _ptr(rho), float(norm), _ptr(out)))
+        return out
 
     def close(self):
         if self.h:

@@ -19,7 +19,7 @@ import numpy as np
 from . import sphere as S
 from . import tables as T
 from ._abi import (PackedProblem, RadiantError, RB_OK, RbCoupling, RbSnProblem, RbSnResult, ResultBuffers,
-                   _ip, _ptr, load_library)
+                   _dp, _ip, _ptr, load_library)
 from .sn_flux import FluxPerParticle
 
 CONV_TYPES = {"flux": 0, "energy-deposition": 1, "charge-deposition": 2}
@@ -163,14 +163,26 @@ class TransportResult:
     fluxes: list            # FluxPerParticle per particle (fluxes summed over the generations)
     generations: int
     eps: float              # the last generation's ϵ (NaN after one generation)
+    deposition: np.ndarray | None = None  # summed deposition of the final fluxes [ncell], if asked
+
+
+class _DepPack:
+    """sigma_dep pointer array (one [ng+1, nmat] table per particle) with its arrays kept alive."""
+
+    def __init__(self, sigma_dep):
+        self.keep = [np.asfortranarray(x, dtype=float) for x in sigma_dep]
+        self.arr = (_dp * len(self.keep))(*[_ptr(x) for x in self.keep])
 
 
 def transport_tables(parts: list, couplings: dict, ngen_max: int = 50, eps_gen: float = 1e-6,
-                     conv_type: str = "flux", device: int = 0) -> TransportResult:
+                     conv_type: str = "flux", device: int = 0, sigma_dep=None, density=None, norm: float = 1.0,
+                     deposition: bool = False) -> TransportResult:
     """transport() (transport.jl:21-147) for particles given as prepared tables on one geometry.
 
-    ``couplings[(i, j)]`` is the Coupling of particle i into j (build_coupling). A single
-    particle is compute_flux itself, as in the reference (transport.jl:33-43)."""
+    ``couplings[(i, j)]`` is the Coupling of particle i into j (build_coupling). The
+    "energy-deposition" and "charge-deposition" criteria need ``sigma_dep`` (one [ng+1, nmat]
+    table per particle: Σe or Σc), ``density`` [nmat] and ``norm`` (the sources' normalization
+    factor); with ``deposition`` the summed deposition of the final fluxes comes back too."""
     if conv_type not in CONV_TYPES:
         raise ValueError("Unknown convergence type.")
     lib = load_library()
@@ -180,14 +192,18 @@ def transport_tables(parts: list, couplings: dict, ngen_max: int = 50, eps_gen: 
     probs = (C.POINTER(RbSnProblem) * n)(*[C.pointer(p.P) for p in packs])
     results = (C.POINTER(RbSnResult) * n)(*[C.pointer(r.R) for r in res])
     cp = _CouplingPack(n, couplings)
+    dp = _DepPack(sigma_dep) if sigma_dep is not None else None
+    rho = np.ascontiguousarray(density, dtype=float) if density is not None else None
+    dep = np.zeros(int(np.prod(parts[0]["ns"]))) if deposition else None
     ngen = C.c_int32(0)
     eps = C.c_double(0.0)
-    st = lib.rb_transport(device, n, probs, cp.arr, int(ngen_max), float(eps_gen), CONV_TYPES[conv_type], results,
-                          C.byref(ngen), C.byref(eps))
+    st = lib.rb_transport(device, n, probs, cp.arr, int(ngen_max), float(eps_gen), CONV_TYPES[conv_type],
+                          dp.arr if dp else None, _ptr(rho), float(norm), results, _ptr(dep), C.byref(ngen),
+                          C.byref(eps))
     if st != RB_OK:
         buf = C.create_string_buffer(1024)
         lib.rb_last_error(None, buf, 1024)
         raise RadiantError(st, buf.value.decode(errors="replace"))
     out = [FluxPerParticle(r.flux, r.flux_cutoff, r.rho, r.group_iters, r.group_resid, r.group_converged, r.passes)
            for r in res]
-    return TransportResult(out, int(ngen.value), float(eps.value))
+    return TransportResult(out, int(ngen.value), float(eps.value), dep)

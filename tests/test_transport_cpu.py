@@ -151,3 +151,34 @@ def test_particle_order_starts_at_the_first_sourced_particle():
         np.testing.assert_array_equal(r2[new].flux, r1[old].flux)
     with pytest.raises(RuntimeError):
         orun.transport(parts[1:], {}, ngen_max=2)
+
+
+def test_deposition_criterion_on_the_geometric_series():
+    """The energy-deposition criterion (transport.jl:122-127) on the two-particle infinite medium:
+    the summed deposition grows like the fluxes, so its relative change per generation is the flux
+    criterion's k^(n-1)/Σ_{g<n} k^g and both stop at the same generation; the deposition returned is
+    (Σe₁·φ₁ + Σe₂·φ₂)/(ρ·norm)."""
+    Q, s1, s2, a, b, nx = 2.0, 1.5, 0.8, 0.6, 0.5, 10
+    sn = SNSettings(solver_type="BTE", quadrature_order=8, legendre_order=0, scheme_type={"x": "DD"},
+                    scheme_order={"x": 1}, acceleration="gmres", convergence_criterion=1e-13,
+                    angular_boltzmann="standard")
+
+    def slab(st, vol):
+        xs = MultigroupXS(sigma_t=np.full((1, 1), st), sigma_s=np.zeros((1, 1, 1, 1)), sigma_a=np.full((1, 1), st),
+                          sigma_e=np.ones((2, 1)), e_width=np.ones(1), density=np.ones(1))
+        return prepare_sn_tables(xs, 1, [nx], [np.full(nx, 0.3)], np.ones((nx, 1, 1), dtype=np.int32),
+                                 [1, 1, 0, 0, 0, 0], sn, volume_sources=vol)
+
+    p1, p2 = slab(s1, np.full((1, 1, 1, nx, 1, 1), Q)), slab(s2, None)
+    cps = {(0, 1): build_coupling(p1, p2, np.full((1, 1, 1, 1), a)),
+           (1, 0): build_coupling(p2, p1, np.full((1, 1, 1, 1), b))}
+    se = [np.array([[0.7], [0.0]]), np.array([[0.3], [0.0]])]
+    rho, norm = np.array([1.3]), 2.0
+    r0, n0, e0 = orun.transport([p1, p2], cps, ngen_max=50, eps_gen=1e-6)
+    r1, n1, e1, dep = orun.transport([p1, p2], cps, ngen_max=50, eps_gen=1e-6, conv_type=1, sigma_dep=se,
+                                     density=rho, norm=norm, deposition=True)
+    assert n1 == n0 and e1 == pytest.approx(e0, rel=1e-9)
+    phi1, phi2 = r1[0].flux[0, 0, 0, :, 0, 0], r1[1].flux[0, 0, 0, :, 0, 0]
+    np.testing.assert_allclose(dep, (0.7 * phi1 + 0.3 * phi2) / (1.3 * 2.0), rtol=1e-14)
+    with pytest.raises(RuntimeError):
+        orun.transport([p1, p2], cps, ngen_max=3, conv_type=3, sigma_dep=se, density=rho)
