@@ -76,6 +76,47 @@ def gauss_legendre(N: int):
     return x, w
 
 
+def gauss_lobatto(N: int):
+    """Gauss-Lobatto nodes/weights: end points ±1, interior nodes the zeros of P'_(N−1) by Newton
+    from the Chebyshev-Lobatto guess (src/tools/gauss_lobatto.jl), nodes in decreasing order."""
+    x = np.cos(np.pi * np.arange(N) / (N - 1))
+    w = np.zeros(N)
+    w[0] = w[-1] = 2 / (N * (N - 1))
+    eps = np.finfo(float).eps
+    for i in range(1, N - 1):
+        xi, xold = float(x[i]), 2.0
+        P1 = 0.0
+        while abs(xi - xold) > eps:
+            xold = xi
+            P0, P1 = 1.0, xi
+            for n in range(2, N):
+                Pn = ((2 * n - 1) * xi * P1 - (n - 1) * P0) / n
+                P0, P1 = P1, Pn
+            dPdx = N * (P0 - xi * P1) / (1 - xi ** 2)
+            d2 = (2 * xi * dPdx - N * (N + 1) * P1) / (1 - xi ** 2)
+            xi -= dPdx / d2
+        x[i] = xi
+        w[i] = 2 / (N * (N - 1) * P1 ** 2)
+    return x, w
+
+
+def gauss_legendre_chebychev(N: int):
+    """Product quadrature: N Gauss-Legendre polar levels (ascending μ) × 2N equally spaced
+    azimuths ϕ = π(m − 1/2)/N, weight w_n·π/N (src/tools/gauss_legendre_chebychev.jl)."""
+    mun, wn = gauss_legendre(N)
+    idx = np.argsort(mun, kind="stable")
+    mun, wn = mun[idx], wn[idx]
+    mu, eta, xi, w = (np.zeros(2 * N * N) for _ in range(4))
+    i = 0
+    for n in range(N):
+        for m in range(1, 2 * N + 1):
+            phi = math.pi / N * (m - 0.5)
+            s = math.sqrt(1 - mun[n] ** 2)
+            mu[i], eta[i], xi[i], w[i] = mun[n], s * math.cos(phi), s * math.sin(phi), wn[n] * math.pi / N
+            i += 1
+    return [mu, eta, xi], w
+
+
 def newton_bisection(f, dfdx, a: float, b: float, tol: float = 1e-12, maxit: int = 100):
     """Safeguarded Newton iteration inside a bracketing interval
     (src/tools/newton_bisection.jl)."""
@@ -91,6 +132,10 @@ def quadrature(N: int, qtype: str, Ndims: int = 1, Qdims: int | None = None):
         Qdims = Ndims
     if qtype == "gauss-legendre" and Ndims == 1:
         Om, w = gauss_legendre(N)
+    elif qtype == "gauss-lobatto" and Ndims == 1:
+        Om, w = gauss_lobatto(N)
+    elif qtype == "gauss-legendre-chebychev":
+        Om, w = gauss_legendre_chebychev(N)
     elif qtype == "carlson":
         from .sphere import carlson
 
@@ -378,14 +423,111 @@ def fokker_planck_finite_difference_1d(N: int, qtype: str, Mn: np.ndarray, Dn: n
     return Dn @ Mnn @ Mn, lam0
 
 
+def fokker_planck_finite_difference_glc(N: int, Qdims: int, Mn: np.ndarray, Dn: np.ndarray):
+    """Finite-difference ℳ and λ₀ on the Gauss-Legendre-Chebychev product quadrature, the Qdims = 2
+    and 3 branches of fokker_planck_finite_difference.jl:79-148 / 190-264 (Morel's polar
+    differencing with β weights, azimuthal differencing scaled by γ_n; the azimuth spans [0, π]
+    without wrap-around for Qdims = 2, [0, 2π] periodically for Qdims = 3), shifted by
+    λ₀ = max |diag|, then Dn·ℳ·Mn."""
+    mui, wi = gauss_legendre(N)
+    idx = np.argsort(mui, kind="stable")
+    mui, wi = mui[idx], wi[idx]
+    Ni = len(mui)
+    wj = math.pi / Ni
+    na = Ni if Qdims == 2 else 2 * Ni          # azimuths per polar level
+    om = np.array([math.pi * (n + 0.5) / Ni for n in range(na)])
+    b12 = np.zeros(Ni + 1)
+    d12 = np.zeros(Ni + 1)
+    for n in range(1, Ni):
+        b12[n] = b12[n - 1] - 2 * wi[n - 1] * mui[n - 1]
+        d12[n] = (math.sqrt(1 - mui[n] ** 2) - math.sqrt(1 - mui[n - 1] ** 2)) / (mui[n] - mui[n - 1])
+    gam = np.zeros(Ni)
+    for n in range(Ni):
+        cn = (b12[n + 1] * d12[n + 1] - b12[n] * d12[n]) / wi[n]
+        Kn = 2 * (1 - mui[n] ** 2) + cn * math.sqrt(1 - mui[n] ** 2)
+        gam[n] = (math.pi ** 2 * Kn) / (2 * Ni ** 2 * (1 - math.cos(math.pi / Ni)))
+    M = np.zeros((Ni * na, Ni * na))
+
+    def gap_left(i):   # ω_i − ω_(i−1) (wrapping through 2π in 3D)
+        return om[i] - om[i - 1] if i > 0 else om[0] + 2 * math.pi - om[-1]
+
+    def gap_right(i):  # ω_(i+1) − ω_i
+        return om[i + 1] - om[i] if i < na - 1 else om[0] + 2 * math.pi - om[i]
+
+    for n in range(Ni):
+        a = 1.0 / (1 - mui[n] ** 2) * gam[n] / wj
+        up = b12[n + 1] / (mui[n + 1] - mui[n]) if n < Ni - 1 else 0.0
+        dn = b12[n] / (mui[n] - mui[n - 1]) if n > 0 else 0.0
+        for i in range(na):
+            ii = i + na * n
+            # polar coupling
+            M[ii, ii] -= (up + dn) / wi[n]
+            if n > 0:
+                M[ii, i + na * (n - 1)] += dn / wi[n]
+            if n < Ni - 1:
+                M[ii, i + na * (n + 1)] += up / wi[n]
+            # azimuthal coupling
+            if Qdims == 2:
+                if i > 0:
+                    M[ii, ii] -= a / gap_left(i)
+                    M[ii, ii - 1] += a / gap_left(i)
+                if i < na - 1:
+                    M[ii, ii] -= a / gap_right(i)
+                    M[ii, ii + 1] += a / gap_right(i)
+            else:
+                M[ii, ii] -= a / gap_left(i) + a / gap_right(i)
+                M[ii, (i - 1) % na + na * n] += a / gap_left(i)
+                M[ii, (i + 1) % na + na * n] += a / gap_right(i)
+    lam0 = float(np.max(np.abs(np.diag(M))))
+    M[np.diag_indices_from(M)] += lam0
+    return Dn @ M @ Mn, lam0
+
+
+def fokker_planck_differential_quadrature(N: int, qtype: str, Mn: np.ndarray, Dn: np.ndarray):
+    """Differential-quadrature ℳ and λ₀, 1D (fokker_planck_differential_quadrature.jl:23-65):
+    ℳ = (I − H²)·W¹² − 2·H·W¹ with the Lagrange first-derivative matrix W¹ on the nodes, shifted
+    by λ₀ = max(−diag)."""
+    mu, _ = quadrature(N, qtype, 1)
+    mu = np.asarray(mu, dtype=float)
+    H = np.diag(mu)
+    I = np.eye(N)
+    Pi = np.ones(N)
+    for n in range(N):
+        for m in range(N):
+            if n != m:
+                Pi[n] *= mu[n] - mu[m]
+    W1 = np.zeros((N, N))
+    for n in range(N):
+        for m in range(N):
+            if n != m:
+                W1[n, m] = Pi[n] / ((mu[n] - mu[m]) * Pi[m])
+    for n in range(N):
+        for m in range(N):
+            if n != m:
+                W1[n, n] -= W1[n, m]
+    M = (I - H @ H) @ (W1 @ W1) - 2 * H @ W1
+    lam0 = 0.0
+    for n in range(N):
+        if M[n, n] < -lam0:
+            lam0 = -M[n, n]
+    M[np.diag_indices_from(M)] += lam0
+    return Dn @ M @ Mn, lam0
+
+
 def fokker_planck_scattering_matrix(N, Nd, qtype, Ndims, method, Mn, Dn, pl, Np, Qdims):
     """fokker_planck_scattering_matrix.jl:29-48."""
     if method == "finite-difference":
-        if Qdims != 1:
-            raise NotImplementedError("finite-difference Fokker-Planck is built here for 1D quadratures only")
-        return fokker_planck_finite_difference_1d(N, qtype, Mn, Dn)
+        if Qdims == 1:
+            return fokker_planck_finite_difference_1d(N, qtype, Mn, Dn)
+        if qtype == "gauss-legendre-chebychev":
+            return fokker_planck_finite_difference_glc(N, Qdims, Mn, Dn)
+        raise NotImplementedError("finite-difference Fokker-Planck on a non-product quadrature needs the "
+                                  "spherical Voronoi weights, which are not built; use gauss-legendre-chebychev "
+                                  "or the galerkin method")
     if method == "galerkin":
         return fokker_planck_galerkin(Nd, Mn, Dn, pl, Np)
     if method == "differential-quadrature":
-        raise NotImplementedError("differential-quadrature Fokker-Planck is not built")
+        if Qdims != 1:
+            raise ValueError("Differential quadrature unavailable in multidimensional geometry.")
+        return fokker_planck_differential_quadrature(N, qtype, Mn, Dn)
     raise ValueError("Unknown method to treat the Fokker-Planck term.")

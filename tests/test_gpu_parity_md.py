@@ -197,3 +197,20 @@ def test_c3_shape_mixed(grid_ctx):
 def test_c4_shape_mixed(grid_ctx):
     check_mixed(grid_ctx, W.c4_tables(1, "photon", ng=1))
 
+
+
+def _sn_fd(N=4, L=2):
+    """The reference's default angular Fokker-Planck ("finite-difference") on the product
+    Gauss-Legendre-Chebychev quadrature."""
+    return SNSettings(solver_type="BFP", quadrature_type="gauss-legendre-chebychev", quadrature_order=N,
+                      legendre_order=L, scheme_type={"x": "DD", "y": "DD", "z": "DD", "E": "DD"},
+                      scheme_order={"x": 1, "y": 1, "z": 1, "E": 1}, acceleration="gmres",
+                      convergence_criterion=1e-9, angular_boltzmann="standard", maximum_iteration=400)
+
+
+def test_2d_bfp_finite_difference_fokker_planck(md_ctx):
+    check(md_ctx, grid2d(_sn_fd(), csd=True))
+
+
+def test_3d_bfp_finite_difference_fokker_planck(md_ctx):
+    check(md_ctx, grid3d(_sn_fd(), csd=True))

@@ -79,3 +79,66 @@ def test_get_schemes_moment_counts():
     assert O == [2, 1, 1, 2] and Nm == [2, 4, 4, 2, 4]
     _, O, Nm = T.get_schemes({"x": "DG", "E": "DG"}, {"x": 2, "E": 2}, ["x"], True, False)
     assert Nm == [2, 3, 3, 2, 3]
+
+
+def test_gauss_lobatto_and_legendre_chebychev_quadratures():
+    x, w = T.gauss_lobatto(7)
+    assert x[0] == 1.0 and x[-1] == -1.0
+    for k in range(0, 11):  # exact to degree 2N - 3
+        np.testing.assert_allclose((w * x ** k).sum(), (1 + (-1) ** k) / (k + 1), atol=1e-14)
+    Om, w = T.gauss_legendre_chebychev(6)
+    assert len(w) == 2 * 36
+    np.testing.assert_allclose(w.sum(), 4 * np.pi, rtol=1e-14)
+    for a in range(3):
+        np.testing.assert_allclose((w * Om[a] ** 2).sum(), 4 * np.pi / 3, rtol=1e-13)
+        np.testing.assert_allclose((w * Om[a]).sum(), 0.0, atol=1e-13)
+
+
+@pytest.mark.parametrize("Qdims", [2, 3])
+def test_finite_difference_fokker_planck_on_the_product_quadrature(Qdims):
+    """fokker_planck_finite_difference.jl, product-quadrature branches: every row of ℳ_n − λ₀I sums
+    to zero (the operator conserves particles), the shifted diagonal is non-negative, and the
+    first-order harmonics are eigenvectors with the Laplace-Beltrami value −l(l+1) = −2 (the scheme
+    is moment-preserving): μ and η in 2D (the folded half-range domain), μ, η, ξ in 3D."""
+    for N in (4, 8, 16):
+        Om, w = T.quadrature(N, "gauss-legendre-chebychev", 3, Qdims)
+        Nd = len(w)
+        M, lam0 = T.fokker_planck_finite_difference_glc(N, Qdims, np.eye(Nd), np.eye(Nd))
+        L = M - lam0 * np.eye(Nd)
+        np.testing.assert_allclose(L.sum(axis=1), 0.0, atol=1e-10 * lam0)
+        assert np.all(np.diag(M) >= -1e-12) and lam0 > 0
+        for a in range(2 if Qdims == 2 else 3):
+            f = np.asarray(Om[a])
+            np.testing.assert_allclose(L @ f, -2 * f, atol=1e-10)
+
+
+def test_differential_quadrature_fokker_planck_is_exact_on_legendre_polynomials():
+    """fokker_planck_differential_quadrature.jl: the Lagrange-derivative form is exact on
+    polynomials below the quadrature order: (ℳ − λ₀I)·P_l(μ) = −l(l+1)·P_l(μ)."""
+    N = 8
+    mu, w = T.quadrature(N, "gauss-legendre", 1)
+    M, lam0 = T.fokker_planck_differential_quadrature(N, "gauss-legendre", np.eye(N), np.eye(N))
+    L = M - lam0 * np.eye(N)
+    for l in range(N):
+        P = np.array([T.legendre_polynomials_up_to_L(l, float(m))[l] for m in mu])
+        np.testing.assert_allclose(L @ P, -l * (l + 1) * P, atol=1e-8 * max(1, l * l))
+
+
+@pytest.mark.parametrize("ndims", [2, 3])
+def test_default_fokker_planck_tables_build_in_2d_and_3d(ndims):
+    """A BFP problem with the default angular Fokker-Planck ("finite-difference") on the product
+    quadrature sets up in 2D and 3D, and the oracle solves it to a finite flux."""
+    from oracle import run as orun
+    from radiant_b200 import workloads as W
+    from radiant_b200.sn_flux import SNSettings
+    sn = SNSettings(solver_type="BFP", quadrature_type="gauss-legendre-chebychev", quadrature_order=4,
+                    legendre_order=2, scheme_type={"x": "DD", "y": "DD", "z": "DD", "E": "DD"},
+                    scheme_order={"x": 1, "y": 1, "z": 1, "E": 1}, acceleration="gmres", convergence_criterion=1e-8,
+                    angular_boltzmann="standard")
+    n = [5, 4] if ndims == 2 else [4, 3, 3]
+    mats = np.ones(n, dtype=np.int32)
+    t = W.grid_tables(ndims, n, [np.full(k, 0.25) for k in n], mats, 3, 1, 1, sn, 2,
+                      volume=(0, {0: (0.0, 0.5)}), csd=True)
+    assert t["fp"] is not None and t["fp"].shape == (t["np"], t["np"])
+    r = orun.solve(t)
+    assert np.all(np.isfinite(r.flux)) and r.flux.sum() > 0
