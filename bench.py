@@ -373,6 +373,15 @@ def run_c2_section(args, ctx, sptr, stream, rank, world):
             peak, pk = peaks()
             out["fp64"]["roofline_frac"] = ab / (ms / 1e3) / 1e9 / peak
     out["mixed"]["max_rel_l2_vs_fp64"] = max(rel_l2(a.flux, b.flux) for a, b in zip(rbs_by["mixed"], rbs_by["fp64"]))
+    # the team size: the packaged launch rules (radiant_b200/autotune.py) where one covers the
+    # batch, else the built-in choice
+    from radiant_b200.autotune import work_of
+    tabs = workload_tables(seeds[:1], "fp64", "c2")
+    wmax = max(work_of(t) for t in tabs)
+    rule = next((r for r in ctx.launch_rules if r["ndims"] == 1 and r["nd_max"] >= tabs[0]["nd"]
+                 and r["work_max"] >= wmax), None)
+    out["launch_team"] = (f"{rule['cluster']} CTAs per problem (tuned rule)" if rule
+                          else "built-in shape choice (no tuned rule covers the batch)")
     return out
 
 

@@ -215,6 +215,8 @@ struct rb_context {
     // serving: stream pool for concurrently running requests
     std::vector<cudaStream_t> serve_streams;
     size_t next_stream = 0;
+    // measured launch rules (rb_set_launch_rules): team size by problem class
+    std::vector<rb_launch_rule> rules;
 };
 
 namespace {
@@ -797,6 +799,31 @@ int ensure_launch_scratch(rb_context *ctx, int n) {
     return RB_OK;
 }
 
+// The work estimate of a problem (the work queue's order and the launch rules' classes):
+// groups × directions × cells × cell moments, doubled for the CSD solvers.
+static double problem_work(const DevProblem &h) {
+    return (double)h.ng * h.nd * (double)h.ncell * h.nm5 * (h.csd ? 2.0 : 1.0);
+}
+
+// The team size the launch rules give a set of problems: the first rule of each problem's
+// dimension whose direction and work bounds cover it; the largest of the problems' sizes; 0 when
+// some problem has no rule (the built-in shape choice then applies).
+static int rule_cluster(const rb_context *ctx, const std::vector<const DevProblem *> &hs) {
+    if (!ctx || ctx->rules.empty() || hs.empty()) return 0;
+    int c = 0;
+    for (const DevProblem *h : hs) {
+        int got = 0;
+        for (const rb_launch_rule &r : ctx->rules)
+            if (r.ndims == h->ndims && h->nd <= r.nd_max && problem_work(*h) <= (double)r.work_max) {
+                got = r.cluster;
+                break;
+            }
+        if (got <= 0) return 0;
+        c = std::max(c, got);
+    }
+    return c;
+}
+
 int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t s) {
     int n = (int)recs.size();
     if (n == 0) return RB_OK;
@@ -817,20 +844,20 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
     // the work queue hands problems out heaviest first (longest-processing-time order), so the
     // light ones fill the teams' last slots; the estimate is groups × directions × cells × cell
     // moments, doubled for the CSD solvers
-    auto work = [](const DevProblem &h) {
-        return (double)h.ng * h.nd * (double)h.ncell * h.nm5 * (h.csd ? 2.0 : 1.0);
-    };
+    auto work = [](const DevProblem &h) { return problem_work(h); };
     std::stable_sort(qs.begin(), qs.end(), [&](const ProblemRec *a, const ProblemRec *b) { return work(a->h) > work(b->h); });
     for (auto *r : qs) { small.push_back(r->d); small_h.push_back(&r->h); }
     if (!small.empty()) {
         CK(cudaMemcpyAsync(ctx->d_list, small.data(), sizeof(DevProblem *) * small.size(), cudaMemcpyHostToDevice, s));
         int cluster = ctx->cluster;
+        const int ruled = cluster > 0 ? 0 : rule_cluster(ctx, small_h);
+        if (ruled > 0) cluster = ruled;  // a measured launch rule
         if (cluster <= 0) {  // one cluster per problem, sized to the problem's directions
             const DevProblem &h0 = recs[0]->h;
             cluster = h0.nd >= 32 ? 4 : (h0.nd >= 16 ? 4 : (h0.nd >= 8 ? 2 : 1));
         }
         int st2 = launch_solve(ctx, ctx->d_list, (int)small.size(), ctx->d_queue, ctx->nsm, cluster, s, small_h,
-                               ctx->cluster > 0 ? LAUNCH_FIXED : LAUNCH_BATCH);
+                               (ctx->cluster > 0 || ruled > 0) ? LAUNCH_FIXED : LAUNCH_BATCH);
         if (st2) return st2;
     }
     for (auto *r : large) {
@@ -1205,6 +1232,17 @@ int32_t rb_energy_deposition(int32_t ng, int32_t np, int32_t nm5, int64_t ncell,
         if (flux_cutoff) d += sigma_e[ng + (int64_t)(ng + 1) * m] * flux_cutoff[(int64_t)np * nm5 * c];
         dep[c] = d / (density[m] * norm);
     }
+    return RB_OK;
+}
+
+int32_t rb_set_launch_rules(rb_context *ctx, const rb_launch_rule *rules, int32_t n) {
+    if (!ctx || n < 0 || (n > 0 && !rules)) return fail(ctx, RB_ERR_INVALID, "bad launch rules");
+    for (int i = 0; i < n; i++)
+        if (rules[i].ndims < 1 || rules[i].ndims > 3 || rules[i].cluster < 1 || rules[i].cluster > RB_MAXCLUSTER ||
+            (rules[i].cluster & (rules[i].cluster - 1)) != 0)
+            return fail(ctx, RB_ERR_INVALID, "launch rule %d: dimension 1-3 and a power-of-two team of 1-%d CTAs",
+                        i, RB_MAXCLUSTER);
+    ctx->rules.assign(rules, rules + n);
     return RB_OK;
 }
 

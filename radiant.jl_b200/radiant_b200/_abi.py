@@ -55,6 +55,10 @@ class RbCoupling(C.Structure):
     _fields_ = [("sigma_s", _dp), ("ls", C.c_int32), ("transfer", _dp), ("moment_map", _ip)]
 
 
+class RbLaunchRule(C.Structure):
+    _fields_ = [("ndims", C.c_int32), ("nd_max", C.c_int32), ("work_max", C.c_int64), ("cluster", C.c_int32)]
+
+
 class RbSnResult(C.Structure):
     _fields_ = [
         ("flux", _dp), ("flux_cutoff", _dp), ("rho", _dp), ("group_iters", _ip),
@@ -221,6 +225,7 @@ def load_library(path: str | None = None):
         "rb_transport": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(PP), C.POINTER(RbCoupling), C.c_int32,
                                      C.c_double, C.c_int32, C.POINTER(_dp), _dp, C.c_double, C.POINTER(RP), _dp,
                                      _ip, _dp]),
+        "rb_set_launch_rules": (C.c_int32, [vp, C.POINTER(RbLaunchRule), C.c_int32]),
         "rb_deposition": (C.c_int32, [vp, C.c_int32, C.POINTER(h64), C.POINTER(_dp), _dp, C.c_double, _dp]),
         "rb_version": (C.c_char_p, []),
     }
@@ -236,8 +241,21 @@ def load_library(path: str | None = None):
 EXPORTED_SYMBOLS = (
     "rb_create", "rb_destroy", "rb_last_error", "rb_upload", "rb_solve", "rb_solve_batch",
     "rb_download", "rb_release", "rb_required_bytes", "rb_compute_flux", "rb_submit", "rb_poll",
-    "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_version",
+    "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_set_launch_rules", "rb_version",
 )
+
+
+RULES_PATH = os.path.join(_HERE, "launch_rules.json")
+
+
+def packaged_launch_rules() -> list:
+    """The tuning table shipped with the package (empty when there is none)."""
+    if not os.path.exists(RULES_PATH):
+        return []
+    import json
+
+    with open(RULES_PATH) as f:
+        return json.load(f)["rules"]
 
 
 class RadiantError(RuntimeError):
@@ -249,13 +267,30 @@ class RadiantError(RuntimeError):
 class Context:
     """Owns one rb_context (one device, one HBM budget)."""
 
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, launch_rules="packaged"):
+        """launch_rules: "packaged" applies the tuning table shipped with the package
+        (launch_rules.json, written by radiant_b200.autotune) when present; a list of rule dicts
+        applies those; None leaves the built-in shape choice."""
         self.lib = load_library()
         self._ncell = {}  # voxels of each uploaded problem (deposition maps)
         self.h = C.c_void_p()
         st = self.lib.rb_create(device, hbm_budget_bytes, C.byref(self.h))
         if st != RB_OK:
             raise RadiantError(st, self.last_error(None))
+        self.launch_rules = []
+        if launch_rules == "packaged":
+            launch_rules = packaged_launch_rules()
+        if launch_rules:
+            self.set_launch_rules(launch_rules)
+
+    def set_launch_rules(self, rules):
+        """rb_set_launch_rules: rules = [{"ndims", "nd_max", "work_max", "cluster"}, ...]."""
+        arr = (RbLaunchRule * max(len(rules), 1))()
+        for k, r in enumerate(rules):
+            arr[k].ndims, arr[k].nd_max = int(r["ndims"]), int(r["nd_max"])
+            arr[k].work_max, arr[k].cluster = int(r["work_max"]), int(r["cluster"])
+        self.check(self.lib.rb_set_launch_rules(self.h, arr, len(rules)))
+        self.launch_rules = [dict(r) for r in rules]
 
     def last_error(self, h="self") -> str:
         buf = C.create_string_buffer(1024)

@@ -83,3 +83,15 @@ def test_rejects_oversized_restart():
 def test_missing_library_fails_loudly(tmp_path):
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         load_library(str(tmp_path / "nope.so"))
+
+
+def test_launch_rule_struct_and_table_shape():
+    """The launch-rule struct mirrors rb_launch_rule, and the packaged table (when present) holds
+    rules the library accepts: dimension 1-3, power-of-two teams up to 16, increasing work."""
+    import ctypes as C
+    from radiant_b200._abi import RbLaunchRule, packaged_launch_rules
+    assert C.sizeof(RbLaunchRule) == 24
+    rules = packaged_launch_rules()
+    for r in rules:
+        assert r["ndims"] in (1, 2, 3) and r["cluster"] in (1, 2, 4, 8, 16) and r["nd_max"] > 0
+    assert [r["work_max"] for r in rules] == sorted(r["work_max"] for r in rules)

@@ -102,3 +102,26 @@ def test_batch_of_mixed_shapes(gpu_ctx):
         ref = oracle_run.solve(t)
         assert rel_l2(rb.flux, ref.flux) <= TOL
         assert rb.passes == ref.passes
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cluster", [2, 16])
+def test_launch_rules_set_the_team_and_keep_parity(cluster):
+    """rb_set_launch_rules: a batch covered by a rule runs with the rule's team size, and the
+    results still match the oracle within the parity tolerance."""
+    from oracle import run as orun
+    from radiant_b200._abi import Context, PackedProblem, ResultBuffers
+    from radiant_b200.autotune import work_of
+    batch = [W.c1_tables(seed=s) for s in (1, 2)]
+    ctx = Context(0, 0, launch_rules=[{"ndims": 1, "nd_max": 64, "work_max": int(max(work_of(t) for t in batch)) + 1,
+                                       "cluster": cluster}])
+    pps = [PackedProblem(t) for t in batch]
+    hs = [ctx.upload(p) for p in pps]
+    ctx.solve_batch(hs)
+    for h, p, t in zip(hs, pps, batch):
+        rb = ResultBuffers(p)
+        ctx.download(h, rb)
+        ref = orun.solve(t)
+        assert np.linalg.norm(rb.flux - ref.flux) / np.linalg.norm(ref.flux) <= 1e-10
+        assert rb.passes == ref.passes
+    ctx.close()
