@@ -237,16 +237,18 @@ RB_API int32_t rb_transport(int32_t device, int32_t npart, const rb_sn_problem *
 
 /* ---- launch rules (the autotuner's table) --------------------------------------------- */
 /* No counterpart in the reference (a Julia solve has no launch shape). A rule gives the team size
- * (CTAs per problem, a power of two up to 16) for the problems of a class: dimension `ndims`, at
- * most nd_max directions and at most work_max work (groups × directions × cells × cell moments,
- * doubled for the CSD solvers). rb_solve / rb_solve_batch of problems that all match a rule (the
- * first matching rule of each; the largest team among them) launch with that team size, which a
- * tuning run measured as the fastest for the class (radiant_b200/autotune.py); other batches keep
- * the built-in shape choice. Serving requests (rb_submit) do not use the rules. n = 0 clears them. */
+ * (CTAs per problem, a power of two up to 16) for the problems of a class in batches of a size:
+ * dimension `ndims`, at most nd_max directions, at most work_max work (groups × directions ×
+ * cells × cell moments, doubled for the CSD solvers), in a batch of at most batch_max problems.
+ * rb_solve / rb_solve_batch of problems that all match a rule (the first matching rule of each;
+ * the largest team among them) launch with that team size, which a tuning run measured as the
+ * fastest for the class at that batch size (radiant_b200/autotune.py); other batches keep the
+ * built-in shape choice. Serving requests (rb_submit) do not use the rules. n = 0 clears them. */
 typedef struct rb_launch_rule {
     int32_t ndims;
     int32_t nd_max;
     int64_t work_max;
+    int32_t batch_max;
     int32_t cluster;
 } rb_launch_rule;
 RB_API int32_t rb_set_launch_rules(rb_context *ctx, const rb_launch_rule *rules, int32_t n);

@@ -805,16 +805,17 @@ static double problem_work(const DevProblem &h) {
     return (double)h.ng * h.nd * (double)h.ncell * h.nm5 * (h.csd ? 2.0 : 1.0);
 }
 
-// The team size the launch rules give a set of problems: the first rule of each problem's
-// dimension whose direction and work bounds cover it; the largest of the problems' sizes; 0 when
-// some problem has no rule (the built-in shape choice then applies).
+// The team size the launch rules give a batch: for each problem the first rule of its dimension
+// whose direction, work and batch-size bounds cover it; the largest of the problems' sizes; 0
+// when some problem has no rule (the built-in shape choice then applies).
 static int rule_cluster(const rb_context *ctx, const std::vector<const DevProblem *> &hs) {
     if (!ctx || ctx->rules.empty() || hs.empty()) return 0;
     int c = 0;
     for (const DevProblem *h : hs) {
         int got = 0;
         for (const rb_launch_rule &r : ctx->rules)
-            if (r.ndims == h->ndims && h->nd <= r.nd_max && problem_work(*h) <= (double)r.work_max) {
+            if (r.ndims == h->ndims && h->nd <= r.nd_max && problem_work(*h) <= (double)r.work_max &&
+                (long long)hs.size() <= (long long)r.batch_max) {
                 got = r.cluster;
                 break;
             }

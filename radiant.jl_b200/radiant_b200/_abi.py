@@ -56,7 +56,8 @@ class RbCoupling(C.Structure):
 
 
 class RbLaunchRule(C.Structure):
-    _fields_ = [("ndims", C.c_int32), ("nd_max", C.c_int32), ("work_max", C.c_int64), ("cluster", C.c_int32)]
+    _fields_ = [("ndims", C.c_int32), ("nd_max", C.c_int32), ("work_max", C.c_int64), ("batch_max", C.c_int32),
+                ("cluster", C.c_int32)]
 
 
 class RbSnResult(C.Structure):
@@ -284,11 +285,12 @@ class Context:
             self.set_launch_rules(launch_rules)
 
     def set_launch_rules(self, rules):
-        """rb_set_launch_rules: rules = [{"ndims", "nd_max", "work_max", "cluster"}, ...]."""
+        """rb_set_launch_rules: rules = [{"ndims", "nd_max", "work_max", "batch_max", "cluster"}, ...]."""
         arr = (RbLaunchRule * max(len(rules), 1))()
         for k, r in enumerate(rules):
             arr[k].ndims, arr[k].nd_max = int(r["ndims"]), int(r["nd_max"])
             arr[k].work_max, arr[k].cluster = int(r["work_max"]), int(r["cluster"])
+            arr[k].batch_max = int(r.get("batch_max", 2 ** 31 - 1))
         self.check(self.lib.rb_set_launch_rules(self.h, arr, len(rules)))
         self.launch_rules = [dict(r) for r in rules]
 

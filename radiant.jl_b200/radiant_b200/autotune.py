@@ -1,12 +1,14 @@
 """Launch-shape autotuner: measures the team size (CTAs per problem) of batched solves per
 problem class and writes the table the library applies (rb_set_launch_rules).
 
-A class is a representative batch of problems (the configurations' shapes and the serving
-stream's size bins). For each class the tuner uploads the batch once, times rb_solve_batch at
-every candidate team size (a rule covering exactly the class, CUDA events around the launch,
-after a warm-up solve), and keeps the fastest. Rules are written in increasing order of work,
-each covering the problems up to its class's largest direction count and work, so a problem
-takes the rule of the smallest class that contains it.
+A class is a representative set of problems (the configurations' shapes and the serving stream's
+size bins), measured at two batch sizes (a small batch and a full one: the best team depends on
+how many problems share the GPU). For each (class, batch size) the tuner uploads the batch once,
+times rb_solve_batch at every candidate team size (a rule covering exactly that batch, wall clock
+around the synchronised launch, best of `reps` after a warm-up solve) and keeps the fastest.
+Rules are written small batches first, then in increasing order of work, each covering the
+problems up to its class's largest direction count and work and batches up to its size, so a
+batch takes the rule of the smallest class and batch size that contain it.
 
     python -m radiant_b200.autotune --out radiant_b200/launch_rules.json
 """
@@ -28,13 +30,17 @@ def work_of(tabs: dict) -> float:
     return float(tabs["ng"]) * tabs["nd"] * ncell * tabs["nm"][4] * (2.0 if tabs["solver_type"] >= 2 else 1.0)
 
 
+SMALL_BATCH, FULL_BATCH = 24, 150
+
+
 def default_classes(seed: int = 1) -> dict:
-    """Representative 1D batches: the two slab configurations and three size bins of the serving
-    stream's slab requests (by work)."""
-    c1 = [W.c1_tables(seed=s) for s in range(1, 9)]
-    c2 = [W.c2_tables(seed=s, particle=p) for s in range(1, 9) for p in ("photon", "electron", "positron")]
+    """Representative 1D problem sets of FULL_BATCH problems: the two slab configurations and
+    three size bins of the serving stream's slab requests (by work)."""
+    c1 = [W.c1_tables(seed=s) for s in range(1, FULL_BATCH + 1)]
+    c2 = [W.c2_tables(seed=s, particle=p) for s in range(1, FULL_BATCH // 3 + 1)
+          for p in ("photon", "electron", "positron")]
     rng = np.random.default_rng(seed)
-    slabs = [W.random_slab_tables(int(rng.integers(0, 2 ** 31 - 1))) for _ in range(72)]
+    slabs = [W.random_slab_tables(int(rng.integers(0, 2 ** 31 - 1))) for _ in range(3 * FULL_BATCH)]
     slabs.sort(key=work_of)
     k = len(slabs) // 3
     return {"serving slabs, small": slabs[:k], "serving slabs, medium": slabs[k:2 * k],
@@ -58,29 +64,35 @@ def time_batch(ctx: Context, handles: list, reps: int) -> float:
     return best
 
 
-def tune(classes: dict, candidates=(2, 4, 8, 16), reps: int = 2) -> dict:
-    """Measures every class at every candidate team size; returns the table and the timings."""
+def tune(classes: dict, candidates=(2, 4, 8, 16), reps: int = 2, sizes=(SMALL_BATCH, FULL_BATCH)) -> dict:
+    """Measures every class at every batch size and candidate team size; returns the table and
+    the timings."""
     ctx = Context(0, 0, launch_rules=None)
     entries = []
-    for name, batch in classes.items():
-        nd_max = max(t["nd"] for t in batch)
-        wmax = max(work_of(t) for t in batch)
-        handles = [ctx.upload(PackedProblem(t)) for t in batch]
-        times = {}
-        for c in candidates:
-            ctx.set_launch_rules([{"ndims": batch[0]["ndims"], "nd_max": nd_max, "work_max": int(wmax) + 1,
-                                   "cluster": c}])
-            times[c] = time_batch(ctx, handles, reps)
-        for h in handles:
-            ctx.release(h)
-        ctx.set_launch_rules([])
-        best = min(times, key=times.get)
-        entries.append({"class": name, "ndims": int(batch[0]["ndims"]), "nd_max": int(nd_max),
-                        "work_max": int(wmax) + 1, "cluster": int(best), "problems": len(batch),
-                        "seconds": {str(c): round(t, 5) for c, t in times.items()}})
+    for name, probs in classes.items():
+        nd_max = max(t["nd"] for t in probs)
+        wmax = max(work_of(t) for t in probs)
+        for size in sizes:
+            # a seeded sample that keeps the set's composition (particles, sizes)
+            pick = np.sort(np.random.default_rng(size).choice(len(probs), size=min(size, len(probs)), replace=False))
+            batch = [probs[i] for i in pick]
+            handles = [ctx.upload(PackedProblem(t)) for t in batch]
+            times = {}
+            for c in candidates:
+                ctx.set_launch_rules([{"ndims": batch[0]["ndims"], "nd_max": nd_max, "work_max": int(wmax) + 1,
+                                       "batch_max": len(batch), "cluster": c}])
+                times[c] = time_batch(ctx, handles, reps)
+            for h in handles:
+                ctx.release(h)
+            ctx.set_launch_rules([])
+            best = min(times, key=times.get)
+            entries.append({"class": name, "ndims": int(batch[0]["ndims"]), "nd_max": int(nd_max),
+                            "work_max": int(wmax) + 1, "batch_max": len(batch) if size != sizes[-1] else 2 ** 31 - 1,
+                            "cluster": int(best), "problems": len(batch),
+                            "seconds": {str(c): round(t, 5) for c, t in times.items()}})
     ctx.close()
-    entries.sort(key=lambda e: e["work_max"])
-    rules = [{k: e[k] for k in ("ndims", "nd_max", "work_max", "cluster")} for e in entries]
+    entries.sort(key=lambda e: (e["batch_max"], e["work_max"]))
+    rules = [{k: e[k] for k in ("ndims", "nd_max", "work_max", "batch_max", "cluster")} for e in entries]
     return {"rules": rules, "measured": entries}
 
 

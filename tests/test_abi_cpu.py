@@ -94,4 +94,5 @@ def test_launch_rule_struct_and_table_shape():
     rules = packaged_launch_rules()
     for r in rules:
         assert r["ndims"] in (1, 2, 3) and r["cluster"] in (1, 2, 4, 8, 16) and r["nd_max"] > 0
-    assert [r["work_max"] for r in rules] == sorted(r["work_max"] for r in rules)
+    keys = [(r["batch_max"], r["work_max"]) for r in rules]
+    assert keys == sorted(keys)

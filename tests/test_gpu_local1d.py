@@ -114,7 +114,7 @@ def test_launch_rules_set_the_team_and_keep_parity(cluster):
     from radiant_b200.autotune import work_of
     batch = [W.c1_tables(seed=s) for s in (1, 2)]
     ctx = Context(0, 0, launch_rules=[{"ndims": 1, "nd_max": 64, "work_max": int(max(work_of(t) for t in batch)) + 1,
-                                       "cluster": cluster}])
+                                       "batch_max": 8, "cluster": cluster}])
     pps = [PackedProblem(t) for t in batch]
     hs = [ctx.upload(p) for p in pps]
     ctx.solve_batch(hs)
