@@ -57,18 +57,22 @@ __device__ __forceinline__ bool one_moment_md(const DevProblem &P) {
 template <typename R> struct OctDB { static constexpr int value = 10; };  // FP64: registers
 template <> struct OctDB<float> { static constexpr int value = 12; };
 
-#define RB_OCT_NB 2        // stages of a step's inputs (cp.async, one step ahead)
+// Stages of a step's inputs (cp.async, one step ahead): three, which lets a step write back the
+// previous step's flux after its single barrier; two for FP64 with CSD (three do not fit beside
+// the FP64 energy-face stages), with a second barrier per step.
+template <typename R, bool CSD> struct OctNB { static constexpr int value = 3; };
+template <> struct OctNB<double, true> { static constexpr int value = 2; };
 #define RB_OCT_MAXNX 1024  // x widths whose inverses the sweep keeps in shared memory
 #define RB_OCT_PUB 2       // a CTA publishes its progress every RB_OCT_PUB steps (and after its last)
 
 // Shared-memory plan of the 3D octant sweep (byte offsets, each array 16-byte aligned): the
-// staged upwind faces of the tile's first row and layer of pencils, RB_OCT_NB stages of a step's
+// staged upwind faces of the tile's first row and layer of pencils, OctNB stages of a step's
 // angular source / flux, energy-face flux (CSD) and materials, the z-face hand-off between
 // pencils (double-buffered by step parity), the direction constants of the octant batch, the
 // inverse x widths and the per-material cell terms, and each pencil's cell base and coordinates.
 template <typename R, bool CSD>
 struct Oct3dSmem {
-    static constexpr long long DB = OctDB<R>::value, T = RB_OCT_TILE, TP = T * T, NB = RB_OCT_NB;
+    static constexpr long long DB = OctDB<R>::value, T = RB_OCT_TILE, TP = T * T, NB = OctNB<R, CSD>::value;
     static constexpr long long RS = (long long)sizeof(R);
     static constexpr long long al(long long b) { return (b + 15) & ~15LL; }
     static constexpr long long fy = 0;                                      // double [NB][T][DB]
@@ -164,7 +168,11 @@ __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShar
                                          int np_source, const double *phiE_in, double *phiE_out, int ig, PS *psi) {
     using L = Oct3dSmem<R, CSD>;
     static_assert(sizeof(PS) == sizeof(R), "angular buffer and arithmetic of one width");
-    constexpr int DB = OctDB<R>::value, TT = RB_OCT_TILE, TP = TT * TT, NB = RB_OCT_NB;
+    constexpr int DB = OctDB<R>::value, TT = RB_OCT_TILE, TP = TT * TT, NB = OctNB<R, CSD>::value;
+    // one barrier per step: the write-back and the publication of step sg follow the barrier of
+    // step sg + 1, which also orders the z-face hand-off; the stage being written back is then
+    // neither the one being staged nor the one being solved
+    constexpr bool ONEBAR = NB >= 3;
     const int nd = P.nd, nx = P.nx, ny = P.ny, nz = P.nz, nfm = P.nfmax;
     const int TY = oct_ty(ny), TZ = min(nz, RB_OCT_TILE);
     const int nty = (ny + TY - 1) / TY, ntz = (nz + TZ - 1) / TZ, ntiles = nty * ntz;
@@ -324,13 +332,40 @@ __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShar
                 fxs[k] = (pok && k < cnt) ? (R)P.fexit[(long long)(first + k) * sstride + o] : R(0);
             }
         }
+        // step s done by every thread: publish it (the barrier before this orders every thread's
+        // face stores before thread 0's fence and release), then write its stage back, consecutive
+        // lanes on consecutive directions of a cell
+        auto finish = [&](int s) {
+            if (me == 0 && ((s + 1) % RB_OCT_PUB == 0 || s == nsteps - 1)) {
+                __threadfence();
+                st_release_u64(P.oct_flags + t.crank, tagr | (unsigned long long)(s + 1));
+            }
+            const int ss = s % NB;
+            int p = p0, k = k0;
+#pragma unroll
+            for (int r = 0; r < DB; r++) {
+                if (r < cnt) {
+                    const long long c = cell_of(p, s);
+                    if (c >= 0) {
+                        const long long so = ((long long)ss * TP + p) * DB + k;
+                        const long long go = first + k + (long long)nd * c;
+                        psi[go] = qb[so];
+                        if (CSD) phiE_out[go] = eb[so];
+                    }
+                }
+                p += qd;
+                k += rm;
+                if (k >= cnt) { k -= cnt; p++; }
+            }
+        };
         wait_up(0);
         __syncthreads();
         issue(0);
         for (int sg = 0; sg < nsteps; sg++) {
             wait_up(sg + 1);
             cp_async_wait<0>();  // this thread's copies of step sg have landed
-            __syncthreads();     // everyone's; step sg − 1's stage is free; step sg + 1's faces are written
+            __syncthreads();     // everyone's; step sg − 1 solved; step sg + 1's faces are written
+            if (ONEBAR && sg > 0) finish(sg - 1);
             issue(sg + 1);       // in flight while step sg is solved
             const int ixx = sg - jy - jz;
             const int rd = (sg + 1) & 1, wr = sg & 1, sb = sg % NB;
@@ -405,33 +440,14 @@ __device__ __noinline__ void sweep3d_oct(Team &t, const DevProblem &P, GroupShar
             }
 #pragma unroll
             for (int k = 0; k < DB; k++) fyl[k] = fyi[k];
+            if (!ONEBAR) {
+                __syncthreads();
+                finish(sg);
+            }
+        }
+        if (ONEBAR && nsteps > 0) {
             __syncthreads();
-            // the faces of step sg are stored: publish (the barrier orders every thread's stores
-            // before thread 0's fence and release)
-            if (me == 0 && ((sg + 1) % RB_OCT_PUB == 0 || sg == nsteps - 1)) {
-                __threadfence();
-                st_release_u64(P.oct_flags + t.crank, tagr | (unsigned long long)(sg + 1));
-            }
-            // the step's angular flux (and outgoing energy-face flux) back to global memory,
-            // consecutive lanes on consecutive directions of a cell
-            {
-                int p = p0, k = k0;
-#pragma unroll
-                for (int r = 0; r < DB; r++) {
-                    if (r < cnt) {
-                        const long long c = cell_of(p, sg);
-                        if (c >= 0) {
-                            const long long so = ((long long)sb * TP + p) * DB + k;
-                            const long long go = first + k + (long long)nd * c;
-                            psi[go] = qb[so];
-                            if (CSD) phiE_out[go] = eb[so];
-                        }
-                    }
-                    p += qd;
-                    k += rm;
-                    if (k >= cnt) { k -= cnt; p++; }
-                }
-            }
+            finish(nsteps - 1);
         }
         cp_async_wait<0>();
         __syncthreads();
