@@ -433,8 +433,11 @@ struct Solver {
         if (resid < tol) { st.iter = iter; st.resid = resid; st.conv = 1; st.rho = CUDART_NAN; return st; }
         double rho_old = 1.0, alpha = 1.0, omega = 1.0;
         const double tiny = 1e-300;
+        // (r̂·r) of the coming iteration: the initial loop's Σ r² (r̂ = r there), then the last
+        // loop's second sum (the same terms, in the same order per thread, as a separate dot)
+        double rho_next = a1[0];
         while (iter < maxit) {
-            const double rho_new = vdot2(t, rh, r, N2);
+            const double rho_new = rho_next;
             if (fabs(rho_new) < tiny) break;
             const double beta = (rho_new / rho_old) * (alpha / omega);
             {
@@ -481,19 +484,22 @@ struct Solver {
             t.template sumk<2>(a3);
             if (a3[0] < tiny) break;
             omega = a3[1] / a3[0];
-            double a4[1] = {0.0};
+            double a4[2] = {0.0, 0.0};
             {
-                double2 xz[4], xp[4], xs[4], xt[4];
-                RB_VPAIRS_D(t, N2, 4, { xz[u_] = z2[q]; xp[u_] = p2[q]; xs[u_] = s2[q]; xt[u_] = t2[q]; }, {
+                double2 xz[4], xp[4], xs[4], xt[4], xh[4];
+                RB_VPAIRS_D(t, N2, 4, { xz[u_] = z2[q]; xp[u_] = p2[q]; xs[u_] = s2[q]; xt[u_] = t2[q]; xh[u_] = rh2[q]; }, {
                     z2[q] = make_double2((xz[u_].x + alpha * xp[u_].x) + omega * xs[u_].x,
                                          (xz[u_].y + alpha * xp[u_].y) + omega * xs[u_].y);
                     const double2 ri = make_double2(xs[u_].x + (-omega) * xt[u_].x, xs[u_].y + (-omega) * xt[u_].y);
                     r2[q] = ri;
                     a4[0] += ri.x * ri.x;
                     a4[0] += ri.y * ri.y;
+                    a4[1] += xh[u_].x * ri.x;
+                    a4[1] += xh[u_].y * ri.y;
                 })
             }
-            t.template sumk<1>(a4);
+            t.template sumk<2>(a4);
+            rho_next = a4[1];
             resid = sqrt(a4[0]) / bnorm;
             if (resid < tol) { conv = 1; break; }
             if (fabs(omega) < tiny) break;
