@@ -278,6 +278,18 @@ RB_API int32_t rb_energy_deposition(int32_t ng, int32_t np, int32_t nm5, int64_t
 RB_API int32_t rb_deposition(rb_context *ctx, int32_t npart, const rb_handle *handles, const double *const *sigma_dep,
                              const double *density, double norm, double *dep);
 
+/* ---- page-locked host buffers ------------------------------------------------------------ */
+/* No counterpart in the reference (Julia arrays are pageable). The upload and download copies
+ * run at the host link's speed only from page-locked memory: from pageable memory the driver
+ * stages every copy through its own buffer at a fraction of it. rb_host_alloc returns `bytes`
+ * of page-locked memory usable by every device (free with rb_host_free); rb_host_register locks
+ * an existing allocation in place (a Julia Array's storage) until rb_host_unregister. Both cost
+ * time per byte (the pages are locked one by one): lock the buffers a caller reuses, once. */
+RB_API int32_t rb_host_alloc(uint64_t bytes, void **out);
+RB_API int32_t rb_host_free(void *p);
+RB_API int32_t rb_host_register(void *p, uint64_t bytes);
+RB_API int32_t rb_host_unregister(void *p);
+
 /* Library version string. */
 RB_API const char *rb_version(void);
 

@@ -1152,6 +1152,35 @@ int32_t rb_release(rb_context *ctx, rb_handle hd) {
     return RB_OK;
 }
 
+int32_t rb_host_alloc(uint64_t bytes, void **out) {
+    if (!out || bytes == 0) return fail(nullptr, RB_ERR_INVALID, "null output or zero size");
+    *out = nullptr;
+    cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return fail(nullptr, RB_ERR_CUDA, "cudaHostAlloc(%llu): %s", (unsigned long long)bytes, cudaGetErrorString(e));
+    }
+    return RB_OK;
+}
+
+int32_t rb_host_free(void *p) {
+    if (!p) return RB_OK;
+    cudaError_t e = cudaFreeHost(p);
+    return e == cudaSuccess ? RB_OK : fail(nullptr, RB_ERR_CUDA, "cudaFreeHost: %s", cudaGetErrorString(e));
+}
+
+int32_t rb_host_register(void *p, uint64_t bytes) {
+    if (!p || bytes == 0) return fail(nullptr, RB_ERR_INVALID, "null pointer or zero size");
+    cudaError_t e = cudaHostRegister(p, bytes, cudaHostRegisterPortable);
+    return e == cudaSuccess ? RB_OK : fail(nullptr, RB_ERR_CUDA, "cudaHostRegister: %s", cudaGetErrorString(e));
+}
+
+int32_t rb_host_unregister(void *p) {
+    if (!p) return fail(nullptr, RB_ERR_INVALID, "null pointer");
+    cudaError_t e = cudaHostUnregister(p);
+    return e == cudaSuccess ? RB_OK : fail(nullptr, RB_ERR_CUDA, "cudaHostUnregister: %s", cudaGetErrorString(e));
+}
+
 int32_t rb_compute_flux(int32_t device, const rb_sn_problem *prob, rb_sn_result *res) {
     rb_context *ctx = nullptr;
     int st = rb_create(device, 0, &ctx);

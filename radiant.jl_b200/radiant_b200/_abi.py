@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -76,6 +77,35 @@ def _i32(a) -> np.ndarray:
     return np.asfortranarray(np.asarray(a, dtype=np.int32))
 
 
+PINNED_MIN_BYTES = 1 << 20
+
+
+def pinned_empty(shape, dtype=np.float64, order: str = "F") -> np.ndarray:
+    """An uninitialised array in page-locked host memory (rb_host_alloc), given back
+    (rb_host_free) when the last view of it is gone."""
+    dt = np.dtype(dtype)
+    count = int(np.prod(shape))
+    if count == 0:
+        return np.empty(shape, dtype=dt, order=order)
+    lib = load_library()
+    p = C.c_void_p()
+    if lib.rb_host_alloc(count * dt.itemsize, C.byref(p)) != 0:
+        buf = C.create_string_buffer(512)
+        lib.rb_last_error(None, buf, 512)
+        raise MemoryError(f"rb_host_alloc({count * dt.itemsize} bytes): {buf.value.decode(errors='replace')}")
+    buf = (C.c_char * (count * dt.itemsize)).from_address(p.value)
+    weakref.finalize(buf, lib.rb_host_free, p.value)
+    return np.frombuffer(buf, dtype=dt, count=count).reshape(shape, order=order)
+
+
+def _pinned_copy(a: np.ndarray) -> np.ndarray:
+    if a.nbytes < PINNED_MIN_BYTES:
+        return a
+    out = pinned_empty(a.shape, a.dtype, "F")
+    out[...] = a
+    return out
+
+
 def _ptr(a, kind=_dp):
     if a is None:
         return C.cast(None, kind)
@@ -83,19 +113,28 @@ def _ptr(a, kind=_dp):
 
 
 class PackedProblem:
-    """An rb_sn_problem whose arrays are kept alive by this object."""
+    """An rb_sn_problem whose arrays are kept alive by this object. pinned=True puts the arrays
+    of PINNED_MIN_BYTES or more in page-locked host memory (the upload's copies then run at the
+    host link's speed)."""
 
-    def __init__(self, tables: dict):
+    def __init__(self, tables: dict, pinned: bool = False):
         self.t = t = {}
+
+        def f64(a):
+            return _pinned_copy(_f64(a)) if pinned else _f64(a)
+
+        def i32(a):
+            return _pinned_copy(_i32(a)) if pinned else _i32(a)
+
         P = RbSnProblem()
         P.ndims = tables["ndims"]
         ns = list(tables["ns"]) + [1] * (3 - len(tables["ns"]))
         P.nx, P.ny, P.nz = ns
         for k, name in enumerate(("dx", "dy", "dz")):
             arr = tables["ds"][k] if k < len(tables["ds"]) else None
-            t[name] = None if arr is None else _f64(arr)
+            t[name] = None if arr is None else f64(arr)
             setattr(P, name, _ptr(t[name]))
-        t["mat"] = _i32(tables["mat"])
+        t["mat"] = i32(tables["mat"])
         P.mat = _ptr(t["mat"], _ip)
         P.nmat = tables["nmat"]
         for f in range(6):
@@ -103,15 +142,15 @@ class PackedProblem:
         P.nd = tables["nd"]
         for k, name in enumerate(("mu", "eta", "xi")):
             arr = tables["omega"][k] if k < len(tables["omega"]) else None
-            t[name] = None if arr is None else _f64(arr)
+            t[name] = None if arr is None else f64(arr)
             setattr(P, name, _ptr(t[name]))
         P.np = tables["np"]
-        t["mn"], t["dn"], t["pl"] = _f64(tables["mn"]), _f64(tables["dn"]), _i32(tables["pl"])
+        t["mn"], t["dn"], t["pl"] = f64(tables["mn"]), f64(tables["dn"]), i32(tables["pl"])
         P.mn, P.dn, P.pl = _ptr(t["mn"]), _ptr(t["dn"]), _ptr(t["pl"], _ip)
         P.np_surf = tables["np_surf"]
         for f in range(6):
             if f < len(tables["mn_surf"]):
-                ms, ds_, nn = _f64(tables["mn_surf"][f]), _f64(tables["dn_surf"][f]), _i32(tables["n_to_nplus"][f])
+                ms, ds_, nn = f64(tables["mn_surf"][f]), f64(tables["dn_surf"][f]), i32(tables["n_to_nplus"][f])
                 t[f"ms{f}"], t[f"ds{f}"], t[f"nn{f}"] = ms, ds_, nn
                 P.nd_plus[f] = ms.shape[0]
                 P.mn_surf[f], P.dn_surf[f], P.n_to_nplus[f] = _ptr(ms), _ptr(ds_), _ptr(nn, _ip)
@@ -119,27 +158,27 @@ class PackedProblem:
                 P.nd_plus[f] = 0
         for a in range(4):
             P.order[a] = tables["order"][a]
-            t[f"w{a}"] = _f64(tables["w_axis"][a])
+            t[f"w{a}"] = f64(tables["w_axis"][a])
             P.w_axis[a] = _ptr(t[f"w{a}"])
         for a in range(5):
             P.nm[a] = tables["nm"][a]
         P.is_fc = int(tables["is_fc"])
-        t["cc"], t["ww"] = _f64(tables["cc"]), _f64(tables["ww"])
+        t["cc"], t["ww"] = f64(tables["cc"]), f64(tables["ww"])
         P.cc, P.ncc, P.ww = _ptr(t["cc"]), len(t["cc"]), _ptr(t["ww"])
         P.is_adaptive = int(tables.get("is_adaptive", 0))
         P.is_em = int(tables.get("is_em", 0))
         P.solver_type = tables["solver_type"]
         P.ng = tables["ng"]
-        t["sigma_t"], t["sigma_s"] = _f64(tables["sigma_t"]), _f64(tables["sigma_s"])
+        t["sigma_t"], t["sigma_s"] = f64(tables["sigma_t"]), f64(tables["sigma_s"])
         P.sigma_t, P.sigma_s, P.ls = _ptr(t["sigma_t"]), _ptr(t["sigma_s"]), tables["ls"]
         for name in ("s_minus", "s_plus", "s_mom", "t_mom", "fp", "e_width", "volume_sources"):
             arr = tables.get(name)
-            t[name] = None if arr is None else _f64(arr)
+            t[name] = None if arr is None else f64(arr)
             setattr(P, name, _ptr(t[name]))
         P.np_source = tables["np_source"]
         for f in range(6):
             ss = tables["surface_sources"][f] if f < len(tables["surface_sources"]) else None
-            t[f"ss{f}"] = None if ss is None else _f64(ss)
+            t[f"ss{f}"] = None if ss is None else f64(ss)
             P.surface_sources[f] = _ptr(t[f"ss{f}"])
         P.accel = ACCEL[tables["accel"]] if isinstance(tables["accel"], str) else tables["accel"]
         P.tol = tables["tol"]
@@ -162,13 +201,21 @@ class PackedProblem:
 
 
 class ResultBuffers:
-    """Caller-owned host buffers of an rb_sn_result."""
+    """Caller-owned host buffers of an rb_sn_result (the large ones page-locked when pinned)."""
 
-    def __init__(self, pp: PackedProblem):
+    def __init__(self, pp: PackedProblem, pinned: bool = False):
         t = pp.tables
         ng = t["ng"]
-        self.flux = np.zeros(pp.flux_shape, order="F")
-        self.flux_cutoff = np.zeros(pp.flux_shape[1:], order="F") if t["solver_type"] >= 2 else None
+
+        def zeros(shape):
+            if pinned and int(np.prod(shape)) * 8 >= PINNED_MIN_BYTES:
+                a = pinned_empty(shape)
+                a[...] = 0.0
+                return a
+            return np.zeros(shape, order="F")
+
+        self.flux = zeros(pp.flux_shape)
+        self.flux_cutoff = zeros(pp.flux_shape[1:]) if t["solver_type"] >= 2 else None
         self.rho = np.zeros(ng)
         self.group_iters = np.zeros(ng, dtype=np.int32)
         self.group_resid = np.zeros(ng)
@@ -228,6 +275,10 @@ def load_library(path: str | None = None):
                                      _ip, _dp]),
         "rb_set_launch_rules": (C.c_int32, [vp, C.POINTER(RbLaunchRule), C.c_int32]),
         "rb_deposition": (C.c_int32, [vp, C.c_int32, C.POINTER(h64), C.POINTER(_dp), _dp, C.c_double, _dp]),
+        "rb_host_alloc": (C.c_int32, [C.c_uint64, C.POINTER(vp)]),
+        "rb_host_free": (C.c_int32, [vp]),
+        "rb_host_register": (C.c_int32, [vp, C.c_uint64]),
+        "rb_host_unregister": (C.c_int32, [vp]),
         "rb_version": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
@@ -242,7 +293,8 @@ def load_library(path: str | None = None):
 EXPORTED_SYMBOLS = (
     "rb_create", "rb_destroy", "rb_last_error", "rb_upload", "rb_solve", "rb_solve_batch",
     "rb_download", "rb_release", "rb_required_bytes", "rb_compute_flux", "rb_submit", "rb_poll",
-    "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_set_launch_rules", "rb_version",
+    "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_set_launch_rules", "rb_host_alloc",
+    "rb_host_free", "rb_host_register", "rb_host_unregister", "rb_version",
 )
 
 
