@@ -253,6 +253,56 @@ typedef struct rb_launch_rule {
 } rb_launch_rule;
 RB_API int32_t rb_set_launch_rules(rb_context *ctx, const rb_launch_rule *rules, int32_t n);
 
+/* ---- fixed sources built on the device ------------------------------------------------- */
+/* A Volume_Source (src/structures/Volume_Source.jl) as volume_source() reads it
+ * (volume_source.jl:21-122): `intensity` in group `energy_group` on every voxel whose centre lies
+ * inside [lo, hi] on each axis of the geometry (bounds inclusive; axes beyond ndims unused). */
+typedef struct rb_volume_box {
+    int32_t energy_group;   /* 1-based */
+    int32_t reserved;       /* 0 */
+    double intensity;
+    double lo[3], hi[3];
+} rb_volume_box;
+
+/* A Surface_Source (src/structures/Surface_Source.jl) of an SN solve as surface_source() reads it
+ * (surface_source.jl:22-330): a beam of `intensity` in group `energy_group` through `face`
+ * (0..5 = X-, X+, Y-, Y+, Z-, Z+) with direction (mu, eta, xi), on the face cells whose centres lie
+ * inside [lo, hi] on the face's in-plane axes. `basis` holds the np_source values of the beam's
+ * half-range basis in the order of the surface moments: the shifted Legendre polynomials
+ * P_l(|mu|) (1D, Qdims 1: surface_source.jl:103) or the half-range real spherical harmonics at
+ * (|mu|, atan(xi, eta)) (surface_source.jl:137, :195, :284), zero beyond the source's own
+ * Legendre order. */
+typedef struct rb_surface_beam {
+    int32_t energy_group;   /* 1-based */
+    int32_t face;
+    double intensity;
+    double direction[3];
+    double lo[3], hi[3];
+    const double *basis;    /* [np_source] */
+} rb_surface_beam;
+
+/* The sources of one problem, added in this order as Source.add_source does
+ * (src/structures/Source.jl:129-203), and the voxel centres they are tested against
+ * (geometry.voxels_position, particle_transport/geometry.jl:68,147-148,252-254). */
+typedef struct rb_source_set {
+    const double *position[3];  /* [nx], [ny], [nz] voxel centres (axes beyond ndims NULL) */
+    int32_t nvolume;
+    int32_t nsurface;
+    const rb_volume_box *volume;
+    const rb_surface_beam *surface;
+} rb_source_set;
+
+/* rb_upload for a problem whose fixed sources come as definitions instead of dense arrays: the
+ * library builds the volume sources [ng, np, nm5, cells] and the per-face surface sources
+ * [ng, np_source, face cells] on the device (what volume_source / surface_source and
+ * Source.add_source build on the host), so only the definitions cross the host link.
+ * prob->volume_sources and prob->surface_sources must be NULL. norms (NULL allowed) receives the
+ * normalization factor of each source, volume boxes first, then beams, summed in the
+ * reference's order. No counterpart in the reference: it exists to take the dense source arrays
+ * off the host (the volume sources of a 64^3 S8 problem with 40 groups are 6.7 GB). */
+RB_API int32_t rb_upload_sources(rb_context *ctx, const rb_sn_problem *prob, const rb_source_set *src,
+                                 rb_handle *out, double *norms);
+
 /* ---- serving: continuous batching ---------------------------------------------------- */
 /* Admits a request (one particle solve) when its state fits the remaining HBM budget
  * (RB_ERR_BUDGET otherwise, nothing allocated). An admitted request is uploaded and launched at

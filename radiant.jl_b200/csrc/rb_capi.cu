@@ -63,6 +63,71 @@ __global__ void from_reference_layout(const double *__restrict__ src, double *__
     }
 }
 
+// ---- fixed sources built on the device (rb_upload_sources) -----------------------------------
+struct DevBeam {
+    int group, face;  // 0-based group; face 0..5
+    double intensity;
+    double dir[3], lo[3], hi[3];
+};
+
+// Volume_Source boxes into the group-major volume sources (zeroed before): angular moment 1,
+// cell moment 1 of every voxel whose centre lies inside a box gets the box's intensity, boxes
+// added in order (volume_source.jl:42-110 builds Q, Source.jl:129-133 adds it). pos holds the
+// voxel centres [nx | ny | nz].
+__global__ void assemble_volume(double *__restrict__ vol, long long nphi, long long npm, int nx, int ny, int nz,
+                                int ndims, const double *__restrict__ pos, const rb_volume_box *__restrict__ boxes,
+                                int nbox) {
+    const long long ncell = (long long)nx * ny * nz;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int ix = (int)(c % nx);
+        const long long r = c / nx;
+        const int iy = (int)(r % ny), iz = (int)(r / ny);
+        const double px = pos[ix], py = ndims >= 2 ? pos[nx + iy] : 0.0, pz = ndims >= 3 ? pos[nx + ny + iz] : 0.0;
+        for (int b = 0; b < nbox; b++) {
+            const rb_volume_box B = boxes[b];
+            bool in = B.lo[0] <= px && B.hi[0] >= px;
+            if (ndims >= 2) in = in && B.lo[1] <= py && B.hi[1] >= py;
+            if (ndims >= 3) in = in && B.lo[2] <= pz && B.hi[2] >= pz;
+            if (in) {
+                double *v = vol + (long long)(B.energy_group - 1) * nphi + npm * c;
+                *v = *v + B.intensity;
+            }
+        }
+    }
+}
+
+// Surface_Source beams of one face into its surface sources [ng, np_source, face cells] (zeroed
+// before): intensity · basis[p] · (face-cell widths, in-plane axes in increasing order) on the
+// face cells inside the aperture, when the beam enters through the face (surface_source.jl:
+// 89-96 in 1D, 158-187 in 2D, 216-275 in 3D), beams added in order (Source.jl:196-201). The
+// face cells are column-major over the in-plane axes a (fastest) and b.
+__global__ void assemble_surface(double *__restrict__ surf, int ng, int nps, int ndims, int face, int na, int nb,
+                                 const double *__restrict__ pos_a, const double *__restrict__ pos_b,
+                                 const double *__restrict__ d_a, const double *__restrict__ d_b, int ax_a, int ax_b,
+                                 const DevBeam *__restrict__ beams, const double *__restrict__ basis, int nbeam) {
+    const long long ncf = (long long)na * nb;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncf;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int ia = (int)(c % na), ib = (int)(c / na);
+        for (int b = 0; b < nbeam; b++) {
+            const DevBeam &B = beams[b];
+            if (B.face != face) continue;
+            const double cosv = B.dir[face / 2];
+            if (!((face % 2 == 0 && cosv > 0.0) || (face % 2 == 1 && cosv < 0.0))) continue;
+            if (ndims >= 2 && (pos_a[ia] < B.lo[ax_a] || pos_a[ia] > B.hi[ax_a])) continue;
+            if (ndims >= 3 && (pos_b[ib] < B.lo[ax_b] || pos_b[ib] > B.hi[ax_b])) continue;
+            for (int p = 0; p < nps; p++) {
+                double q = B.intensity * basis[(long long)b * nps + p];
+                if (ndims >= 2) q = q * d_a[ia];
+                if (ndims >= 3) q = q * d_b[ib];
+                double *v = surf + B.group + (long long)ng * (p + (long long)nps * c);
+                *v = __dadd_rn(*v, q);  // the beam's value rounded on its own, then added (no FMA)
+            }
+        }
+    }
+}
+
 // ---- coupled transport (rb_transport) ------------------------------------------------------
 // tot += gen over [ng][nphi]; for the entries of angular moment 1, cell moment 1 also the
 // largest |tot_new − tot_old| / max(|tot_new|, eps) (the reference's flux criterion,
@@ -876,8 +941,17 @@ ProblemRec *find(rb_context *ctx, rb_handle h) {
 
 // Lays one problem out in the device block `b` (offsets `o` from required()): fills the
 // device record `h`, queues the table copies on `s` and writes the record to *dptr.
+// Source definitions of rb_upload_sources and where their device copies sit in the block.
+struct SourceDefs {
+    const rb_source_set *src;
+    size_t off_pos, off_box, off_beam, off_basis;
+};
+
+int place_sources(rb_context *ctx, const rb_sn_problem *P, const Derived &D, const SourceDefs &S, char *b,
+                  cudaStream_t s, const DevProblem &h);
+
 int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, const size_t *o, char *b,
-                  cudaStream_t s, DevProblem &h, DevProblem **dptr, double *stage) {
+                  cudaStream_t s, DevProblem &h, DevProblem **dptr, double *stage, const SourceDefs *defs = nullptr) {
     memset(&h, 0, sizeof(h));
     const int nd = P->nd, np = P->np, nm5 = D.M.nm, ng = P->ng, nmat = P->nmat;
     h.ndims = P->ndims; h.nx = D.ns[0]; h.ny = D.ns[1]; h.nz = D.ns[2]; h.ncell = D.ncell;
@@ -955,7 +1029,9 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
         PUT(double, 24, P->e_width, ng);
     }
     if (P->t_mom) PUT(double, 23, P->t_mom, (size_t)ng * nmat);
-    if (P->volume_sources) {
+    if (defs) {
+        if ((r = place_sources(ctx, P, D, *defs, b, s, h)) != RB_OK) return r;
+    } else if (P->volume_sources) {
         // the volume sources arrive in the reference's layout [ng, np, nm5, cells] (group
         // fastest): copied to the staging buffer and turned group-major on the device
         CK(cudaMemcpyAsync(stage, P->volume_sources, sizeof(double) * (size_t)ng * D.nphi, cudaMemcpyHostToDevice, s));
@@ -966,12 +1042,205 @@ int place_problem(rb_context *ctx, const rb_sn_problem *P, const Derived &D, con
     PUT(float, 52, D.tc_m2d.data(), D.tc_m2d.size());
     PUT(float, 53, D.tc_d2m.data(), D.tc_d2m.size());
     for (int f = 0; f < 2 * P->ndims; f++)
-        if (P->surface_sources[f])
+        if (P->surface_sources[f] && !defs)
             PUT(double, 26 + f, P->surface_sources[f], (size_t)ng * P->np_source * face_cells(P->ndims, D.ns, f / 2));
 #undef PUT
     *dptr = DP(DevProblem, 0);
 #undef DP
     CK(cudaMemcpyAsync(*dptr, &h, sizeof(DevProblem), cudaMemcpyHostToDevice, s));
+    return RB_OK;
+}
+
+// The in-plane axes of a face (increasing order; -1 where the geometry has fewer axes).
+void face_axes(int ndims, int face, int &a, int &b) {
+    const int ax = face / 2;
+    int k = 0, o[2] = {-1, -1};
+    for (int d = 0; d < ndims; d++)
+        if (d != ax) o[k++] = d;
+    a = o[0];
+    b = o[1];
+}
+
+// Copies the definitions into the block and builds the volume and surface sources from them.
+int place_sources(rb_context *ctx, const rb_sn_problem *P, const Derived &D, const SourceDefs &S, char *b,
+                  cudaStream_t s, const DevProblem &h) {
+    const rb_source_set *src = S.src;
+    const int ndims = P->ndims, ng = P->ng, nps = P->np_source;
+    double *pos = reinterpret_cast<double *>(b + S.off_pos);
+    const long long na = D.ns[0], nb = D.ns[1], nc = D.ns[2];
+    CK(cudaMemcpyAsync(pos, src->position[0], sizeof(double) * na, cudaMemcpyHostToDevice, s));
+    if (ndims >= 2) CK(cudaMemcpyAsync(pos + na, src->position[1], sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+    if (ndims >= 3) CK(cudaMemcpyAsync(pos + na + nb, src->position[2], sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+    const int threads = 256;
+    auto blocks = [&](long long n) { return (unsigned)std::max<long long>(1, std::min<long long>((n + threads - 1) / threads, 4096)); };
+    if (h.vol) {
+        auto *boxes = reinterpret_cast<rb_volume_box *>(b + S.off_box);
+        CK(cudaMemcpyAsync(boxes, src->volume, sizeof(rb_volume_box) * src->nvolume, cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(const_cast<double *>(h.vol), 0, sizeof(double) * (size_t)ng * D.nphi, s));
+        rb::assemble_volume<<<blocks(D.ncell), threads, 0, s>>>(const_cast<double *>(h.vol), D.nphi,
+                                                                 (long long)P->np * D.M.nm, D.ns[0], D.ns[1], D.ns[2],
+                                                                 ndims, pos, boxes, src->nvolume);
+        CK(cudaGetLastError());
+    }
+    if (src->nsurface > 0) {
+        std::vector<rb::DevBeam> beams(src->nsurface);
+        std::vector<double> basis((size_t)src->nsurface * nps);
+        for (int k = 0; k < src->nsurface; k++) {
+            const rb_surface_beam &B = src->surface[k];
+            rb::DevBeam &d = beams[k];
+            d.group = B.energy_group - 1;
+            d.face = B.face;
+            d.intensity = B.intensity;
+            for (int a = 0; a < 3; a++) { d.dir[a] = B.direction[a]; d.lo[a] = B.lo[a]; d.hi[a] = B.hi[a]; }
+            for (int p = 0; p < nps; p++) basis[(size_t)k * nps + p] = B.basis[p];
+        }
+        auto *dbeams = reinterpret_cast<rb::DevBeam *>(b + S.off_beam);
+        auto *dbasis = reinterpret_cast<double *>(b + S.off_basis);
+        CK(cudaMemcpyAsync(dbeams, beams.data(), sizeof(rb::DevBeam) * beams.size(), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(dbasis, basis.data(), sizeof(double) * basis.size(), cudaMemcpyHostToDevice, s));
+        const double *widths[3] = {h.dx, h.dy, h.dz};
+        const long long off_axis[3] = {0, na, na + nb};
+        for (int f = 0; f < 2 * ndims; f++) {
+            if (!h.surf[f]) continue;
+            int a, c;
+            face_axes(ndims, f, a, c);
+            const int la = a >= 0 ? D.ns[a] : 1, lc = c >= 0 ? D.ns[c] : 1;
+            CK(cudaMemsetAsync(const_cast<double *>(h.surf[f]), 0, sizeof(double) * (size_t)ng * nps * la * lc, s));
+            rb::assemble_surface<<<blocks((long long)la * lc), threads, 0, s>>>(
+                const_cast<double *>(h.surf[f]), ng, nps, ndims, f, la, lc, a >= 0 ? pos + off_axis[a] : pos,
+                c >= 0 ? pos + off_axis[c] : pos, a >= 0 ? widths[a] : h.dx, c >= 0 ? widths[c] : h.dx,
+                a >= 0 ? a : 0, c >= 0 ? c : 0, dbeams, dbasis, src->nsurface);
+            CK(cudaGetLastError());
+        }
+    }
+    return RB_OK;
+}
+
+// Checks the definitions against the problem and writes each source's normalization factor:
+// volume_source.jl:42-110 (Σ intensity · voxel volume over the voxels inside, x outermost) and
+// surface_source.jl:89 (1D: the intensity), :158-187 (2D), :216-275 (3D: Σ intensity · face-cell
+// area over the face cells inside, the first in-plane axis outermost).
+int check_sources(rb_context *ctx, const rb_sn_problem *P, const rb_source_set *src, double *norms) {
+    if (P->volume_sources) return fail(ctx, RB_ERR_INVALID, "volume_sources must be NULL with source definitions");
+    for (int f = 0; f < 6; f++)
+        if (P->surface_sources[f]) return fail(ctx, RB_ERR_INVALID, "surface_sources must be NULL with source definitions");
+    if (src->nvolume < 0 || src->nsurface < 0 || (src->nvolume > 0 && !src->volume) || (src->nsurface > 0 && !src->surface))
+        return fail(ctx, RB_ERR_INVALID, "bad source counts or NULL source arrays");
+    const int ndims = P->ndims;
+    const int n[3] = {P->nx, ndims >= 2 ? P->ny : 1, ndims >= 3 ? P->nz : 1};
+    const double *w[3] = {P->dx, P->dy, P->dz};
+    for (int a = 0; a < ndims; a++)
+        if (!src->position[a]) return fail(ctx, RB_ERR_INVALID, "voxel positions of axis %d are NULL", a);
+    if (src->nsurface > 0 && (P->np_source < 1 || P->np_source > P->np_surf))
+        return fail(ctx, RB_ERR_INVALID, "np_source %d out of [1, np_surf=%d] with surface beams", P->np_source, P->np_surf);
+    for (int k = 0; k < src->nvolume; k++) {
+        const rb_volume_box &B = src->volume[k];
+        if (B.energy_group < 1 || B.energy_group > P->ng)
+            return fail(ctx, RB_ERR_INVALID, "volume source %d: energy group %d out of [1, %d]", k, B.energy_group, P->ng);
+        double norm = 0.0;
+        for (int ix = 0; ix < n[0]; ix++) {
+            const double x = src->position[0][ix];
+            if (!(B.lo[0] <= x && B.hi[0] >= x)) continue;
+            for (int iy = 0; iy < n[1]; iy++) {
+                if (ndims >= 2) { const double y = src->position[1][iy]; if (!(B.lo[1] <= y && B.hi[1] >= y)) continue; }
+                for (int iz = 0; iz < n[2]; iz++) {
+                    if (ndims >= 3) { const double z = src->position[2][iz]; if (!(B.lo[2] <= z && B.hi[2] >= z)) continue; }
+                    if (ndims == 1) norm = norm + B.intensity * w[0][ix];
+                    else if (ndims == 2) norm = norm + B.intensity * w[0][ix] * w[1][iy];
+                    else norm = norm + B.intensity * w[0][ix] * w[1][iy] * w[2][iz];
+                }
+            }
+        }
+        if (norms) norms[k] = norm;
+    }
+    for (int k = 0; k < src->nsurface; k++) {
+        const rb_surface_beam &B = src->surface[k];
+        if (B.energy_group < 1 || B.energy_group > P->ng)
+            return fail(ctx, RB_ERR_INVALID, "surface source %d: energy group %d out of [1, %d]", k, B.energy_group, P->ng);
+        if (B.face < 0 || B.face >= 2 * ndims)
+            return fail(ctx, RB_ERR_INVALID, "surface source %d: face %d out of [0, %d)", k, B.face, 2 * ndims);
+        if (!B.basis) return fail(ctx, RB_ERR_INVALID, "surface source %d: NULL basis", k);
+        double norm = 0.0;
+        if (ndims == 1) {
+            norm = B.intensity;
+        } else {
+            int a, c;
+            face_axes(ndims, B.face, a, c);
+            const int nc = c >= 0 ? n[c] : 1;
+            for (int ia = 0; ia < n[a]; ia++) {
+                const double pa = src->position[a][ia];
+                if (pa < B.lo[a] || pa > B.hi[a]) continue;
+                for (int ic = 0; ic < nc; ic++) {
+                    if (c < 0) { norm += B.intensity * w[a][ia]; continue; }
+                    const double pc = src->position[c][ic];
+                    if (pc < B.lo[c] || pc > B.hi[c]) continue;
+                    norm += B.intensity * w[a][ia] * w[c][ic];
+                }
+            }
+        }
+        if (norms) norms[src->nvolume + k] = norm;
+    }
+    return RB_OK;
+}
+
+const double k_built_on_device = 0.0;  // marks the source slots rb_upload_sources fills
+
+int upload_impl(rb_context *ctx, const rb_sn_problem *P0, const rb_source_set *src, rb_handle *out, double *norms) {
+    if (!ctx || !out) return fail(ctx, RB_ERR_INVALID, "null context or handle");
+    if (!P0) return fail(ctx, RB_ERR_INVALID, "null problem");
+    CK(cudaSetDevice(ctx->device));
+    rb_sn_problem Pm = *P0;
+    const rb_sn_problem *P = P0;
+    if (src) {
+        int st = check_sources(ctx, P0, src, norms);
+        if (st) return st;
+        if (src->nvolume > 0) Pm.volume_sources = &k_built_on_device;
+        for (int k = 0; k < src->nsurface; k++) Pm.surface_sources[src->surface[k].face] = &k_built_on_device;
+        P = &Pm;
+    }
+    Derived D;
+    int st = validate_and_derive(ctx, P, D);
+    if (st) return st;
+    Layout L;
+    size_t o[64];
+    required(P, D, L, o);
+    SourceDefs defs{};
+    if (src) {
+        defs.src = src;
+        defs.off_pos = L.take<double>((size_t)D.ns[0] + D.ns[1] + D.ns[2]);
+        defs.off_box = L.take<rb_volume_box>(src->nvolume);
+        defs.off_beam = L.take<rb::DevBeam>(src->nsurface);
+        defs.off_basis = L.take<double>((size_t)src->nsurface * P->np_source);
+    }
+    if (ctx->used + L.off > ctx->budget)
+        return fail(ctx, RB_ERR_BUDGET, "problem needs %zu bytes, %llu of %llu budget bytes in use", L.off,
+                    (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
+    if (P->volume_sources && !src) {  // staging for the volume sources' layout change
+        const size_t need = (size_t)P->ng * D.nphi;
+        if (need > ctx->stage_cap) {
+            if (ctx->d_stage) cudaFree(ctx->d_stage);
+            ctx->d_stage = nullptr;
+            ctx->stage_cap = 0;
+            CK(cudaMalloc(&ctx->d_stage, need * sizeof(double)));
+            ctx->stage_cap = need;
+        }
+    }
+    auto rec = std::make_unique<ProblemRec>();
+    CK(cudaMalloc(&rec->block, L.off));
+    rec->bytes = L.off;
+    cudaStream_t s = ctx->stream;
+    DevProblem &h = rec->h;
+    st = place_problem(ctx, P, D, o, rec->block, s, h, &rec->d, ctx->d_stage, src ? &defs : nullptr);
+    if (st) { cudaStreamSynchronize(s); cudaFree(rec->block); return st; }
+    rec->own_list = reinterpret_cast<DevProblem **>(rec->block + o[50]);
+    rec->own_queue = reinterpret_cast<int *>(rec->block + o[51]);
+    CK(cudaMemcpyAsync(rec->own_list, &rec->d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    rec->ng = P->ng; rec->np = P->np; rec->nm5 = D.M.nm; rec->csd = D.csd; rec->ncell = D.ncell; rec->nphi = D.nphi;
+    ctx->used += L.off;
+    rb_handle hd = ctx->next_handle++;
+    ctx->probs[hd] = std::move(rec);
+    *out = hd;
     return RB_OK;
 }
 
@@ -1046,44 +1315,13 @@ int32_t rb_required_bytes(const rb_sn_problem *prob, uint64_t *bytes) {
 }
 
 int32_t rb_upload(rb_context *ctx, const rb_sn_problem *P, rb_handle *out) {
-    if (!ctx || !out) return fail(ctx, RB_ERR_INVALID, "null context or handle");
-    CK(cudaSetDevice(ctx->device));
-    Derived D;
-    int st = validate_and_derive(ctx, P, D);
-    if (st) return st;
-    Layout L;
-    size_t o[64];
-    required(P, D, L, o);
-    if (ctx->used + L.off > ctx->budget)
-        return fail(ctx, RB_ERR_BUDGET, "problem needs %zu bytes, %llu of %llu budget bytes in use", L.off,
-                    (unsigned long long)ctx->used, (unsigned long long)ctx->budget);
-    if (P->volume_sources) {  // staging for the volume sources' layout change
-        const size_t need = (size_t)P->ng * D.nphi;
-        if (need > ctx->stage_cap) {
-            if (ctx->d_stage) cudaFree(ctx->d_stage);
-            ctx->d_stage = nullptr;
-            ctx->stage_cap = 0;
-            CK(cudaMalloc(&ctx->d_stage, need * sizeof(double)));
-            ctx->stage_cap = need;
-        }
-    }
-    auto rec = std::make_unique<ProblemRec>();
-    CK(cudaMalloc(&rec->block, L.off));
-    rec->bytes = L.off;
-    cudaStream_t s = ctx->stream;
-    DevProblem &h = rec->h;
-    st = place_problem(ctx, P, D, o, rec->block, s, h, &rec->d, ctx->d_stage);
-    if (st) { cudaFree(rec->block); return st; }
-    rec->own_list = reinterpret_cast<DevProblem **>(rec->block + o[50]);
-    rec->own_queue = reinterpret_cast<int *>(rec->block + o[51]);
-    CK(cudaMemcpyAsync(rec->own_list, &rec->d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
-    CK(cudaStreamSynchronize(s));
-    rec->ng = P->ng; rec->np = P->np; rec->nm5 = D.M.nm; rec->csd = D.csd; rec->ncell = D.ncell; rec->nphi = D.nphi;
-    ctx->used += L.off;
-    rb_handle hd = ctx->next_handle++;
-    ctx->probs[hd] = std::move(rec);
-    *out = hd;
-    return RB_OK;
+    return upload_impl(ctx, P, nullptr, out, nullptr);
+}
+
+int32_t rb_upload_sources(rb_context *ctx, const rb_sn_problem *P, const rb_source_set *src, rb_handle *out,
+                          double *norms) {
+    if (!src) return fail(ctx, RB_ERR_INVALID, "null source set");
+    return upload_impl(ctx, P, src, out, norms);
 }
 
 int32_t rb_solve(rb_context *ctx, rb_handle hd, void *stream) {

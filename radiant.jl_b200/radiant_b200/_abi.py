@@ -275,6 +275,7 @@ def load_library(path: str | None = None):
                                      _ip, _dp]),
         "rb_set_launch_rules": (C.c_int32, [vp, C.POINTER(RbLaunchRule), C.c_int32]),
         "rb_deposition": (C.c_int32, [vp, C.c_int32, C.POINTER(h64), C.POINTER(_dp), _dp, C.c_double, _dp]),
+        "rb_upload_sources": (C.c_int32, [vp, PP, vp, C.POINTER(h64), _dp]),
         "rb_host_alloc": (C.c_int32, [C.c_uint64, C.POINTER(vp)]),
         "rb_host_free": (C.c_int32, [vp]),
         "rb_host_register": (C.c_int32, [vp, C.c_uint64]),
@@ -293,8 +294,8 @@ def load_library(path: str | None = None):
 EXPORTED_SYMBOLS = (
     "rb_create", "rb_destroy", "rb_last_error", "rb_upload", "rb_solve", "rb_solve_batch",
     "rb_download", "rb_release", "rb_required_bytes", "rb_compute_flux", "rb_submit", "rb_poll",
-    "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_set_launch_rules", "rb_host_alloc",
-    "rb_host_free", "rb_host_register", "rb_host_unregister", "rb_version",
+    "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_set_launch_rules", "rb_upload_sources",
+    "rb_host_alloc", "rb_host_free", "rb_host_register", "rb_host_unregister", "rb_version",
 )
 
 
@@ -360,6 +361,17 @@ class Context:
         self.check(self.lib.rb_upload(self.h, C.byref(pp.P), C.byref(h)))
         self._ncell[h.value] = int(np.prod(pp.tables["ns"]))
         return h.value
+
+    def upload_sources(self, pp: PackedProblem, sources) -> tuple:
+        """rb_upload_sources: the problem with its fixed sources built on the device from
+        `sources` (a sources.SourceSet); returns (handle, normalization factors)."""
+        h = C.c_int64()
+        n = int(sources.S.nvolume + sources.S.nsurface)
+        norms = np.zeros(max(n, 1))
+        self.check(self.lib.rb_upload_sources(self.h, C.byref(pp.P), C.cast(C.pointer(sources.S), C.c_void_p),
+                                              C.byref(h), norms.ctypes.data_as(_dp)))
+        self._ncell[h.value] = int(np.prod(pp.tables["ns"]))
+        return h.value, norms[:n]
 
     def solve(self, h: int, stream=None):
         self.check(self.lib.rb_solve(self.h, h, C.c_void_p(stream) if stream else None))

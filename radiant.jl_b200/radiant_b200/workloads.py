@@ -15,6 +15,7 @@ import math
 
 import numpy as np
 
+from . import sources as S
 from . import tables as T
 from .sn_flux import MultigroupXS, SNSettings, prepare_sn_tables
 
@@ -172,44 +173,19 @@ def random_slab_tables(seed: int, precision: str = "fp64", max_cells: int = 2000
                        precision=precision, xs=xs)
 
 
-def surface_source_md(ndims, ns, ds, positions, Om, w, L: int, btype: str, Qdims: int, ng: int, group: int,
-                      face: str, direction, aperture=None, intensity: float = 1.0):
-    """Moments of a monodirectional beam through one face of a 2D/3D grid (surface_source.jl:
-    129-188 for 2D, :189-276 for 3D): the half-range moments times the face-cell area, inside
-    the aperture ({axis: (lo, hi)}, voxel midpoints compared as the reference does).
-    Returns per-face arrays [ng, Np, face cells] (None for the other faces)."""
-    from .sphere import surface_source_moments
-
-    q, pl, pm = surface_source_moments(Om, w, L, btype, Qdims, face, direction, intensity)
-    Np = len(q)
-    axis = "XYZ".index(face[0])
-    others = [a for a in range(ndims) if a != axis]
-    shape = [ns[a] for a in others]
-    arr = np.zeros((ng, Np, int(np.prod(shape))))
-    mus, etas, xis = direction
-    cosv = [mus, etas, xis][axis]
-    ok_dir = (face[1] == "-" and cosv > 0) or (face[1] == "+" and cosv < 0)
-    if ok_dir:
-        idx = np.ndindex(*shape)
-        for k, cell in enumerate(np.ndindex(*shape[::-1])):
-            cell = cell[::-1]
-            inside, area = True, 1.0
-            for j, a in enumerate(others):
-                pos = positions[a][cell[j]]
-                if aperture and a in aperture and not (aperture[a][0] <= pos <= aperture[a][1]):
-                    inside = False
-                area *= ds[a][cell[j]]
-            if inside:
-                flat = 0
-                stride = 1
-                for j in range(len(shape)):
-                    flat += cell[j] * stride
-                    stride *= shape[j]
-                arr[group, :, flat] = q * area
-        del idx
-    faces = [None] * (2 * ndims)
-    faces["XYZ".index(face[0]) * 2 + (0 if face[1] == "-" else 1)] = arr
-    return faces
+def grid_source_definitions(ndims, beam=None, volume=None) -> dict:
+    """The Volume_Source / Surface_Source definitions of grid_tables' `beam` = (face, group,
+    direction, aperture) and `volume` = (group, {axis: (lo, hi)}) (0-based groups and axes):
+    unit intensity, the beam's Legendre order the reference's default (64)."""
+    out = {"volume": [], "surface": []}
+    if volume is not None:
+        group, box = volume
+        out["volume"].append(S.VolumeSource(group + 1, {"xyz"[a]: tuple(v) for a, v in box.items()}))
+    if beam is not None:
+        face, group, direction, aperture = beam
+        out["surface"].append(S.SurfaceSource(group + 1, face, tuple(direction),
+                                              {"xyz"[a]: tuple(v) for a, v in (aperture or {}).items()}))
+    return out
 
 
 def grid_tables(ndims, ns, widths, mats, ng, nmat, seed, sn: SNSettings, L_xs: int, beam=None, volume=None,
@@ -220,23 +196,9 @@ def grid_tables(ndims, ns, widths, mats, ng, nmat, seed, sn: SNSettings, L_xs: i
     xs = xs or synthetic_xs(ng, nmat, L_xs, seed, csd=csd)
     ns = list(ns)
     ds = [np.asarray(wd, dtype=float) for wd in widths]
-    positions = [np.cumsum(d) - d / 2 for d in ds]
-    Qdims = sn.qdims(ndims)
-    Om, w = T.quadrature(sn.quadrature_order, sn.quadrature_type, ndims, Qdims)
-    surf = None
-    if beam is not None:
-        face, group, direction, aperture = beam
-        surf = surface_source_md(ndims, ns, ds, positions, Om, w, min(64, sn.legendre_order), sn.angular_boltzmann,
-                                 Qdims, ng, group, face, direction, aperture)
-    vol = None
-    if volume is not None:
-        group, box = volume
-        full = ns + [1] * (3 - ndims)
-        vol = np.zeros((ng, 1, 1, *full))
-        for idx in np.ndindex(*ns):
-            inside = all(box[a][0] <= positions[a][idx[a]] <= box[a][1] for a in range(ndims) if a in box)
-            if inside:
-                vol[(group, 0, 0) + tuple(idx) + (0,) * (3 - ndims)] = 1.0
+    defs = grid_source_definitions(ndims, beam, volume)
+    positions = [S.positions_of(d) for d in ds]
+    vol, surf, _ = S.dense_sources(sn, ndims, ng, ns, ds, positions, defs["volume"], defs["surface"])
     full = ns + [1] * (3 - ndims)
     tabs = prepare_sn_tables(xs, ndims, ns, ds, np.asarray(mats).reshape(full, order="F"), list(bc), sn,
                              volume_sources=vol, surface_sources=surf, precision=precision)
