@@ -14,8 +14,8 @@ shapes (the reference's physics generator is not available here).
 
   value  updates/s of the step, inputs resident in HBM
   e2e    the same through the C ABI with page-locked host buffers: upload (H2D) + solve +
-         download (D2H) of every problem per step, the next problem's upload overlapping the
-         current solve
+         download (D2H) of every problem per step, the next problem's upload and the previous
+         problem's download overlapping the current solve
   unit   of work: one (cell, direction) visit inside one transport pass of one group;
          updates = sum of passes x cells x directions, passes as the reference counts them.
 
@@ -28,6 +28,7 @@ is not installed) on all host cores over a bounded sample of the same 3D workloa
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -282,17 +283,25 @@ def run_ours(args, rank, world):
               for rb in rbs)
     e2e_steps = max(5, args.steps)
 
-    def e2e_step():
+    def pipelined(upload):
         # problem k+1's tables cross the host link while problem k solves (rb_upload's copies run
-        # on the context's stream, the solve on sptr); problem k's results come back before
-        # problem k+1 is launched, since the layout change of the download needs the SMs
-        hs = [ctx.upload(packs[0])]
+        # on the context's stream, the solve on sptr); problem k's results cross back while
+        # problem k+1 solves (rb_download_async queues the layout change right behind solve k
+        # and the copies on the context's copy stream)
+        hs = [upload(0)]
         for k in range(len(packs)):
             ctx.solve(hs[k], sptr)
             if k + 1 < len(packs):
-                hs.append(ctx.upload(packs[k + 1]))
-            ctx.download(hs[k], rbs[k])
-            ctx.release(hs[k])
+                hs.append(upload(k + 1))
+            if k > 0:
+                ctx.download_wait(hs[k - 1])
+                ctx.release(hs[k - 1])
+            ctx.download_async(hs[k], rbs[k])
+        ctx.download_wait(hs[-1])
+        ctx.release(hs[-1])
+
+    def e2e_step():
+        pipelined(lambda k: ctx.upload(packs[k]))
 
     e2e_step()
     torch.cuda.synchronize()
@@ -303,6 +312,36 @@ def run_ours(args, rank, world):
         e2e_step()
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, world)
+
+    # the same e2e step with the fixed sources as definitions (rb_upload_sources): the volume
+    # sources are built on the device instead of crossing the host link as dense arrays
+    e2e_src = None
+    if all("sources" in t for t in tabs):
+        from radiant_b200.workloads import without_dense_sources
+
+        bare = [without_dense_sources(t) for t in tabs]
+        bpacks = [PackedProblem(b, pinned=True) for b, _ in bare]
+        ssets = [ss for _, ss in bare]
+        h2d_src = sum(p_bytes(b) for b, _ in bare) + sum(
+            sum(p.nbytes for p in ss.positions) + C.sizeof(ss.boxes) + C.sizeof(ss.beams) + sum(b.nbytes for b in ss.bases)
+            for ss in ssets)
+
+        def e2e_src_step():
+            pipelined(lambda k: ctx.upload_sources(bpacks[k], ssets[k])[0])
+
+        e2e_src_step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_src_step()
+        torch.cuda.synchronize()
+        src_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, world)
+        e2e_src = {"value": updates * world / (src_ms / 1e3), "unit": "updates/s", "h2d_bytes_per_step": h2d_src,
+                   "d2h_bytes_per_step": d2h, "ms_per_step": src_ms, "steps": e2e_steps,
+                   "entry": "rb_upload_sources (Volume_Source / Surface_Source definitions, arrays built on the device)"}
+        del bpacks
 
     c2 = run_c2_section(args, ctx, sptr, stream, rank, world) if args.workload == "c4" and not args.no_c2 else None
     serving = run_serving(args, ctx, dev) if (args.serve > 0 and rank == 0) else None
@@ -335,6 +374,7 @@ def run_ours(args, rank, world):
                      "kernel": kernel_name(args.workload)},
         "e2e": {"value": updates * world / (e2e_ms / 1e3), "unit": "updates/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "steps": e2e_steps},
+        "e2e_source_definitions": e2e_src,
         "updates_per_step": updates,
         "gpu_launches": args.steps * (len(tabs) if args.workload in ("c4", "c4g1") else 1),
         "clocks": clk.summary(),

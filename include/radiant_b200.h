@@ -172,6 +172,15 @@ RB_API int32_t rb_solve(rb_context *ctx, rb_handle h, void *stream);
 RB_API int32_t rb_solve_batch(rb_context *ctx, const rb_handle *hs, int32_t n, void *stream);
 /* Waits for the problem's stream and copies the results into caller-owned host buffers. */
 RB_API int32_t rb_download(rb_context *ctx, rb_handle h, rb_sn_result *res);
+/* rb_download in two halves, for a caller that launches more work meanwhile: rb_download_async
+ * queues the layout change of the flux on the problem's solve stream (right behind the solve,
+ * before anything launched there later) and the copies on a copy stream of the context, and
+ * returns; rb_download_wait waits for them and reports the solve's status. `res` and its buffers
+ * must stay alive until the wait (page-locked buffers let the copies overlap later solves). The
+ * context holds one staging buffer for these downloads: a second rb_download_async first waits
+ * for the copies of the one before. */
+RB_API int32_t rb_download_async(rb_context *ctx, rb_handle h, rb_sn_result *res);
+RB_API int32_t rb_download_wait(rb_context *ctx, rb_handle h);
 RB_API int32_t rb_release(rb_context *ctx, rb_handle h);
 /* Bytes of device memory rb_upload would reserve for `prob` (admission control). */
 RB_API int32_t rb_required_bytes(const rb_sn_problem *prob, uint64_t *bytes);

@@ -253,7 +253,12 @@ struct ProblemRec {
     int ng = 0, np = 0, nm5 = 0, csd = 0;
     long long ncell = 0, nphi = 0;
     cudaStream_t stream = nullptr;  // stream of the last solve
+    cudaEvent_t solve_done = nullptr;  // recorded behind the last solve on `stream`
     bool solved = false;
+    // rb_download_async: copies in flight into `dl_res`, pass count and status into `dl_small`
+    bool dl_pending = false;
+    rb_sn_result *dl_res = nullptr;
+    long long *dl_small = nullptr;  // page-locked [passes, status]
 };
 
 }  // namespace
@@ -282,6 +287,12 @@ struct rb_context {
     size_t next_stream = 0;
     // measured launch rules (rb_set_launch_rules): team size by problem class
     std::vector<rb_launch_rule> rules;
+    // rb_download_async: its own staging buffer, copy stream and events
+    double *d_dstage = nullptr;
+    size_t dstage_cap = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t dl_ready = nullptr, dl_done = nullptr;
+    bool dl_busy = false;
 };
 
 namespace {
@@ -930,7 +941,12 @@ int launch(rb_context *ctx, const std::vector<ProblemRec *> &recs, cudaStream_t 
         int st3 = launch_grid(ctx, r->d, r->h, s);
         if (st3) return st3;
     }
-    for (auto *r : recs) { r->stream = s; r->solved = true; }
+    for (auto *r : recs) {
+        if (!r->solve_done) CK(cudaEventCreateWithFlags(&r->solve_done, cudaEventDisableTiming));
+        CK(cudaEventRecord(r->solve_done, s));
+        r->stream = s;
+        r->solved = true;
+    }
     return RB_OK;
 }
 
@@ -1226,12 +1242,15 @@ int upload_impl(rb_context *ctx, const rb_sn_problem *P0, const rb_source_set *s
         }
     }
     auto rec = std::make_unique<ProblemRec>();
-    CK(cudaMalloc(&rec->block, L.off));
-    rec->bytes = L.off;
     cudaStream_t s = ctx->stream;
+    // stream-ordered allocation from the device's pool: unlike cudaMalloc / cudaFree it does not
+    // wait for kernels running on other streams, so an upload overlaps a solve in flight and a
+    // release does not stall the requests still running
+    CK(cudaMallocAsync(&rec->block, L.off, s));
+    rec->bytes = L.off;
     DevProblem &h = rec->h;
     st = place_problem(ctx, P, D, o, rec->block, s, h, &rec->d, ctx->d_stage, src ? &defs : nullptr);
-    if (st) { cudaStreamSynchronize(s); cudaFree(rec->block); return st; }
+    if (st) { cudaStreamSynchronize(s); cudaFreeAsync(rec->block, s); cudaStreamSynchronize(s); return st; }
     rec->own_list = reinterpret_cast<DevProblem **>(rec->block + o[50]);
     rec->own_queue = reinterpret_cast<int *>(rec->block + o[51]);
     CK(cudaMemcpyAsync(rec->own_list, &rec->d, sizeof(DevProblem *), cudaMemcpyHostToDevice, s));
@@ -1274,6 +1293,13 @@ int32_t rb_create(int32_t device, uint64_t hbm_budget_bytes, rb_context **out) {
     if (const char *lo = getenv("RB_LOCAL1D")) c->local1d = atoi(lo) != 0;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete c; return fail(nullptr, RB_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
+    // problem blocks come from the device's default pool (cudaMallocAsync); the pool keeps what
+    // is freed for the next upload instead of unmapping it at every synchronisation
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     *out = c;
     return RB_OK;
 }
@@ -1282,13 +1308,22 @@ int32_t rb_destroy(rb_context *ctx) {
     if (!ctx) return RB_ERR_INVALID;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
-    for (auto &kv : ctx->probs) cudaFree(kv.second->block);
+    for (auto &kv : ctx->probs) {
+        cudaFreeAsync(kv.second->block, ctx->stream);
+        if (kv.second->solve_done) cudaEventDestroy(kv.second->solve_done);
+        if (kv.second->dl_small) cudaFreeHost(kv.second->dl_small);
+    }
     ctx->probs.clear();
+    cudaStreamSynchronize(ctx->stream);
     if (ctx->d_list) cudaFree(ctx->d_list);
     if (ctx->d_queue) cudaFree(ctx->d_queue);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
     if (ctx->d_gpart) cudaFree(ctx->d_gpart);
     for (auto ss : ctx->serve_streams) cudaStreamDestroy(ss);
+    if (ctx->d_dstage) cudaFree(ctx->d_dstage);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->dl_ready) cudaEventDestroy(ctx->dl_ready);
+    if (ctx->dl_done) cudaEventDestroy(ctx->dl_done);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return RB_OK;
@@ -1379,12 +1414,87 @@ int32_t rb_download(rb_context *ctx, rb_handle hd, rb_sn_result *res) {
     return RB_OK;
 }
 
+int32_t rb_download_async(rb_context *ctx, rb_handle hd, rb_sn_result *res) {
+    if (!ctx || !res) return fail(ctx, RB_ERR_INVALID, "null context or result");
+    CK(cudaSetDevice(ctx->device));
+    ProblemRec *r = find(ctx, hd);
+    if (!r) return fail(ctx, RB_ERR_NOT_FOUND, "unknown problem handle %lld", (long long)hd);
+    if (!r->solved) return fail(ctx, RB_ERR_INVALID, "problem %lld was not solved", (long long)hd);
+    if (r->dl_pending) return fail(ctx, RB_ERR_INVALID, "problem %lld already has a download in flight", (long long)hd);
+    if (!ctx->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->dl_ready, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->dl_done, cudaEventDisableTiming));
+    }
+    // one staging buffer per context: the copies of the previous download must be done with it
+    if (ctx->dl_busy) CK(cudaEventSynchronize(ctx->dl_done));
+    const size_t need = (size_t)r->ng * r->nphi;
+    if (res->flux && need > ctx->dstage_cap) {
+        if (ctx->d_dstage) cudaFree(ctx->d_dstage);
+        ctx->d_dstage = nullptr;
+        ctx->dstage_cap = 0;
+        CK(cudaMalloc(&ctx->d_dstage, need * sizeof(double)));
+        ctx->dstage_cap = need;
+    }
+    if (!r->dl_small) CK(cudaHostAlloc(&r->dl_small, 2 * sizeof(long long), cudaHostAllocPortable));
+    cudaStream_t s = r->stream, c = ctx->copy_stream;
+    const DevProblem &h = r->h;
+    // the layout change runs on the solve's stream, right behind the solve (before whatever is
+    // launched there next); the copies wait for it on the copy stream and overlap later work
+    if (res->flux) {
+        dim3 blk(32, 8), grd((unsigned)((r->nphi + 31) / 32), (unsigned)((r->ng + 31) / 32));
+        rb::to_reference_layout<<<grd, blk, 0, s>>>(h.flux, ctx->d_dstage, r->ng, r->nphi);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(ctx->dl_ready, s));
+    CK(cudaStreamWaitEvent(c, ctx->dl_ready, 0));
+    if (res->flux) CK(cudaMemcpyAsync(res->flux, ctx->d_dstage, need * sizeof(double), cudaMemcpyDeviceToHost, c));
+    if (res->flux_cutoff && r->csd)
+        CK(cudaMemcpyAsync(res->flux_cutoff, h.cutoff, r->nphi * sizeof(double), cudaMemcpyDeviceToHost, c));
+    if (res->rho) CK(cudaMemcpyAsync(res->rho, h.rho, r->ng * sizeof(double), cudaMemcpyDeviceToHost, c));
+    if (res->group_resid) CK(cudaMemcpyAsync(res->group_resid, h.resid, r->ng * sizeof(double), cudaMemcpyDeviceToHost, c));
+    if (res->group_iters) CK(cudaMemcpyAsync(res->group_iters, h.iters, r->ng * sizeof(int), cudaMemcpyDeviceToHost, c));
+    if (res->group_converged) CK(cudaMemcpyAsync(res->group_converged, h.conv, r->ng * sizeof(int), cudaMemcpyDeviceToHost, c));
+    r->dl_small[1] = 0;
+    CK(cudaMemcpyAsync(&r->dl_small[0], h.passes, sizeof(long long), cudaMemcpyDeviceToHost, c));
+    CK(cudaMemcpyAsync(&r->dl_small[1], h.status, sizeof(int), cudaMemcpyDeviceToHost, c));
+    CK(cudaEventRecord(ctx->dl_done, c));
+    ctx->dl_busy = true;
+    r->dl_pending = true;
+    r->dl_res = res;
+    return RB_OK;
+}
+
+int32_t rb_download_wait(rb_context *ctx, rb_handle hd) {
+    if (!ctx) return RB_ERR_INVALID;
+    CK(cudaSetDevice(ctx->device));
+    ProblemRec *r = find(ctx, hd);
+    if (!r) return fail(ctx, RB_ERR_NOT_FOUND, "unknown problem handle %lld", (long long)hd);
+    if (!r->dl_pending) return fail(ctx, RB_ERR_INVALID, "problem %lld has no download in flight", (long long)hd);
+    // the copy stream runs in order: the last download's event covers every earlier one
+    CK(cudaEventSynchronize(ctx->dl_done));
+    r->dl_pending = false;
+    r->dl_res->passes = r->dl_small[0];
+    const int status = (int)r->dl_small[1];
+    if (status & RB_DEV_TIMEOUT) return fail(ctx, RB_ERR_TIMEOUT, "a device wait gave up");
+    if (status & RB_DEV_BAD_TABLE) return fail(ctx, RB_ERR_INVALID, "singular cell system or bad table");
+    return RB_OK;
+}
+
 int32_t rb_release(rb_context *ctx, rb_handle hd) {
     if (!ctx) return RB_ERR_INVALID;
     auto it = ctx->probs.find(hd);
     if (it == ctx->probs.end()) return fail(ctx, RB_ERR_NOT_FOUND, "unknown problem handle %lld", (long long)hd);
-    if (it->second->stream) cudaStreamSynchronize(it->second->stream);
-    cudaFree(it->second->block);
+    // wait for this problem's own work only (later launches on the same stream may still run)
+    if (it->second->done) cudaEventSynchronize(it->second->done);
+    else if (it->second->solve_done) cudaEventSynchronize(it->second->solve_done);
+    else if (it->second->stream) cudaStreamSynchronize(it->second->stream);
+    if (it->second->solve_done) cudaEventDestroy(it->second->solve_done);
+    if (it->second->dl_pending && ctx->dl_done) cudaEventSynchronize(ctx->dl_done);
+    if (it->second->dl_small) cudaFreeHost(it->second->dl_small);
+    // the problem's stream is idle (synchronised above): the block goes back to the pool in the
+    // context stream's order, without waiting for other streams' work
+    cudaFreeAsync(it->second->block, ctx->stream);
     ctx->used -= it->second->bytes;
     ctx->probs.erase(it);
     return RB_OK;

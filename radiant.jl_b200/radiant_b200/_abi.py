@@ -264,6 +264,8 @@ def load_library(path: str | None = None):
         "rb_solve_batch": (C.c_int32, [vp, C.POINTER(h64), C.c_int32, vp]),
         "rb_download": (C.c_int32, [vp, h64, RP]),
         "rb_release": (C.c_int32, [vp, h64]),
+        "rb_download_async": (C.c_int32, [vp, h64, RP]),
+        "rb_download_wait": (C.c_int32, [vp, h64]),
         "rb_required_bytes": (C.c_int32, [PP, C.POINTER(C.c_uint64)]),
         "rb_compute_flux": (C.c_int32, [C.c_int32, PP, RP]),
         "rb_submit": (C.c_int32, [vp, PP, C.POINTER(h64)]),
@@ -292,10 +294,11 @@ def load_library(path: str | None = None):
 
 
 EXPORTED_SYMBOLS = (
-    "rb_create", "rb_destroy", "rb_last_error", "rb_upload", "rb_solve", "rb_solve_batch",
-    "rb_download", "rb_release", "rb_required_bytes", "rb_compute_flux", "rb_submit", "rb_poll",
-    "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_set_launch_rules", "rb_upload_sources",
-    "rb_host_alloc", "rb_host_free", "rb_host_register", "rb_host_unregister", "rb_version",
+    "rb_create", "rb_destroy", "rb_last_error", "rb_upload", "rb_solve", "rb_solve_batch", "rb_download",
+    "rb_download_async", "rb_download_wait", "rb_release", "rb_required_bytes", "rb_compute_flux",
+    "rb_submit", "rb_poll", "rb_energy_deposition", "rb_transport", "rb_deposition", "rb_set_launch_rules",
+    "rb_upload_sources", "rb_host_alloc", "rb_host_free", "rb_host_register", "rb_host_unregister",
+    "rb_version",
 )
 
 
@@ -382,6 +385,13 @@ class Context:
 
     def download(self, h: int, rb: ResultBuffers):
         self.check(self.lib.rb_download(self.h, h, C.byref(rb.R)))
+
+    def download_async(self, h: int, rb: ResultBuffers):
+        """rb_download_async: the copies are queued; `rb` must stay alive until download_wait."""
+        self.check(self.lib.rb_download_async(self.h, h, C.byref(rb.R)))
+
+    def download_wait(self, h: int):
+        self.check(self.lib.rb_download_wait(self.h, h))
 
     def release(self, h: int):
         self.check(self.lib.rb_release(self.h, h))

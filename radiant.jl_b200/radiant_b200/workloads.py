@@ -203,7 +203,21 @@ def grid_tables(ndims, ns, widths, mats, ng, nmat, seed, sn: SNSettings, L_xs: i
     tabs = prepare_sn_tables(xs, ndims, ns, ds, np.asarray(mats).reshape(full, order="F"), list(bc), sn,
                              volume_sources=vol, surface_sources=surf, precision=precision)
     tabs["xs"] = xs
+    tabs["sources"] = dict(defs, positions=positions, sn=sn)  # the definitions behind vol / surf
     return tabs
+
+
+def without_dense_sources(tabs: dict):
+    """(tables with no dense source arrays, sources.SourceSet of their definitions): the problem as
+    rb_upload_sources takes it."""
+    src = tabs["sources"]
+    sset = S.SourceSet(src["sn"], tabs["ndims"], src["positions"], src["volume"], src["surface"],
+                       np_surf=tabs["np_surf"])
+    bare = dict(tabs)
+    bare["volume_sources"] = None
+    bare["surface_sources"] = [None] * 6
+    bare["np_source"] = sset.np_source
+    return bare, sset
 
 
 def c3_tables(seed: int = 1, particle: str = "photon", precision: str = "fp64", n: int = 128, ng: int = 60,

@@ -89,3 +89,39 @@ def test_pinned_empty_lifetime():
     v = a[1]
     del a
     assert float(v.sum()) == 1.5 * 35  # the view keeps the page-locked block alive
+
+
+def test_download_async_overlaps_the_next_solve():
+    """rb_download_async of one problem while the next one solves gives the bits of rb_download,
+    for both problems; a wait with nothing in flight and a second async download of the same
+    problem are refused."""
+    tabs = [W.c4_tables(seed=3, particle="photon", n=16, ng=2), W.c4_tables(seed=3, particle="electron", n=16, ng=2)]
+    ctx = Context(0, 0)
+    try:
+        refs = [_solve(ctx, PackedProblem(t), ResultBuffers(PackedProblem(t))) for t in tabs]
+        packs = [PackedProblem(t, pinned=True) for t in tabs]
+        rbs = [ResultBuffers(p, pinned=True) for p in packs]
+        hs = [ctx.upload(packs[0])]
+        ctx.solve(hs[0])
+        hs.append(ctx.upload(packs[1]))
+        ctx.download_async(hs[0], rbs[0])
+        with pytest.raises(_abi.RadiantError) as ei:
+            ctx.download_async(hs[0], rbs[0])
+        assert ei.value.status == RB_ERR_INVALID
+        ctx.solve(hs[1])
+        ctx.download_wait(hs[0])
+        with pytest.raises(_abi.RadiantError) as ei:
+            ctx.download_wait(hs[0])
+        assert ei.value.status == RB_ERR_INVALID
+        ctx.download_async(hs[1], rbs[1])
+        ctx.download_wait(hs[1])
+        for h in hs:
+            ctx.release(h)
+        for got, ref in zip(rbs, refs):
+            assert np.array_equal(got.flux, ref.flux) and got.passes == ref.passes
+            assert (got.flux_cutoff is None) == (ref.flux_cutoff is None)
+            if ref.flux_cutoff is not None:
+                assert np.array_equal(got.flux_cutoff, ref.flux_cutoff)
+            assert np.array_equal(got.group_iters, ref.group_iters) and np.array_equal(got.rho, ref.rho)
+    finally:
+        ctx.close()
