@@ -255,10 +255,12 @@ struct ProblemRec {
     cudaStream_t stream = nullptr;  // stream of the last solve
     cudaEvent_t solve_done = nullptr;  // recorded behind the last solve on `stream`
     bool solved = false;
-    // rb_download_async: copies in flight into `dl_res`, pass count and status into `dl_small`
+    // rb_download_async: copies in flight into `dl_res` (flux, cutoff) and into `dl_small`, a
+    // page-locked buffer from the context's list: [passes, status, rho, resid, iters, conv]
     bool dl_pending = false;
     rb_sn_result *dl_res = nullptr;
-    long long *dl_small = nullptr;  // page-locked [passes, status]
+    char *dl_small = nullptr;
+    size_t dl_small_cap = 0;
 };
 
 }  // namespace
@@ -293,6 +295,10 @@ struct rb_context {
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t dl_ready = nullptr, dl_done = nullptr;
     bool dl_busy = false;
+    // page-locked small buffers of the async downloads, reused (cudaFreeHost would wait for the
+    // whole device, so they are given back only by rb_destroy)
+    std::vector<std::pair<char *, size_t>> small_free;
+    std::vector<char *> small_all;
 };
 
 namespace {
@@ -1311,8 +1317,8 @@ int32_t rb_destroy(rb_context *ctx) {
     for (auto &kv : ctx->probs) {
         cudaFreeAsync(kv.second->block, ctx->stream);
         if (kv.second->solve_done) cudaEventDestroy(kv.second->solve_done);
-        if (kv.second->dl_small) cudaFreeHost(kv.second->dl_small);
     }
+    for (char *p : ctx->small_all) cudaFreeHost(p);
     ctx->probs.clear();
     cudaStreamSynchronize(ctx->stream);
     if (ctx->d_list) cudaFree(ctx->d_list);
@@ -1436,7 +1442,25 @@ int32_t rb_download_async(rb_context *ctx, rb_handle hd, rb_sn_result *res) {
         CK(cudaMalloc(&ctx->d_dstage, need * sizeof(double)));
         ctx->dstage_cap = need;
     }
-    if (!r->dl_small) CK(cudaHostAlloc(&r->dl_small, 2 * sizeof(long long), cudaHostAllocPortable));
+    const size_t small = 16 + (size_t)r->ng * (8 + 8 + 4 + 4);
+    if (!r->dl_small) {
+        for (size_t i = 0; i < ctx->small_free.size(); i++)
+            if (ctx->small_free[i].second >= small) {
+                r->dl_small = ctx->small_free[i].first;
+                r->dl_small_cap = ctx->small_free[i].second;
+                ctx->small_free.erase(ctx->small_free.begin() + i);
+                break;
+            }
+        if (!r->dl_small) {
+            const size_t cap = std::max<size_t>(small, 4096);
+            CK(cudaHostAlloc(reinterpret_cast<void **>(&r->dl_small), cap, cudaHostAllocPortable));
+            ctx->small_all.push_back(r->dl_small);
+            r->dl_small_cap = cap;
+        }
+    }
+    char *sm = r->dl_small;
+    double *s_rho = reinterpret_cast<double *>(sm + 16), *s_resid = s_rho + r->ng;
+    int *s_iters = reinterpret_cast<int *>(s_resid + r->ng), *s_conv = s_iters + r->ng;
     cudaStream_t s = r->stream, c = ctx->copy_stream;
     const DevProblem &h = r->h;
     // the layout change runs on the solve's stream, right behind the solve (before whatever is
@@ -1451,13 +1475,15 @@ int32_t rb_download_async(rb_context *ctx, rb_handle hd, rb_sn_result *res) {
     if (res->flux) CK(cudaMemcpyAsync(res->flux, ctx->d_dstage, need * sizeof(double), cudaMemcpyDeviceToHost, c));
     if (res->flux_cutoff && r->csd)
         CK(cudaMemcpyAsync(res->flux_cutoff, h.cutoff, r->nphi * sizeof(double), cudaMemcpyDeviceToHost, c));
-    if (res->rho) CK(cudaMemcpyAsync(res->rho, h.rho, r->ng * sizeof(double), cudaMemcpyDeviceToHost, c));
-    if (res->group_resid) CK(cudaMemcpyAsync(res->group_resid, h.resid, r->ng * sizeof(double), cudaMemcpyDeviceToHost, c));
-    if (res->group_iters) CK(cudaMemcpyAsync(res->group_iters, h.iters, r->ng * sizeof(int), cudaMemcpyDeviceToHost, c));
-    if (res->group_converged) CK(cudaMemcpyAsync(res->group_converged, h.conv, r->ng * sizeof(int), cudaMemcpyDeviceToHost, c));
-    r->dl_small[1] = 0;
-    CK(cudaMemcpyAsync(&r->dl_small[0], h.passes, sizeof(long long), cudaMemcpyDeviceToHost, c));
-    CK(cudaMemcpyAsync(&r->dl_small[1], h.status, sizeof(int), cudaMemcpyDeviceToHost, c));
+    // the per-group record lands in the page-locked small buffer (a copy into pageable memory
+    // would make this call wait for the flux copy queued before it); rb_download_wait hands it on
+    CK(cudaMemcpyAsync(s_rho, h.rho, r->ng * sizeof(double), cudaMemcpyDeviceToHost, c));
+    CK(cudaMemcpyAsync(s_resid, h.resid, r->ng * sizeof(double), cudaMemcpyDeviceToHost, c));
+    CK(cudaMemcpyAsync(s_iters, h.iters, r->ng * sizeof(int), cudaMemcpyDeviceToHost, c));
+    CK(cudaMemcpyAsync(s_conv, h.conv, r->ng * sizeof(int), cudaMemcpyDeviceToHost, c));
+    memset(sm, 0, 16);
+    CK(cudaMemcpyAsync(sm, h.passes, sizeof(long long), cudaMemcpyDeviceToHost, c));
+    CK(cudaMemcpyAsync(sm + 8, h.status, sizeof(int), cudaMemcpyDeviceToHost, c));
     CK(cudaEventRecord(ctx->dl_done, c));
     ctx->dl_busy = true;
     r->dl_pending = true;
@@ -1474,8 +1500,19 @@ int32_t rb_download_wait(rb_context *ctx, rb_handle hd) {
     // the copy stream runs in order: the last download's event covers every earlier one
     CK(cudaEventSynchronize(ctx->dl_done));
     r->dl_pending = false;
-    r->dl_res->passes = r->dl_small[0];
-    const int status = (int)r->dl_small[1];
+    const char *sm = r->dl_small;
+    const double *s_rho = reinterpret_cast<const double *>(sm + 16), *s_resid = s_rho + r->ng;
+    const int *s_iters = reinterpret_cast<const int *>(s_resid + r->ng), *s_conv = s_iters + r->ng;
+    rb_sn_result *res = r->dl_res;
+    if (res->rho) memcpy(res->rho, s_rho, r->ng * sizeof(double));
+    if (res->group_resid) memcpy(res->group_resid, s_resid, r->ng * sizeof(double));
+    if (res->group_iters) memcpy(res->group_iters, s_iters, r->ng * sizeof(int));
+    if (res->group_converged) memcpy(res->group_converged, s_conv, r->ng * sizeof(int));
+    long long passes = 0;
+    int status = 0;
+    memcpy(&passes, sm, sizeof(long long));
+    memcpy(&status, sm + 8, sizeof(int));
+    res->passes = passes;
     if (status & RB_DEV_TIMEOUT) return fail(ctx, RB_ERR_TIMEOUT, "a device wait gave up");
     if (status & RB_DEV_BAD_TABLE) return fail(ctx, RB_ERR_INVALID, "singular cell system or bad table");
     return RB_OK;
@@ -1491,7 +1528,7 @@ int32_t rb_release(rb_context *ctx, rb_handle hd) {
     else if (it->second->stream) cudaStreamSynchronize(it->second->stream);
     if (it->second->solve_done) cudaEventDestroy(it->second->solve_done);
     if (it->second->dl_pending && ctx->dl_done) cudaEventSynchronize(ctx->dl_done);
-    if (it->second->dl_small) cudaFreeHost(it->second->dl_small);
+    if (it->second->dl_small) ctx->small_free.push_back({it->second->dl_small, it->second->dl_small_cap});
     // the problem's stream is idle (synchronised above): the block goes back to the pool in the
     // context stream's order, without waiting for other streams' work
     cudaFreeAsync(it->second->block, ctx->stream);
