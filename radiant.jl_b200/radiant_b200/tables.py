@@ -117,14 +117,6 @@ def gauss_legendre_chebychev(N: int):
     return [mu, eta, xi], w
 
 
-def newton_bisection(f, dfdx, a: float, b: float, tol: float = 1e-12, maxit: int = 100):
-    """Safeguarded Newton iteration inside a bracketing interval
-    (src/tools/newton_bisection.jl)."""
-    from .newton import newton_bisection as _nb
-
-    return _nb(f, dfdx, a, b, tol, maxit)
-
-
 def quadrature(N: int, qtype: str, Ndims: int = 1, Qdims: int | None = None):
     """Directions and weights (src/tools/quadrature.jl:19-58). 1D returns (mu, w); the
     unit-sphere types return ([mu, eta, xi], w), folded onto ξ ≥ 0 when Qdims == 2."""
