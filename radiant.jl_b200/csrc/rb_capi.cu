@@ -275,6 +275,7 @@ struct rb_context {
     uint64_t budget = 0;
     uint64_t used = 0;
     cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;  // problem blocks (stream-ordered allocation)
     std::string err;
     std::map<int64_t, std::unique_ptr<ProblemRec>> probs;
     int64_t next_handle = 1;
@@ -1249,10 +1250,10 @@ int upload_impl(rb_context *ctx, const rb_sn_problem *P0, const rb_source_set *s
     }
     auto rec = std::make_unique<ProblemRec>();
     cudaStream_t s = ctx->stream;
-    // stream-ordered allocation from the device's pool: unlike cudaMalloc / cudaFree it does not
+    // stream-ordered allocation from the context's pool: unlike cudaMalloc / cudaFree it does not
     // wait for kernels running on other streams, so an upload overlaps a solve in flight and a
     // release does not stall the requests still running
-    CK(cudaMallocAsync(&rec->block, L.off, s));
+    CK(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&rec->block), L.off, ctx->pool, s));
     rec->bytes = L.off;
     DevProblem &h = rec->h;
     st = place_problem(ctx, P, D, o, rec->block, s, h, &rec->d, ctx->d_stage, src ? &defs : nullptr);
@@ -1299,13 +1300,22 @@ int32_t rb_create(int32_t device, uint64_t hbm_budget_bytes, rb_context **out) {
     if (const char *lo = getenv("RB_LOCAL1D")) c->local1d = atoi(lo) != 0;
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { delete c; return fail(nullptr, RB_ERR_CUDA, "stream: %s", cudaGetErrorString(e)); }
-    // problem blocks come from the device's default pool (cudaMallocAsync); the pool keeps what
-    // is freed for the next upload instead of unmapping it at every synchronisation
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    // problem blocks come from the context's own stream-ordered pool: it keeps what is freed for
+    // the next upload instead of unmapping it at every synchronisation, and gives everything back
+    // when the context is destroyed (the device's default pool, which other code in the process
+    // may use, is left as it is)
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    e = cudaMemPoolCreate(&c->pool, &props);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return fail(nullptr, RB_ERR_CUDA, "memory pool: %s", cudaGetErrorString(e));
     }
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     *out = c;
     return RB_OK;
 }
@@ -1321,6 +1331,7 @@ int32_t rb_destroy(rb_context *ctx) {
     for (char *p : ctx->small_all) cudaFreeHost(p);
     ctx->probs.clear();
     cudaStreamSynchronize(ctx->stream);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     if (ctx->d_list) cudaFree(ctx->d_list);
     if (ctx->d_queue) cudaFree(ctx->d_queue);
     if (ctx->d_stage) cudaFree(ctx->d_stage);
