@@ -96,3 +96,38 @@ def test_launch_rule_struct_and_table_shape():
         assert r["ndims"] in (1, 2, 3) and r["cluster"] in (1, 2, 4, 8, 16) and r["nd_max"] > 0
     keys = [(r["batch_max"], r["work_max"]) for r in rules]
     assert keys == sorted(keys)
+
+
+def test_ctypes_mirrors_match_the_header_layout(tmp_path):
+    """Every struct of the header has the size and field offsets of its ctypes mirror: the C
+    compiler's layout (gcc on the header itself) against ctypes'."""
+    import shutil
+    import subprocess
+
+    from radiant_b200 import _abi as A
+    from radiant_b200 import sources as S
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    mirrors = {"rb_sn_problem": A.RbSnProblem, "rb_sn_result": A.RbSnResult, "rb_coupling": A.RbCoupling,
+               "rb_launch_rule": A.RbLaunchRule, "rb_volume_box": S.RbVolumeBox,
+               "rb_surface_beam": S.RbSurfaceBeam, "rb_source_set": S.RbSourceSet}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HDR}"', 'int main(void) {']
+    for cname, py in mirrors.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call([cc, "-std=c99", "-o", str(exe), str(src)])
+    got = {}
+    for line in subprocess.check_output([str(exe)], text=True).splitlines():
+        cname, what, val = line.split()
+        got[(cname, what)] = int(val)
+    for cname, py in mirrors.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
