@@ -100,3 +100,25 @@ def test_source_set_layout():
     assert ss.beams[0].face == 3 and ss.beams[0].energy_group == 2
     assert ss.boxes[0].lo[1] == -math.inf and ss.boxes[0].hi[0] == 1.0
     np.testing.assert_array_equal(np.ctypeslib.as_array(ss.beams[0].basis, (3,)), S.beam_basis(sn, 2, beam)[0][:3])
+
+
+def test_workload_definitions_rebuild_the_workload_arrays():
+    """The definitions a grid workload keeps (its volume box, its beam) rebuild exactly the dense
+    arrays its tables carry, and the tables without them take the definitions' np_source."""
+    from radiant_b200 import workloads as W
+
+    for tabs in (W.c4_tables(seed=2, particle="photon", n=8, ng=2), W.random_grid_tables(5)):
+        src = tabs["sources"]
+        ns = list(tabs["ns"])
+        vol, surf, _ = S.dense_sources(src["sn"], tabs["ndims"], tabs["ng"], ns, tabs["ds"], src["positions"],
+                                       src["volume"], src["surface"])
+        if vol is not None:
+            np.testing.assert_array_equal(tabs["volume_sources"][:, :1, :1], vol)
+            assert not tabs["volume_sources"][:, 1:].any()
+        for f in range(2 * tabs["ndims"]):
+            if surf is not None and surf[f] is not None:
+                k = tabs["np_source"]
+                np.testing.assert_array_equal(tabs["surface_sources"][f], surf[f][:, :k])
+        bare, sset = W.without_dense_sources(tabs)
+        assert bare["volume_sources"] is None and all(a is None for a in bare["surface_sources"])
+        assert sset.np_source == tabs["np_source"]
