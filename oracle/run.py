@@ -69,3 +69,39 @@ def transport(parts, couplings, ngen_max=50, eps_gen=1e-6, conv_type=0, sigma_de
     if deposition:
         return res, int(ngen.value), float(eps.value), dep
     return res, int(ngen.value), float(eps.value)
+
+
+def sources(ndims, ng, ns, widths, positions, source_set, nps):
+    """oracle_sources: (volume sources [ng, ncell] or None, per-face surface sources [ng, nps, face
+    cells] for the faces beams enter, normalization factors) of an rb_source_set's definitions."""
+    import numpy as np
+
+    L = lib()
+    dp = C.POINTER(C.c_double)
+    S = source_set.S
+    ns3 = [int(v) for v in ns] + [1] * (3 - len(ns))
+    ncell = int(np.prod(ns3))
+    w = [np.ascontiguousarray(widths[a], dtype=np.float64) for a in range(ndims)]
+    p = [np.ascontiguousarray(positions[a], dtype=np.float64) for a in range(ndims)]
+    nsa = (C.c_int32 * 3)(*ns3)
+    wa = (dp * 3)(*[w[a].ctypes.data_as(dp) if a < ndims else None for a in range(3)])
+    pa = (dp * 3)(*[p[a].ctypes.data_as(dp) if a < ndims else None for a in range(3)])
+    vol = np.zeros((ng, ncell), order="F") if S.nvolume else None
+    faces = [None] * 6
+    for k in range(S.nsurface):
+        f = source_set.beams[k].face
+        ax = [a for a in range(ndims) if a != f // 2]
+        ncf = int(np.prod([ns3[a] for a in ax])) if ax else 1
+        if faces[f] is None:
+            faces[f] = np.zeros((ng, nps, ncf), order="F")
+    fa = (dp * 6)(*[a.ctypes.data_as(dp) if a is not None else None for a in faces])
+    basis = np.concatenate(source_set.bases) if source_set.bases else np.zeros(1)
+    norms = np.zeros(max(1, S.nvolume + S.nsurface))
+    L.oracle_sources.restype = C.c_int
+    st = L.oracle_sources(C.c_int32(ndims), nsa, wa, pa, C.c_int32(ng), C.c_int32(nps), C.c_int32(S.nvolume),
+                          C.cast(S.volume, C.c_void_p), C.c_int32(S.nsurface), C.cast(S.surface, C.c_void_p),
+                          basis.ctypes.data_as(dp), vol.ctypes.data_as(dp) if vol is not None else None, fa,
+                          norms.ctypes.data_as(dp))
+    if st != 0:
+        raise ValueError("oracle_sources: bad definitions")
+    return vol, faces, norms[:S.nvolume + S.nsurface]

@@ -12,6 +12,9 @@
  *   cell_closure          <- flux_{1,2,3}D_{BTE,BFP}    sn_1D_bte.jl:27-65, sn_1D_bfp.jl:39-125,
  *                                                       sn_2D_bte.jl:35-116, sn_2D_bfp.jl:45-154,
  *                                                       sn_3D_bte.jl:42-152, sn_3D_bfp.jl:52-191
+ *   oracle_sources        <- volume_source, surface_source (SN), Source.add_source
+ *                                                       volume_source.jl:21-122, surface_source.jl:22-330,
+ *                                                       src/structures/Source.jl:129-203
  *   gmres / bicgstab / anderson / livolant
  *                         <- src/tools/gmres.jl:35-133, bicgstab.jl:30-101, anderson.jl:38-140,
  *                            livolant.jl:69-154, krylov_state.jl:53-144
@@ -1240,4 +1243,80 @@ int oracle_transport(int32_t npart, const rb_sn_problem *const *probs, const rb_
     free(tot); free(ps); free(prev); free(gen); free(src); free(tot_cut); free(gen_cut); free(nall); free(nphi);
     free(order);
     return st;
+}
+
+/* ---- fixed sources ----------------------------------------------------------------------------
+ * oracle_sources <- volume_source (src/particle_transport/volume_source.jl:21-122), the SN branch of
+ * surface_source (surface_source.jl:22-330) and Source.add_source (src/structures/Source.jl:129-203):
+ * the volume sources [ng, ncell] (angular moment 1, cell moment 1; cells column-major) and the
+ * surface sources of each face [ng, nps, face cells], summed source after source, with each
+ * source's normalization factor (boxes first, then beams). The beams' half-range basis values are
+ * given (basis[k*nps + p]); a face no beam enters is left untouched. */
+int oracle_sources(int32_t ndims, const int32_t *ns, const double *const *widths, const double *const *pos,
+                   int32_t ng, int32_t nps, int32_t nvol, const rb_volume_box *vol, int32_t nsurf,
+                   const rb_surface_beam *surf, const double *basis, double *vol_out, double *const *surf_out,
+                   double *norms) {
+    const int32_t n0 = ns[0], n1 = ndims >= 2 ? ns[1] : 1, n2 = ndims >= 3 ? ns[2] : 1;
+    const int64_t ncell = (int64_t)n0 * n1 * n2;
+    for (int32_t b = 0; b < nvol; b++) {
+        const rb_volume_box *B = &vol[b];
+        const int32_t g = B->energy_group - 1;
+        if (g < 0 || g >= ng) return 1;
+        double norm = 0.0;
+        for (int32_t ix = 0; ix < n0; ix++)
+            for (int32_t iy = 0; iy < n1; iy++)
+                for (int32_t iz = 0; iz < n2; iz++) {
+                    int in = B->lo[0] <= pos[0][ix] && B->hi[0] >= pos[0][ix];
+                    if (ndims >= 2) in = in && B->lo[1] <= pos[1][iy] && B->hi[1] >= pos[1][iy];
+                    if (ndims >= 3) in = in && B->lo[2] <= pos[2][iz] && B->hi[2] >= pos[2][iz];
+                    if (!in) continue;
+                    const int64_t c = ix + (int64_t)n0 * (iy + (int64_t)n1 * iz);
+                    const double q = 0.0 + B->intensity; /* Q of this source, then added to the total */
+                    vol_out[g + (int64_t)ng * c] = vol_out[g + (int64_t)ng * c] + q;
+                    double t = B->intensity * widths[0][ix];
+                    if (ndims >= 2) t = t * widths[1][iy];
+                    if (ndims >= 3) t = t * widths[2][iz];
+                    norm = norm + t;
+                }
+        if (norms) norms[b] = norm;
+    }
+    (void)ncell;
+    for (int32_t k = 0; k < nsurf; k++) {
+        const rb_surface_beam *B = &surf[k];
+        const int32_t g = B->energy_group - 1, f = B->face, ax = f / 2;
+        if (g < 0 || g >= ng || f < 0 || f >= 2 * ndims) return 1;
+        double *Q = surf_out[f];
+        const double cosv = B->direction[ax];
+        const int enters = (f % 2 == 0) ? cosv > 0 : cosv < 0;
+        int a = -1, c = -1, m = 0;
+        for (int d = 0; d < ndims; d++)
+            if (d != ax) { if (m == 0) a = d; else c = d; m++; }
+        double norm = 0.0;
+        if (ndims == 1) {
+            norm = B->intensity;
+            if (enters)
+                for (int32_t p = 0; p < nps; p++) Q[g + (int64_t)ng * p] = Q[g + (int64_t)ng * p] + B->intensity * basis[(int64_t)k * nps + p];
+        } else {
+            const int32_t na = ns[a], nc = c >= 0 ? ns[c] : 1;
+            for (int32_t ia = 0; ia < na; ia++) {
+                if (pos[a][ia] < B->lo[a] || pos[a][ia] > B->hi[a]) continue;
+                for (int32_t ic = 0; ic < nc; ic++) {
+                    if (c >= 0 && (pos[c][ic] < B->lo[c] || pos[c][ic] > B->hi[c])) continue;
+                    const int64_t cell = ia + (int64_t)na * ic;
+                    if (enters)
+                        for (int32_t p = 0; p < nps; p++) {
+                            double q = B->intensity * basis[(int64_t)k * nps + p] * widths[a][ia];
+                            if (c >= 0) q = q * widths[c][ic];
+                            double *v = &Q[g + (int64_t)ng * (p + (int64_t)nps * cell)];
+                            *v = *v + q;
+                        }
+                    double t = B->intensity * widths[a][ia];
+                    if (c >= 0) t = t * widths[c][ic];
+                    norm += t;
+                }
+            }
+        }
+        if (norms) norms[nvol + k] = norm;
+    }
+    return 0;
 }

@@ -122,3 +122,53 @@ def test_workload_definitions_rebuild_the_workload_arrays():
         bare, sset = W.without_dense_sources(tabs)
         assert bare["volume_sources"] is None and all(a is None for a in bare["surface_sources"])
         assert sset.np_source == tabs["np_source"]
+
+
+@pytest.mark.parametrize("ndims", [1, 2, 3])
+def test_host_builders_against_the_oracle(ndims):
+    """The Python host builders (the dense path) against the oracle's C restatement
+    (oracle_sources) on seeded random definitions: identical arrays and normalization factors."""
+    from oracle import run as orun
+
+    rng = np.random.default_rng(10 + ndims)
+    if ndims == 1:
+        sn = SNSettings(solver_type="BTE", quadrature_type="gauss-legendre", quadrature_order=16, legendre_order=5,
+                        scheme_type={"x": "DD"}, scheme_order={"x": 1}, acceleration="gmres",
+                        convergence_criterion=1e-10, angular_boltzmann="standard")
+        ns = [37]
+    else:
+        sn = SNSettings(solver_type="BTE", quadrature_type="carlson", quadrature_order=4, legendre_order=3,
+                        scheme_type={a: "DD" for a in "xyz"[:ndims]}, scheme_order={a: 1 for a in "xyz"[:ndims]},
+                        acceleration="gmres", convergence_criterion=1e-10, angular_boltzmann="galerkin-d")
+        ns = [9, 7, 5][:ndims]
+    ng = 4
+    widths = [rng.uniform(0.1, 0.5, n) for n in ns]
+    pos = [S.positions_of(w) for w in widths]
+    ext = [float(np.sum(w)) for w in widths]
+
+    def box():
+        out = {}
+        for a in range(ndims):
+            lo, hi = np.sort(rng.uniform(-0.1, ext[a] + 0.1, 2))
+            out["xyz"[a]] = (float(lo), float(hi))
+        return out
+
+    vols = [S.VolumeSource(int(rng.integers(1, ng + 1)), box(), float(rng.uniform(0.1, 3.0))) for _ in range(4)]
+    faces = S.FACES[:2 * ndims]
+    beams = []
+    for _ in range(5):
+        f = faces[int(rng.integers(0, len(faces)))]
+        d = rng.normal(size=3)
+        d = tuple(d / np.linalg.norm(d))
+        aperture = {k: v for k, v in box().items() if k != "xyz"[faces.index(f) // 2]}
+        beams.append(S.SurfaceSource(int(rng.integers(1, ng + 1)), f, d, aperture, float(rng.uniform(0.2, 2.0)),
+                                     legendre_order=int(rng.integers(1, 4))))
+    vol, surf, norms = S.dense_sources(sn, ndims, ng, ns, widths, pos, vols, beams)
+    sset = S.SourceSet(sn, ndims, pos, vols, beams)
+    ovol, osurf, onorms = orun.sources(ndims, ng, ns, widths, pos, sset, sset.np_source)
+    np.testing.assert_array_equal(vol.reshape(ng, -1, order="F"), ovol)
+    for f in range(2 * ndims):
+        assert (surf[f] is None) == (osurf[f] is None)
+        if surf[f] is not None:
+            np.testing.assert_array_equal(surf[f], osurf[f])
+    np.testing.assert_array_equal(np.asarray(norms), onorms)
