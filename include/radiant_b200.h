@@ -154,7 +154,10 @@ typedef int64_t rb_handle;
 
 /* ---- context ------------------------------------------------------------------------- */
 /* Replaces nothing in the reference (which owns no device); the context holds the device,
- * its stream pool and the HBM budget that admission control checks against. */
+ * its stream pool and the HBM budget that admission control checks against. Problem memory
+ * comes from a stream-ordered memory pool the context owns: uploads and releases do not wait
+ * for kernels on other streams, freed blocks are kept for later uploads, and rb_destroy gives
+ * everything back. */
 RB_API int32_t rb_create(int32_t device, uint64_t hbm_budget_bytes, rb_context **ctx);
 RB_API int32_t rb_destroy(rb_context *ctx);
 /* Copies the message of the last failed call on ctx (or of the last rb_create failure when
